@@ -1,0 +1,316 @@
+"""Benchmark: PCG ms per optimisation iteration on the 96x192x96 cantilever.
+
+Workload (the metric's configuration): true(96,192,96) voxels (1,769,472
+elements, 5,447,811 DOFs), cantilever BCs (optCase 1), E0 = 1, Emin = 1e-9,
+nu = 0.3, SIMP p = 3, five multigrid levels (coarsestResolutionControl 400;
+192x96x96 -> 48x24x24 -> 24x12x12 -> 12x6x6 -> 6x3x3), damped Jacobi
+omega = 0.6, relative residual 1e-6.  One step = one optimisation
+iteration's FEA: SIMP moduli from the design, Galerkin assembly of every
+coarse level + coarsest Cholesky, and the PCG state solve warm-started from
+the previous iteration (TOP_GPU.m:180-187).  The design and warm start of a
+step are those of optimisation iteration 1 (x = V0 = 0.12 everywhere, U from
+the fully solid solve), so every step does identical work.
+
+value = PCG ms per optimisation iteration of the mixed-precision path
+(FP32 V-cycle, FP64 outer recurrence / matvec / coarsest Cholesky), device
+time from CUDA events with inputs resident in HBM.  The same steps run with
+the plain FP64 path for the ratio and the compliance error.  e2e repeats the
+step through the C ABI with the design on the host (pinned) and the
+compliance read back every step.
+
+--impl reference times the FP64 CPU restatement of the reference (oracle/,
+the MATLAB driver cannot run here) on the host cores on a bounded sample.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SHAPE = (96, 192, 96)
+CONTROL = 400
+V0 = 0.12
+E0, EMIN, PENAL, NU = 1.0, 1e-9, 3.0, 0.3
+TOL, MAXIT, OMEGA = 1e-6, 800, 0.6
+WORKLOAD = "cantilever_96x192x96_optiter1"
+
+
+def _env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if self.p is None:
+            return out
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if rows:
+            sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+            mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+            out = {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                   "reasons": reasons, "samples": len(rows)}
+        try:
+            os.unlink(self.f.name)
+        except OSError:
+            pass
+        return out
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _cpu_cores():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def cpu_sample(iters=2, gpu_its=None):
+    """Oracle (FP64 C + OpenMP) PCG iterations on the same problem; ms per iteration."""
+    from oracle import oracle as O
+    cores = _cpu_cores()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    mask = np.ones(SHAPE, bool)
+    o = O.Model(mask, control=CONTROL)
+    o.apply_optcase(1)
+    o.set_material(E0, EMIN, PENAL)
+    o.set_solver(TOL, MAXIT, OMEGA)
+    ne = o.level(0).numElements
+    o.set_density(np.full(ne, V0))
+    t0 = time.perf_counter()
+    o.assemble()
+    t_asm = time.perf_counter() - t0
+    b = o.F()[:, 0]
+    t0 = time.perf_counter()
+    _, its, _ = o.pcg(b, maxIT=iters, tol=1e-300)
+    t_it = (time.perf_counter() - t0) / its
+    return {"ms_per_pcg_iter": 1e3 * t_it, "assemble_ms": 1e3 * t_asm, "cores": cores, "iters": its}
+
+
+def run_reference(args):
+    rank, world, _ = _env_rank()
+    if rank != 0:
+        return
+    samples = []
+    for k in range(args.warmup + args.steps):
+        s = cpu_sample(iters=2)
+        if k >= args.warmup:
+            samples.append(s)
+    ms_it = float(np.mean([s["ms_per_pcg_iter"] for s in samples]))
+    its = args.ref_its
+    value = ms_it * its
+    line = {
+        "impl": "reference", "metric": "PCG ms/opt-iter", "value": value, "unit": "ms",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOAD, "shape": list(SHAPE), "levels": 5, "tol": TOL},
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": samples[0]["cores"], "kind": "port",
+                         "sample": "2 FP64 PCG iterations of the oracle per step, ms/iteration x %d iterations "
+                                   "(the FP64 iteration count of this problem)" % its},
+        "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    from top_gpu_on_matlab_b200._lib import check, lib
+    import ctypes as C
+
+    rank, world, local = _env_rank()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    mask = np.ones(SHAPE, bool)
+    mesh = Mesh(mask, control=CONTROL)
+    mesh.apply_optcase(1)
+    info = mesh.info()
+    ne, nn = info[0]["numElements"], info[0]["numNodes"]
+    solvers = {}
+    for name, mixed in (("mixed", True), ("fp64", False)):
+        solvers[name] = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=mixed)
+    # optimisation iteration 0: fully solid solve (TOP_GPU.m:144-155)
+    s64 = solvers["fp64"]
+    s64.set_modulus(torch.full((ne,), E0, dtype=torch.float64, device=dev))
+    s64.assemble()
+    U_solid, its_solid, _ = s64.pcg(0)
+    x = torch.full((ne,), V0, dtype=torch.float64, device=dev)
+    F = torch.from_numpy(mesh.get(0, "F")).to(dev)
+    stream = torch.cuda.current_stream()
+
+    def step(s, U0):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        s.set_density(x)
+        s.assemble()
+        ev[1].record(stream)
+        U, its, res = s.pcg(0, U=U0)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        return U, its, res, ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+
+    results = {}
+    for name in ("fp64", "mixed"):
+        s = solvers[name]
+        for _ in range(args.warmup):
+            step(s, U_solid)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = Clocks(local) if name == "mixed" else None
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        asm, pcg, its_l = [], [], []
+        U = None
+        for _ in range(args.steps):
+            U, its, res, ta, tp = step(s, U_solid)
+            asm.append(ta); pcg.append(tp); its_l.append(its)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        total = t0.elapsed_time(t1)
+        clocks = clk.stop() if clk else None
+        vals = torch.tensor([float(np.mean(pcg)), total / args.steps, float(np.mean(asm))], device=dev)
+        if world > 1:
+            dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+        results[name] = dict(pcg_ms=float(vals[0]), step_ms=float(vals[1]), asm_ms=float(vals[2]), its=its_l[-1],
+                             compliance=float(F @ U), clocks=clocks)
+    mixed, fp64 = results["mixed"], results["fp64"]
+    comp_err = abs(mixed["compliance"] - fp64["compliance"]) / abs(fp64["compliance"])
+
+    # ---- e2e through the C ABI with the design on the host (pinned) ----
+    s = solvers["mixed"]
+    x_host = torch.full((ne,), V0, dtype=torch.float64).pin_memory()
+    c_host = torch.zeros(1, dtype=torch.float64).pin_memory()
+    xd = torch.empty_like(x_host, device=dev)
+    U_dev = U_solid.clone()
+    e2e = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        xd.copy_(x_host, non_blocking=True)
+        s.set_density(xd)
+        s.assemble()
+        U, its, res = s.pcg(0, U=U_dev)
+        c_host.copy_((F @ U).reshape(1), non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k >= args.warmup:
+            e2e.append(e0.elapsed_time(e1))
+    e2e_ms = float(np.mean(e2e))
+
+    # ---- kernel roofline: level-0 stiffness products, L2 flushed ----
+    peak, peak_kind = _peaks()
+    flush = 512 << 20
+    tk = {}
+    for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32"), (3, "l1_f32")):
+        ms = C.c_double(0)
+        check(lib().top_solver_time_kernel(s._h, which, 20, flush, C.byref(ms)), "time_kernel")
+        tk[key] = ms.value
+    bytes64 = 6 * nn * 8 + ne * 8
+    bytes32 = 6 * nn * 4 + ne * 4
+    flops = 1152 * ne
+    # mixed PCG iteration: 1 FP64 outer product + 2 FP32 level-0 smoother products
+    share64, share32 = tk["l0_f64"], 2 * tk["l0_f32"]
+    if share64 >= share32:
+        dom, t_dom, byt = "l0_kernel<double> (outer K*p)", tk["l0_f64"], bytes64
+    else:
+        dom, t_dom, byt = "l0_kernel<float> (V-cycle smoother K*u)", tk["l0_f32"], bytes32
+    achieved = byt / (t_dom * 1e-3) / 1e9
+    line = {
+        "metric": "PCG ms/opt-iter", "value": mixed["pcg_ms"], "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed["step_ms"],
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "shape": list(SHAPE), "elements": ne, "dofs": 3 * nn, "levels": len(info),
+                   "control": CONTROL, "tol": TOL, "precision": "mixed (FP32 V-cycle, FP64 outer)",
+                   "l2": "working set > L2 per PCG iteration; kernel timings flush L2",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "pcg_its": mixed["its"], "fp64_pcg_ms": fp64["pcg_ms"], "fp64_pcg_its": fp64["its"],
+        "mixed_vs_fp64_speedup": fp64["pcg_ms"] / mixed["pcg_ms"],
+        "compliance_rel_err_mixed_vs_fp64": comp_err,
+        "assembly_ms": mixed["asm_ms"], "fp64_assembly_ms": fp64["asm_ms"],
+        "kernel_ms": tk,
+        "matvec_gbs": {"fp64": bytes64 / (tk["l0_f64"] * 1e-3) / 1e9, "fp32": bytes32 / (tk["l0_f32"] * 1e-3) / 1e9},
+        "matvec_tflops": {"fp64": flops / (tk["l0_f64"] * 1e-3) / 1e12, "fp32": flops / (tk["l0_f32"] * 1e-3) / 1e12},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": None},
+        "gpu_launches": None,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": ne * 8, "d2h_bytes_per_step": 8,
+                "includes": "H2D design, SIMP, assembly, PCG, D2H compliance"},
+        "clocks": mixed["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cs = cpu_sample(iters=2)
+        line["cpu_baseline"] = {"value": cs["ms_per_pcg_iter"] * fp64["its"], "unit": "ms", "cores": cs["cores"],
+                                "kind": "port",
+                                "sample": "2 FP64 PCG iterations of the oracle (C + OpenMP) on this problem, "
+                                          "ms/iteration x the FP64 iteration count (%d)" % fp64["its"],
+                                "assemble_ms": cs["assemble_ms"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--ref-its", type=int, default=60, help="FP64 iteration count used to scale the CPU sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

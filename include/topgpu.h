@@ -1,0 +1,206 @@
+/*
+ * topgpu.h -- C ABI of libtopgpu.so, a B200 (sm_100a) implementation of the
+ * TOP_GPU FEA hot path: matrix-free voxel stiffness product, multigrid-
+ * preconditioned CG and Galerkin coarse-stiffness assembly.
+ *
+ * Conventions
+ *   - Every function returns a status: TOP_OK (0) or a negative TOP_ERR_*.
+ *     top_last_error() returns a message for the calling thread's last error.
+ *   - Array arguments are plain pointers.  Unless a function says "host",
+ *     pointers are CUDA device pointers on the current device.
+ *   - Arrays follow MATLAB layout: column-major, index arrays are int32 (or
+ *     uint32 where stated) holding 1-based indices, 0 = void / none.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream, which is what MATLAB's MEX calls use).
+ *   - dtype: TOP_F32 (MATLAB single) or TOP_F64 (MATLAB double).
+ *
+ * Part 1 mirrors the six MEX gateways of mnivan/TOP_GPU_on_matlab one to one
+ * (same arguments, same in-place semantics).  Part 2 is the host mesh model
+ * (voxel discretisation, mesh hierarchy, boundary conditions) and Part 3 the
+ * fused device solver that replaces Solving_PCG / Solving_Vcycle /
+ * Solving_KbyU_MatrixFree / Solving_AssembleFEAstencil of TOP_GPU.m.
+ */
+#ifndef TOPGPU_H
+#define TOPGPU_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TOP_OK                 0
+#define TOP_ERR_ARGS          -1   /* <Name>:Args / arity                     */
+#define TOP_ERR_TYPE          -2   /* <Name>:Type                             */
+#define TOP_ERR_SHAPE         -3   /* <Name>:Shape                            */
+#define TOP_ERR_CUDA          -4   /* <Name>:CUDA                             */
+#define TOP_ERR_NOT_CONVERGED -5   /* PCG reached maxIT (TOP_GPU.m:656-659)   */
+#define TOP_ERR_NAN           -6   /* non-finite PCG scalar                   */
+#define TOP_ERR_NOMEM         -7
+#define TOP_ERR_STATE         -8   /* call out of order (e.g. no assembly)    */
+
+#define TOP_F32 1
+#define TOP_F64 2
+
+const char *top_last_error(void);
+int top_version(void);
+
+/* ======================================================================= */
+/* Part 1 -- drop-in replacements of the MEX kernels                        */
+/* ======================================================================= */
+
+/* Gathering_inplace(gUMat, gU, gE)   (Gathering_inplace.cu:75-171)
+ * uMat[nElem x 24] (overwritten) = u[eNod(e,n)-1, c] at column 3n+c.
+ * u: [nNodes x 3]; eNod: [nElem x 8] int32 (eNodIsU32 = 0) or uint32. */
+int top_gather(void *uMat, const void *u, const void *eNod, int eNodIsU32,
+               int64_t nElem, int64_t nNodes, int dtype, void *stream);
+
+/* Scattering_inplace(Y, eNodMat, uMat)   (Scattering_inplace.cu:81-146)
+ * Y[nNodes x 3] += uMat rows; node ids outside [1, nNodes] are skipped.
+ * Synchronises the stream before returning, as the reference does (141). */
+int top_scatter(void *Y, const int32_t *eNod, const void *uMat,
+                int64_t nElem, int64_t nNodes, int dtype, void *stream);
+
+/* scatter_accum3_inplace(keys, Tmp, xF)   (scatter_accum3_inplace.cu:115-145)
+ * xF[key-1, 0..2] += Tmp[i, 0..2]; keys outside [1, M] are skipped. */
+int top_scatter_accum3(const int32_t *keys, const void *Tmp, int64_t N,
+                       void *xF, int64_t M, int dtype, void *stream);
+
+/* assembleKs_level2_inplace(d_Ks, d_upMap, d_eleModulus, d_K_0, d_Pch,
+ *   d_mapUnique, d_uniqueFree, d_uniqueFixed)
+ *   (assembleKs_level2_inplace.cu:165-284)
+ * Ks[24x24xnElem] = sum_s Pch_s' * Kch_s * Pch_s, Kch = E*K0, or
+ * E*uniqueFree(:,uid) + uniqueFixed(:,uid) for children with mapUnique > 0.
+ * nUnique = 0 (and NULL free/fixed) disables the boundary branch. */
+int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void *eleModulus,
+                           const void *K0, const void *Pch, const int32_t *mapUnique,
+                           const void *uniqueFree, const void *uniqueFixed,
+                           int64_t nElem, int nCh, int64_t nFine, int64_t nUnique,
+                           int dtype, void *stream);
+
+/* assembleKs_higherLevel_inplace(d_Ks, d_upMap, d_KsPrev, d_Psub)
+ *   (assembleKs_higherLevel_inplace.cu:134-217) */
+int top_assemble_ks_higher(void *Ks, const int32_t *upMap, const void *KsPrev,
+                           const void *Psub, int64_t nElem, int nSub, int64_t nFine,
+                           int dtype, void *stream);
+
+/* assembleKs_level2_superEle_inplace(d_Ks, d_upMap, d_Ks0, d_Psub,
+ *   d_mapUnique, d_eleModulus, d_uniqueFree, d_uniqueFixed)
+ *   (assembleKs_level2_superEle_inplace.cu:178-325)
+ * eleModulus [64 x nFine]; uniqueFree [576 x 64 x nUnique]. */
+int top_assemble_ks_level2_super(void *Ks, const int32_t *upMap, const void *Ks0,
+                                 const void *Psub, const int32_t *mapUnique,
+                                 const void *eleModulus, const void *uniqueFree,
+                                 const void *uniqueFixed, int64_t nElem, int nSub,
+                                 int64_t nFine, int64_t nUnique, int dtype, void *stream);
+
+/* ======================================================================= */
+/* Part 2 -- host mesh model (no GPU needed)                                 */
+/* ======================================================================= */
+typedef struct top_mesh top_mesh;
+
+/* Voxel discretisation + mesh hierarchy (FEA_VoxelBasedDiscretization
+ * TOP_GPU.m:2019-2119, Solving_BuildingMeshHierarchy 1276-1434).
+ * mask: host [nely x nelx x nelz] col-major, nonzero = solid.
+ * control = coarsestResolutionControl_ (TOP_GPU.m:42, default 20000).
+ * cellSize: 1/nelx for logical-array models, 1 for file models. */
+int top_mesh_create(const uint8_t *mask, int nely, int nelx, int nelz,
+                    int control, double nu, double cellSize, int superElement,
+                    top_mesh **out);
+int top_mesh_destroy(top_mesh *m);
+
+/* Built-in cantilever (1) / MBB (2) boundary conditions (TOP_GPU.m:505-534),
+ * then FEA_ApplyBoundaryCondition (1505-1546) and the fixed-DOF element
+ * matrices of Solving_SetupKeWithFixedDOFs (1548-1727). */
+int top_mesh_apply_optcase(top_mesh *m, int optCase);
+/* Generic BCs (the .TopVoxel semantics, TOP_GPU.m:441-461), host arrays:
+ * fixRows [nFix x 4] row-major (node 1-based compact, fixX, fixY, fixZ);
+ * loadRows[k] [nLoadRows[k] x 4] row-major (node, fx, fy, fz);
+ * weights [nLoads] or NULL for the mean (objWeightingList_). */
+int top_mesh_apply_bc(top_mesh *m, int64_t nFix, const double *fixRows,
+                      int nLoads, const int64_t *nLoadRows,
+                      const double *const *loadRows, const double *weights);
+
+/* Sizes: out[0] numLevels, then per level l (8 values each, from index
+ * 1 + 8*l): resX, resY, resZ, spanWidth, numElements, numNodes,
+ * intermediateNumNodes, nUnique (level 0 only).  Fills min(n, total). */
+int top_mesh_info(const top_mesh *m, int64_t *out, int n);
+
+/* Copy a named array of a level into a host buffer (MATLAB layout).
+ * Names: eleMapBack eleMapForward eNodMat nodMapBack nodMapForward
+ *   nodesOnBoundary elementsOnBoundary elementUpwardMap transferMat
+ *   transferMatCoeffi solidNodeMapCoarser2Finer RI Ke mapUniqueKes
+ *   eleWithFixedDOFs uniqueKesFree uniqueKesFixed fixingCond F objWeights
+ *   I_mat.  *count receives the element count; dst may be NULL to query. */
+int top_mesh_get(const top_mesh *m, int level, const char *name, void *dst,
+                 int64_t capacity, int64_t *count);
+
+/* ======================================================================= */
+/* Part 3 -- fused device solver                                            */
+/* ======================================================================= */
+typedef struct top_solver top_solver;
+
+#define TOP_PREC_FP64  0   /* everything FP64                                 */
+#define TOP_PREC_MIXED 1   /* V-cycle FP32, outer PCG / compliance / Cholesky FP64 */
+
+typedef struct {
+    double E0, Emin, penal;      /* modulus_, modulusMin_, SIMPpenalty_        */
+    double tol;                  /* tol_ (relative residual)                   */
+    int    maxIT;                /* maxIT_                                     */
+    double omega;                /* weightFactorJacobi_                        */
+    int    precision;            /* TOP_PREC_*                                 */
+    int    outerFP32;            /* 1: outer matvec in FP32 like the reference's
+                                    mixed mode (TOP_GPU.m:683-684)              */
+} top_solver_params;
+
+/* Upload a mesh (with BCs applied) to the current CUDA device. */
+int top_solver_create(const top_mesh *mesh, const top_solver_params *p, top_solver **out);
+int top_solver_destroy(top_solver *s);
+int top_solver_set_stream(top_solver *s, void *stream);
+
+/* Element moduli.  where: 0 = host pointer, 1 = device pointer.
+ * set_density applies SIMP: E = Emin + x^p (E0 - Emin) (TOP_GPU.m:169). */
+int top_solver_set_modulus(top_solver *s, const double *E, int where);
+int top_solver_set_density(top_solver *s, const double *xPhys, int where);
+
+/* Solving_AssembleFEAstencil (TOP_GPU.m:1033-1267): Galerkin Ks on every
+ * coarse level, Jacobi diagonals, coarsest Cholesky (FP64, on the device). */
+int top_solver_assemble(top_solver *s);
+
+/* y = K_level u on compact node-interleaved vectors [3 Nn(level)], FP64,
+ * device pointers (Solving_KbyU_MatrixFree, TOP_GPU.m:669-765).
+ * fp32 = 1 runs the FP32 path used inside the mixed V-cycle. */
+int top_solver_matvec(top_solver *s, int level, const double *u, double *y, int fp32);
+/* z = V-cycle(r), level-1 compact interleaved FP64 vectors (766-816). */
+int top_solver_vcycle(top_solver *s, const double *r, double *z);
+/* Restriction (817-847) / prolongation (848-878) between level ii-1 and ii. */
+int top_solver_restrict(top_solver *s, int ii, const double *rFine, double *rCoarse);
+int top_solver_interpolate(top_solver *s, int ii, const double *xCoarse, double *xFine);
+/* Jacobi diagonal (compact interleaved) and coarse Ks [24x24xNe] of a level. */
+int top_solver_get_diag(top_solver *s, int level, double *diag);
+int top_solver_get_ks(top_solver *s, int level, double *Ks);
+
+/* Solving_PCG (602-667) on load case k: U (device, [3 Nn] compact
+ * interleaved) is the warm start when warm = 1 and receives the solution.
+ * its / relres may be NULL.  Returns TOP_ERR_NOT_CONVERGED at maxIT. */
+int top_solver_pcg(top_solver *s, int loadCase, double *U, int warm, int *its, double *relres);
+/* Same on an explicit right-hand side b (device, compact interleaved). */
+int top_solver_pcg_rhs(top_solver *s, const double *b, double *U, int warm, int *its, double *relres);
+
+/* Element energies ce_e = sum_k w_k u_ke' Ke u_ke over the load cases
+ * (TopOpti_ComputeUnitCompliance, TOP_GPU.m:580-600), U device [3Nn x nLoads]. */
+int top_solver_unit_compliance(top_solver *s, const double *U, double *ce);
+
+/* Kernel timing with CUDA events on the solver's stream (no host copies):
+ * which = 0 level-0 K*u FP64, 1 level-0 K*u FP32, 2 one V-cycle,
+ * 3 level-1 K*u FP32; L2 is flushed by writing flushBytes before each launch.
+ * No counterpart in the reference (its MATLAB driver times with tic/toc). */
+int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushBytes, double *msPerLaunch);
+
+/* Number of levels / load cases / DOFs of level 0. */
+int top_solver_sizes(const top_solver *s, int64_t *out3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -320,7 +320,7 @@ class Model:
     def solve_state(self, U=None):
         n = self.m.L[0].numDOFs
         warm = U is not None
-        U = np.zeros((n, self.m.nLoads), order="F") if U is None else np.asfortranarray(U, dtype=np.float64).copy()
+        U = np.zeros((n, self.m.nLoads), order="F") if U is None else np.array(U, dtype=np.float64, order="F", copy=True)
         its = lib().orc_solve_state(self._m, _p(U), 1 if warm else 0)
         return U, its
 
@@ -368,7 +368,7 @@ def gather(u_nx3, eNod):
 
 
 def scatter(Y_nx3, eNod, uMat):
-    Y = np.asfortranarray(Y_nx3, dtype=np.float64).copy()
+    Y = np.array(Y_nx3, dtype=np.float64, order="F", copy=True)
     e = np.asfortranarray(eNod, dtype=np.int32)
     U = np.asfortranarray(uMat, dtype=np.float64)
     lib().orc_scatter(_p(Y), _p(e), _p(U), e.shape[0], Y.shape[0])
@@ -378,7 +378,7 @@ def scatter(Y_nx3, eNod, uMat):
 def scatter_accum3(keys, Tmp, xF):
     k = np.ascontiguousarray(keys, dtype=np.int32).ravel(order="F")
     T = np.asfortranarray(Tmp, dtype=np.float64)
-    X = np.asfortranarray(xF, dtype=np.float64).copy()
+    X = np.array(xF, dtype=np.float64, order="F", copy=True)
     lib().orc_scatter_accum3(_p(k), _p(T), T.shape[0], _p(X), X.shape[0])
     return X
 

@@ -594,6 +594,7 @@ int orc_apply_bc(OModel *m, int64_t nFix, const double *fixRows,
     for (int64_t i = 0; i < nFix; ++i) {
         fx[i].node = (int32_t)fixRows[4 * i];
         for (int c = 0; c < 3; ++c) fx[i].v[c] = fixRows[4 * i + 1 + c];
+        if (fx[i].node < 1 || fx[i].node > Nn) { free(fx); return -1; }   /* MATLAB: index error */
     }
     int64_t nf = nFix;
     BCRow **ld = xc(nLoads, sizeof(BCRow *));
@@ -603,6 +604,7 @@ int orc_apply_bc(OModel *m, int64_t nFix, const double *fixRows,
         for (int64_t i = 0; i < nLoadRows[ii]; ++i) {
             ld[ii][i].node = (int32_t)loadRows[ii][4 * i];
             for (int c = 0; c < 3; ++c) ld[ii][i].v[c] = loadRows[ii][4 * i + 1 + c];
+            if (ld[ii][i].node < 1 || ld[ii][i].node > Nn) { for (int j = 0; j <= ii; ++j) free(ld[j]); free(ld); free(nl); free(fx); return -1; }
         }
         nl[ii] = uniq_rows(ld[ii], nLoadRows[ii]);
         /* setdiff(fixed nodes, loaded nodes) (1513-1516) */

@@ -1,0 +1,178 @@
+"""Fused B200 solver vs the FP64 oracle: operators level by level, V-cycle, PCG."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def smooth_design(level0, resY, resX):
+    """Smooth density field in [0.1, 0.95] (optimisation-like, moderate contrast)."""
+    eb = level0.eleMapBack - 1
+    y, x, z = eb % resY, (eb // resY) % resX, eb // (resY * resX)
+    return 0.1 + 0.85 * (np.sin(x / 3.0) ** 2) * (np.cos(z / 4.0 + y / 5.0) ** 2)
+
+
+def _irregular(shape, seed, fill=0.7):
+    mk = np.random.default_rng(seed).random(shape) < fill
+    mk[:, 0, :] = True
+    mk[:, -1, :] = True
+    return mk
+
+
+MODELS = {
+    "cantilever_24x48x24": (np.ones((24, 48, 24), bool), 20000, 1),
+    "cantilever_24x48x24_smooth": (np.ones((24, 48, 24), bool), 20000, 1),
+    "cantilever_24x48x24_4lvl": (np.ones((24, 48, 24), bool), 50, 1),
+    "irregular_20x30x14": (_irregular((20, 30, 14), 0), 20000, 1),
+    "mbb_10x60x10": (np.ones((10, 60, 10), bool), 20000, 2),
+}
+
+
+@pytest.fixture(scope="module", params=list(MODELS))
+def pair(request):
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    mask, control, opt = MODELS[request.param]
+    o = O.Model(mask, control=control)
+    o.apply_optcase(opt)
+    o.set_material(1.0, 1e-9, 3.0)
+    o.set_solver(1e-6, 800, 0.6)
+    m = Mesh(mask, control=control)
+    m.apply_optcase(opt)
+    s = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6)
+    ne = o.level(0).numElements
+    x = 0.05 + 0.95 * np.random.default_rng(11).random(ne)
+    if request.param.endswith("_smooth"):
+        L0 = o.level(0)
+        x = smooth_design(L0, L0.resY, L0.resX)
+    o.set_density(x)
+    o.assemble()
+    s.set_density(torch.from_numpy(x).cuda())
+    s.assemble()
+    return o, s, m, ("smooth" if request.param.endswith("_smooth") else "random")
+
+
+def test_coarse_ks_match(pair):
+    o, s, _, _ = pair
+    for l in range(1, o.numLevels):
+        ref = o.level(l).Ks().ravel(order="F")
+        assert _rel(s.Ks(l), ref) < 1e-13, l
+
+
+def test_diagonals_match(pair):
+    o, s, _, _ = pair
+    for l in range(o.numLevels - 1):
+        assert _rel(s.diag(l), o.level(l).diagK()) < 1e-13, l
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_matvec_every_level(pair, fp32):
+    o, s, _, _ = pair
+    rng = np.random.default_rng(2)
+    for l in range(o.numLevels - 1):
+        u = rng.standard_normal(o.level(l).numDOFs)
+        ref = o.matvec(l, u)
+        y = s.matvec(l, torch.from_numpy(u).cuda(), fp32=fp32)
+        assert _rel(y, ref) < (2e-6 if fp32 else 1e-13), (l, fp32)
+
+
+def test_transfers(pair):
+    o, s, _, _ = pair
+    rng = np.random.default_rng(4)
+    for ii in range(1, o.numLevels):
+        rf = rng.standard_normal(o.level(ii - 1).numDOFs)
+        xc = rng.standard_normal(o.level(ii).numDOFs)
+        assert _rel(s.restrict(ii, torch.from_numpy(rf).cuda()), o.restrict(ii, rf)) < 1e-14
+        assert _rel(s.interpolate(ii, torch.from_numpy(xc).cuda()), o.interpolate(ii, xc)) < 1e-14
+
+
+def test_vcycle_fp64(pair):
+    o, s, _, _ = pair
+    r = np.random.default_rng(6).standard_normal(o.level(0).numDOFs)
+    assert _rel(s.vcycle(torch.from_numpy(r).cuda()), o.vcycle(r)) < 1e-11
+
+
+def _smooth_only(pair):
+    # i.i.d. random moduli (contrast 8000) make the reference's damped-Jacobi
+    # V-cycle (omega 0.6) indefinite; PCG parity runs on smooth designs
+    if pair[3] != "smooth":
+        pytest.skip("PCG parity on the smooth design")
+
+
+def test_pcg_fp64_matches_oracle(pair):
+    _smooth_only(pair)
+    o, s, _, _ = pair
+    b = o.F()[:, 0]
+    xo, its_o, res_o = o.pcg(b)
+    U, its, res = s.pcg(0)
+    assert abs(its - its_o) <= 1, (its, its_o)
+    assert res < 1e-6
+    # compliance F'U
+    c_o, c = b @ xo, float(torch.from_numpy(b).cuda() @ U)
+    assert abs(c - c_o) <= 1e-9 * abs(c_o)
+
+
+def test_pcg_warm_start_and_unit_compliance(pair):
+    _smooth_only(pair)
+    o, s, _, _ = pair
+    U1, its1, _ = s.pcg(0)
+    U2, its2, res2 = s.pcg(0, U=U1)
+    assert its2 <= 2 and res2 < 1e-6
+    ce = s.unit_compliance(U1)
+    ce_o = o.unit_compliance(U1.cpu().numpy()[:, None])
+    assert _rel(ce, ce_o) < 1e-12
+
+
+def test_mixed_precision_compliance_within_1e6():
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    mask = np.ones((24, 48, 24), bool)
+    o = O.Model(mask); o.apply_optcase(1); o.set_material(1.0, 1e-9, 3.0); o.set_solver(1e-12, 2000, 0.6)
+    m = Mesh(mask); m.apply_optcase(1)
+    s = Solver(m, E0=1.0, Emin=1e-9, tol=1e-6, maxIT=800, mixed=True)
+    L0 = o.level(0)
+    x = smooth_design(L0, L0.resY, L0.resX)
+    o.set_density(x); o.assemble()
+    s.set_density(torch.from_numpy(x).cuda()); s.assemble()
+    b = o.F()[:, 0]
+    xo, _, _ = o.pcg(b)
+    U, its, res = s.pcg(0)
+    assert res < 1e-6
+    c_o, c = b @ xo, float(torch.from_numpy(b).cuda() @ U)
+    assert abs(c - c_o) <= 1e-6 * abs(c_o)
+
+
+def test_maxit_status():
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    from top_gpu_on_matlab_b200 import TopGpuError
+    m = Mesh(np.ones((8, 16, 8), bool)); m.apply_optcase(1)
+    s = Solver(m, tol=1e-14, maxIT=3)
+    s.set_density(torch.full((m.info()[0]["numElements"],), 0.5, dtype=torch.float64, device="cuda"))
+    s.assemble()
+    U, its, res = s.pcg(0)
+    assert its == 3 and res > 1e-14
+    with pytest.raises(TopGpuError) as ei:
+        s.pcg(0, raise_on_maxit=True)
+    assert ei.value.status == -5
+
+
+def test_iid_densities_converge_with_smaller_omega():
+    # i.i.d. U[0.05,1] densities: omega 0.6 stalls (as in the oracle), 0.4 converges
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    mask = np.ones((8, 16, 8), bool)
+    o = O.Model(mask); o.apply_optcase(1); o.set_material(1.0, 1e-9, 3.0); o.set_solver(1e-6, 400, 0.4)
+    m = Mesh(mask); m.apply_optcase(1)
+    s = Solver(m, Emin=1e-9, tol=1e-6, maxIT=400, omega=0.4)
+    x = 0.05 + 0.95 * np.random.default_rng(11).random(mask.size)
+    o.set_density(x); o.assemble()
+    s.set_density(torch.from_numpy(x).cuda()); s.assemble()
+    b = o.F()[:, 0]
+    xo, its_o, _ = o.pcg(b)
+    U, its, res = s.pcg(0)
+    assert res < 1e-6 and abs(its - its_o) <= 1

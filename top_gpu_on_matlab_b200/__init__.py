@@ -1,0 +1,11 @@
+"""B200 (sm_100a) implementation of the TOP_GPU FEA hot path.
+
+Drop-in MEX entry points live in :mod:`top_gpu_on_matlab_b200.mex`, the
+voxel model and the fused GPU solver in :mod:`top_gpu_on_matlab_b200.fea`.
+All compute runs in libtopgpu.so; importing without it raises ImportError.
+"""
+from ._lib import TopGpuError, lib
+
+lib()   # the CUDA library is required: no CPU fallback
+
+__all__ = ["TopGpuError", "lib"]

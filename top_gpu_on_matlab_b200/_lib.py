@@ -1,0 +1,119 @@
+"""ctypes loader of libtopgpu.so (the package's CUDA library for sm_100a).
+
+The library is built in-tree by ``python -m top_gpu_on_matlab_b200.build``
+(or ``make -C top_gpu_on_matlab_b200/csrc``).  Importing this module without
+the built library raises ImportError: there is no CPU fallback.
+"""
+import ctypes as C
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libtopgpu.so"
+
+TOP_OK = 0
+TOP_ERR_ARGS = -1
+TOP_ERR_TYPE = -2
+TOP_ERR_SHAPE = -3
+TOP_ERR_CUDA = -4
+TOP_ERR_NOT_CONVERGED = -5
+TOP_ERR_NAN = -6
+TOP_ERR_NOMEM = -7
+TOP_ERR_STATE = -8
+TOP_F32 = 1
+TOP_F64 = 2
+TOP_PREC_FP64 = 0
+TOP_PREC_MIXED = 1
+
+_ERR_NAMES = {
+    TOP_ERR_ARGS: "Args", TOP_ERR_TYPE: "Type", TOP_ERR_SHAPE: "Shape", TOP_ERR_CUDA: "CUDA",
+    TOP_ERR_NOT_CONVERGED: "NotConverged", TOP_ERR_NAN: "NaN", TOP_ERR_NOMEM: "NoMem",
+    TOP_ERR_STATE: "State",
+}
+
+
+class TopGpuError(RuntimeError):
+    """Error raised for a non-zero status of libtopgpu.so.
+
+    ``identifier`` follows MATLAB's mexErrMsgIdAndTxt convention,
+    e.g. ``Gathering_inplace:Shape``.
+    """
+
+    def __init__(self, status, name, message):
+        self.status = status
+        self.identifier = "%s:%s" % (name, _ERR_NAMES.get(status, "Error"))
+        super().__init__("%s (%d): %s" % (self.identifier, status, message))
+
+
+class SolverParams(C.Structure):
+    _fields_ = [
+        ("E0", C.c_double), ("Emin", C.c_double), ("penal", C.c_double),
+        ("tol", C.c_double), ("maxIT", C.c_int), ("omega", C.c_double),
+        ("precision", C.c_int), ("outerFP32", C.c_int),
+    ]
+
+
+_vp, _i32p, _i64, _int, _dbl = C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_double
+
+SIGNATURES = {
+    "top_last_error": (C.c_char_p, []),
+    "top_version": (_int, []),
+    "top_gather": (_int, [_vp, _vp, _vp, _int, _i64, _i64, _int, _vp]),
+    "top_scatter": (_int, [_vp, _vp, _vp, _i64, _i64, _int, _vp]),
+    "top_scatter_accum3": (_int, [_vp, _vp, _i64, _vp, _i64, _int, _vp]),
+    "top_assemble_ks_level2": (_int, [_vp] * 8 + [_i64, _int, _i64, _i64, _int, _vp]),
+    "top_assemble_ks_higher": (_int, [_vp] * 4 + [_i64, _int, _i64, _int, _vp]),
+    "top_assemble_ks_level2_super": (_int, [_vp] * 8 + [_i64, _int, _i64, _i64, _int, _vp]),
+    "top_mesh_create": (_int, [_vp, _int, _int, _int, _int, _dbl, _dbl, _int, _vp]),
+    "top_mesh_destroy": (_int, [_vp]),
+    "top_mesh_apply_optcase": (_int, [_vp, _int]),
+    "top_mesh_apply_bc": (_int, [_vp, _i64, _vp, _int, _vp, _vp, _vp]),
+    "top_mesh_info": (_int, [_vp, _vp, _int]),
+    "top_mesh_get": (_int, [_vp, _int, C.c_char_p, _vp, _i64, _vp]),
+    "top_solver_create": (_int, [_vp, _vp, _vp]),
+    "top_solver_destroy": (_int, [_vp]),
+    "top_solver_set_stream": (_int, [_vp, _vp]),
+    "top_solver_set_modulus": (_int, [_vp, _vp, _int]),
+    "top_solver_set_density": (_int, [_vp, _vp, _int]),
+    "top_solver_assemble": (_int, [_vp]),
+    "top_solver_matvec": (_int, [_vp, _int, _vp, _vp, _int]),
+    "top_solver_vcycle": (_int, [_vp, _vp, _vp]),
+    "top_solver_restrict": (_int, [_vp, _int, _vp, _vp]),
+    "top_solver_interpolate": (_int, [_vp, _int, _vp, _vp]),
+    "top_solver_get_diag": (_int, [_vp, _int, _vp]),
+    "top_solver_get_ks": (_int, [_vp, _int, _vp]),
+    "top_solver_pcg": (_int, [_vp, _int, _vp, _int, _vp, _vp]),
+    "top_solver_pcg_rhs": (_int, [_vp, _vp, _vp, _int, _vp, _vp]),
+    "top_solver_unit_compliance": (_int, [_vp, _vp, _vp]),
+    "top_solver_sizes": (_int, [_vp, _vp]),
+    "top_solver_time_kernel": (_int, [_vp, _int, _int, _i64, _vp]),
+}
+
+_LIB = None
+
+
+def lib():
+    """Load libtopgpu.so (once) and declare its C ABI."""
+    global _LIB
+    if _LIB is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                "libtopgpu.so is not built (%s); run `make -C top_gpu_on_matlab_b200/csrc` "
+                "or __graft_entry__.build()" % LIB_PATH)
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def last_error() -> str:
+    msg = lib().top_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status, name):
+    if status != TOP_OK:
+        raise TopGpuError(status, name, last_error())
+    return status

@@ -1,0 +1,311 @@
+// topgpu_dropin.cu -- the six MEX kernels of TOP_GPU as C-ABI entry points
+// for sm_100a.  Same arguments, layouts and in-place semantics as the MEX
+// gateways (see include/topgpu.h for the file:line each one replaces).
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "topgpu_kernels.cuh"
+
+using namespace topgpu;
+
+namespace {
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// ---------------------------------------------------------------------------
+// gather: one thread per element; node ids held in registers; 24 coalesced
+// column stores (uMat is column-major [nElem x 24]).  An out-of-range node
+// id yields 0 instead of an out-of-bounds read.
+template <typename T, typename IDX>
+__global__ void gather_kernel(T *__restrict__ uMat, const T *__restrict__ u,
+                              const IDX *__restrict__ eNod, int64_t nElem, int64_t nNodes)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nElem) return;
+    int64_t node[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) node[n] = (int64_t)__ldg(&eNod[e + n * nElem]) - 1;
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        const bool ok = node[n] >= 0 && node[n] < nNodes;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            uMat[e + (int64_t)(3 * n + c) * nElem] = ok ? __ldg(&u[node[n] + c * nNodes]) : T(0);
+    }
+}
+
+// scatter: one thread per element; each of the 24 contributions is a single
+// fire-and-forget reduction into the L2-resident node array.
+template <typename T>
+__global__ void scatter_kernel(T *__restrict__ Y, const int32_t *__restrict__ eNod,
+                               const T *__restrict__ uMat, int64_t Ne, int64_t nNodes)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ne) return;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int64_t nid = (int64_t)__ldg(&eNod[e + j * Ne]) - 1;
+        if (nid < 0 || nid >= nNodes) continue;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(&Y[nid + c * nNodes], __ldg(&uMat[e + (int64_t)(c + 3 * j) * Ne]));
+    }
+}
+
+template <typename T>
+__global__ void scatter_accum3_kernel(const int32_t *__restrict__ keys, const T *__restrict__ Tmp,
+                                      int64_t N, T *__restrict__ xF, int64_t M)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int64_t key = (int64_t)__ldg(&keys[i]) - 1;
+    if (key < 0 || key >= M) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) atomicAdd(&xF[key + c * M], __ldg(&Tmp[i + c * N]));
+}
+
+// Q_s = P_s^T K0 P_s for every child slot (one CTA each): the child-
+// independent part of the level-2 Galerkin product.
+template <typename T>
+struct K0Child {
+    const T *K0;
+    __device__ T operator()(int32_t, int i) const { return K0[i]; }
+};
+struct NoSkip { __device__ bool operator()(int32_t) const { return false; } };
+
+// [n x n] identity child map: CTA e of ptkp_kernel then processes slot e only
+__global__ void eye_upmap_kernel(int32_t *up, int n)
+{ int i = blockIdx.x * blockDim.x + threadIdx.x; if (i < n * n) up[i] = (i % (n + 1) == 0) ? 1 : 0; }
+
+// A row of the level-2 GEMM: the moduli of a coarse cell's regular children
+// (0 for void children and for children with fixed DOFs).
+struct Level2Row {
+    const int32_t *upMap; const double *E; const int32_t *mapUnique; int64_t nElem; int nCh; int hasFixed;
+    __device__ double operator()(int64_t m, int k) const {
+        if (k >= nCh) return 0.0;
+        const int32_t f1 = upMap[m + (int64_t)k * nElem];
+        if (f1 <= 0) return 0.0;
+        if (hasFixed && mapUnique[f1 - 1] > 0) return 0.0;
+        return E[f1 - 1];
+    }
+};
+
+template <typename T>
+struct Level2Child {   // K_child of assembleKs_level2_inplace.cu:104-115
+    const T *E; const T *K0; const int32_t *mapUnique; const T *uFree; const T *uFixed; int hasFixed;
+    __device__ T operator()(int32_t f0, int i) const {
+        const T mod = E[f0];
+        const int32_t uid0 = hasFixed ? mapUnique[f0] - 1 : -1;
+        if (uid0 >= 0) return uFree[(size_t)uid0 * 576 + i] * mod + uFixed[(size_t)uid0 * 576 + i];
+        return K0[i] * mod;
+    }
+};
+struct RegularChild {  // skip children with fixed DOFs (handled by the GEMM otherwise)
+    const int32_t *mapUnique; int hasFixed; int invert;
+    __device__ bool operator()(int32_t f0) const {
+        const bool bnd = hasFixed && mapUnique[f0] > 0;
+        return invert ? !bnd : bnd;
+    }
+};
+template <typename T>
+struct PrevChild {
+    const T *KsPrev;
+    __device__ T operator()(int32_t f0, int i) const { return KsPrev[(size_t)f0 * 576 + i]; }
+};
+template <typename T>
+struct SuperChild {   // assembleKs_level2_superEle_inplace.cu:113-140
+    const T *Ks0; const int32_t *mapUnique; const T *E; const T *uFree; const T *uFixed; int hasFixed;
+    __device__ T operator()(int32_t f0, int i) const {
+        const int32_t uid1 = hasFixed ? mapUnique[f0] : 0;
+        if (uid1 > 0) {
+            const size_t fb = (size_t)(uid1 - 1) * 576 * 64, mb = (size_t)f0 * 64;
+            T acc = T(0);
+            for (int q = 0; q < 64; ++q) acc += uFree[fb + (size_t)q * 576 + i] * E[mb + q];
+            return acc + uFixed[(size_t)(uid1 - 1) * 576 + i];
+        }
+        return Ks0[(size_t)f0 * 576 + i];
+    }
+};
+
+inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+extern "C" int top_gather(void *uMat, const void *u, const void *eNod, int eNodIsU32,
+                          int64_t nElem, int64_t nNodes, int dtype, void *stream)
+{
+    if (nElem < 0 || nNodes < 0) { set_error("Gathering_inplace:Shape negative size"); return TOP_ERR_SHAPE; }
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("Gathering_inplace:Type gU must be single or double."); return TOP_ERR_TYPE; }
+    if (nElem == 0) return TOP_OK;
+    if (!uMat || !u || !eNod) { set_error("Gathering_inplace:Args null pointer"); return TOP_ERR_ARGS; }
+    const int T = 256, G = blocks_for(nElem, T);
+    if (dtype == TOP_F64) {
+        if (eNodIsU32) gather_kernel<double, uint32_t><<<G, T, 0, S(stream)>>>((double *)uMat, (const double *)u, (const uint32_t *)eNod, nElem, nNodes);
+        else gather_kernel<double, int32_t><<<G, T, 0, S(stream)>>>((double *)uMat, (const double *)u, (const int32_t *)eNod, nElem, nNodes);
+    } else {
+        if (eNodIsU32) gather_kernel<float, uint32_t><<<G, T, 0, S(stream)>>>((float *)uMat, (const float *)u, (const uint32_t *)eNod, nElem, nNodes);
+        else gather_kernel<float, int32_t><<<G, T, 0, S(stream)>>>((float *)uMat, (const float *)u, (const int32_t *)eNod, nElem, nNodes);
+    }
+    TOP_CUDA_CHECK(cudaGetLastError(), "Gathering_inplace");
+    return TOP_OK;
+}
+
+extern "C" int top_scatter(void *Y, const int32_t *eNod, const void *uMat,
+                           int64_t nElem, int64_t nNodes, int dtype, void *stream)
+{
+    if (nElem < 0 || nNodes < 0) { set_error("Scattering_inplace:shape negative size"); return TOP_ERR_SHAPE; }
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("Scattering_inplace:type unsupported class"); return TOP_ERR_TYPE; }
+    if (nElem > 0) {
+        if (!Y || !eNod || !uMat) { set_error("Scattering_inplace:arity null pointer"); return TOP_ERR_ARGS; }
+        const int T = 256, G = blocks_for(nElem, T);
+        if (dtype == TOP_F64) scatter_kernel<double><<<G, T, 0, S(stream)>>>((double *)Y, eNod, (const double *)uMat, nElem, nNodes);
+        else scatter_kernel<float><<<G, T, 0, S(stream)>>>((float *)Y, eNod, (const float *)uMat, nElem, nNodes);
+        TOP_CUDA_CHECK(cudaGetLastError(), "Scattering_inplace");
+    }
+    TOP_CUDA_CHECK(cudaStreamSynchronize(S(stream)), "Scattering_inplace");
+    return TOP_OK;
+}
+
+extern "C" int top_scatter_accum3(const int32_t *keys, const void *Tmp, int64_t N,
+                                  void *xF, int64_t M, int dtype, void *stream)
+{
+    if (N < 0 || M < 0) { set_error("scatter_accum3:shape negative size"); return TOP_ERR_SHAPE; }
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("scatter_accum3:type Only single or double supported for `Tmp`/`xFiner`."); return TOP_ERR_TYPE; }
+    if (N == 0) return TOP_OK;
+    if (!keys || !Tmp || !xF) { set_error("scatter_accum3:gpu All inputs must be gpuArray."); return TOP_ERR_ARGS; }
+    const int T = 256, G = blocks_for(N, T);
+    if (dtype == TOP_F64) scatter_accum3_kernel<double><<<G, T, 0, S(stream)>>>(keys, (const double *)Tmp, N, (double *)xF, M);
+    else scatter_accum3_kernel<float><<<G, T, 0, S(stream)>>>(keys, (const float *)Tmp, N, (float *)xF, M);
+    TOP_CUDA_CHECK(cudaGetLastError(), "scatter_accum3");
+    return TOP_OK;
+}
+
+namespace topgpu {
+// Level-2 Galerkin assembly in the form Ks = (moduli of regular children) x Q
+// on the FP64 tensor cores, plus the full triple product for children with
+// fixed DOFs.  Shared with the fused solver.  Qscratch: [64 x 576] doubles,
+// zero-filled by the caller; eyeScratch: [nCh x nCh] int32.
+int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
+                        const double *Pch, const int32_t *mapUnique, const double *uFree,
+                        const double *uFixed, int64_t nElem, int nCh, int64_t nUnique,
+                        double *Qscratch, int32_t *eyeScratch, cudaStream_t st)
+{
+    const int hasFixed = (nUnique > 0 && mapUnique && uFree && uFixed) ? 1 : 0;
+    // Q_s = P_s^T K0 P_s, one CTA per child slot
+    if (nCh > 0) {
+        eye_upmap_kernel<<<(nCh * nCh + 255) / 256, 256, 0, st>>>(eyeScratch, nCh);
+        ptkp_kernel<double><<<nCh, kPtkpThreads, 0, st>>>(Qscratch, eyeScratch, nCh, nCh, Pch,
+                                                          K0Child<double>{K0}, NoSkip{}, 0);
+    }
+    if (nElem == 0) return TOP_OK;
+    if (nCh <= kGemmK) {
+        cudaFuncSetAttribute(dgemm_k64_kernel<Level2Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+        dim3 grid((unsigned)((nElem + kGemmBM - 1) / kGemmBM), (576 + kGemmBN - 1) / kGemmBN);
+        // rows of B beyond nCh are never read (ARow returns 0 there) but must
+        // exist: Qscratch is sized for 64 slots
+        dgemm_k64_kernel<<<grid, 128, kGemmSmem, st>>>(Ks, nElem, 576, 576, Qscratch, 576,
+                                                       Level2Row{upMap, E, mapUnique, nElem, nCh, hasFixed});
+        if (hasFixed)
+            ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+                Ks, upMap, nElem, nCh, Pch,
+                Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed},
+                RegularChild{mapUnique, hasFixed, 1}, 1);
+    } else {
+        ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+            Ks, upMap, nElem, nCh, Pch, Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed}, NoSkip{}, 0);
+    }
+    return cudaGetLastError() == cudaSuccess ? TOP_OK : TOP_ERR_CUDA;
+}
+
+int assemble_higher_f64(double *Ks, const int32_t *upMap, const double *KsPrev, const double *Psub,
+                        int64_t nElem, int nSub, cudaStream_t st)
+{
+    if (nElem == 0) return TOP_OK;
+    ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(Ks, upMap, nElem, nSub, Psub,
+                                                                  PrevChild<double>{KsPrev}, NoSkip{}, 0);
+    return cudaGetLastError() == cudaSuccess ? TOP_OK : TOP_ERR_CUDA;
+}
+}  // namespace topgpu
+
+extern "C" int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void *eleModulus,
+                                      const void *K0, const void *Pch, const int32_t *mapUnique,
+                                      const void *uniqueFree, const void *uniqueFixed,
+                                      int64_t nElem, int nCh, int64_t nFine, int64_t nUnique,
+                                      int dtype, void *stream)
+{
+    const char *N = "assembleKs_level2_inplace";
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("%s:Type d_Ks must be single/double gpuArray.", N); return TOP_ERR_TYPE; }
+    if (nElem < 0 || nCh < 0 || nFine < 0 || nUnique < 0) { set_error("%s:Shape negative size", N); return TOP_ERR_SHAPE; }
+    if (nElem == 0) return TOP_OK;
+    if (!Ks || !upMap || !eleModulus || !K0 || !Pch) { set_error("%s:Input null pointer", N); return TOP_ERR_ARGS; }
+    const int hasFixed = (nUnique > 0 && mapUnique && uniqueFree && uniqueFixed) ? 1 : 0;
+    cudaStream_t st = S(stream);
+    if (dtype == TOP_F64) {
+        double *Q = nullptr; int32_t *one = nullptr;
+        const size_t qn = (size_t)576 * (nCh > 64 ? nCh : 64);
+        TOP_CUDA_CHECK(cudaMallocAsync(&Q, sizeof(double) * qn, st), N);
+        TOP_CUDA_CHECK(cudaMemsetAsync(Q, 0, sizeof(double) * qn, st), N);
+        TOP_CUDA_CHECK(cudaMallocAsync(&one, sizeof(int32_t) * (size_t)nCh * nCh + 4, st), N);
+        int rc = assemble_level2_f64((double *)Ks, upMap, (const double *)eleModulus, (const double *)K0,
+                                     (const double *)Pch, mapUnique, (const double *)uniqueFree,
+                                     (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, Q, one, st);
+        cudaFreeAsync(Q, st); cudaFreeAsync(one, st);
+        if (rc) { set_error("%s:CUDA launch failed: %s", N, cudaGetErrorString(cudaGetLastError())); return rc; }
+    } else {
+        ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+            (float *)Ks, upMap, nElem, nCh, (const float *)Pch,
+            Level2Child<float>{(const float *)eleModulus, (const float *)K0, mapUnique,
+                               (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed},
+            NoSkip{}, 0);
+    }
+    TOP_CUDA_CHECK(cudaGetLastError(), N);
+    TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // assembleKs_level2_inplace.cu:272
+    return TOP_OK;
+}
+
+extern "C" int top_assemble_ks_higher(void *Ks, const int32_t *upMap, const void *KsPrev,
+                                      const void *Psub, int64_t nElem, int nSub, int64_t nFine,
+                                      int dtype, void *stream)
+{
+    const char *N = "assembleKs_higherLevel_inplace";
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("%s:Type d_Ks must be single/double gpuArray.", N); return TOP_ERR_TYPE; }
+    if (nElem < 0 || nSub < 0 || nFine < 0) { set_error("%s:Shape negative size", N); return TOP_ERR_SHAPE; }
+    if (nElem == 0) return TOP_OK;
+    if (!Ks || !upMap || !KsPrev || !Psub) { set_error("%s:Input null pointer", N); return TOP_ERR_ARGS; }
+    cudaStream_t st = S(stream);
+    if (dtype == TOP_F64)
+        ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>((double *)Ks, upMap, nElem, nSub, (const double *)Psub,
+                                                                      PrevChild<double>{(const double *)KsPrev}, NoSkip{}, 0);
+    else
+        ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>((float *)Ks, upMap, nElem, nSub, (const float *)Psub,
+                                                                     PrevChild<float>{(const float *)KsPrev}, NoSkip{}, 0);
+    TOP_CUDA_CHECK(cudaGetLastError(), N);
+    TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // assembleKs_higherLevel_inplace.cu:209
+    return TOP_OK;
+}
+
+extern "C" int top_assemble_ks_level2_super(void *Ks, const int32_t *upMap, const void *Ks0,
+                                            const void *Psub, const int32_t *mapUnique,
+                                            const void *eleModulus, const void *uniqueFree,
+                                            const void *uniqueFixed, int64_t nElem, int nSub,
+                                            int64_t nFine, int64_t nUnique, int dtype, void *stream)
+{
+    const char *N = "assembleKs_level2_superEle_inplace";
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("%s:Type d_Ks must be single/double gpuArray.", N); return TOP_ERR_TYPE; }
+    if (nElem < 0 || nSub < 0 || nFine < 0 || nUnique < 0) { set_error("%s:Shape negative size", N); return TOP_ERR_SHAPE; }
+    if (nElem == 0) return TOP_OK;
+    if (!Ks || !upMap || !Ks0 || !Psub || !eleModulus) { set_error("%s:Input null pointer", N); return TOP_ERR_ARGS; }
+    const int hasFixed = (nUnique > 0 && mapUnique && uniqueFree && uniqueFixed) ? 1 : 0;
+    cudaStream_t st = S(stream);
+    if (dtype == TOP_F64)
+        ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+            (double *)Ks, upMap, nElem, nSub, (const double *)Psub,
+            SuperChild<double>{(const double *)Ks0, mapUnique, (const double *)eleModulus,
+                               (const double *)uniqueFree, (const double *)uniqueFixed, hasFixed}, NoSkip{}, 0);
+    else
+        ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+            (float *)Ks, upMap, nElem, nSub, (const float *)Psub,
+            SuperChild<float>{(const float *)Ks0, mapUnique, (const float *)eleModulus,
+                              (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed}, NoSkip{}, 0);
+    TOP_CUDA_CHECK(cudaGetLastError(), N);
+    TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // ..._superEle_inplace.cu:313
+    return TOP_OK;
+}

@@ -1,0 +1,342 @@
+// topgpu_grid.cuh -- structured-grid device kernels of the fused solver.
+//
+// Layout of every level: node (Y, X, Z) of the (ny+1) x (nx+1) x (nz+1) node
+// grid lives at  idx = Y + PY*(X+1) + PLANE*(Z+1)  of a zero-guarded array
+// (PY >= NY+1, PX = NX+2, PZ = NZ+2, PLANE = PY*PX), one such array per
+// displacement component (component stride CS).  Element (ey, ex, ez) is
+// stored at the slot of its base node (ey, ex, ez).  All guard slots hold
+// zeros, so every stencil access is in bounds and void / outside elements
+// contribute nothing.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "topgpu_internal.h"
+
+namespace topgpu {
+
+constexpr int64_t kMargin = 64;        // elements of zero padding before/after each array
+constexpr int kNodeThreads = 256;
+constexpr uint8_t kActive = 8;         // flag bit: node belongs to an active element
+constexpr uint8_t kFixedMask = 7;      // flag bits 0..2: component fixed (level 0)
+
+struct Geom {
+    int NY, NX, NZ;       // node counts
+    int PY;               // y pitch
+    int nbx;              // node-kernel blocks per z plane
+    int64_t plane;        // PY * PX
+    int64_t cs;           // component stride
+    int64_t origin;       // index of node (0,0,0)
+};
+
+// corner j of an element with offsets (dy, dx, dz) in {0,1}
+__host__ __device__ constexpr int corner_of(int dy, int dx, int dz)
+{
+    return 4 * dz + (dy ? (dx ? 1 : 0) : (dx ? 2 : 3));
+}
+__host__ __device__ constexpr int cdy(int j) { return (j & 3) < 2 ? 1 : 0; }
+__host__ __device__ constexpr int cdx(int j) { return ((j & 3) == 1 || (j & 3) == 2) ? 1 : 0; }
+__host__ __device__ constexpr int cdz(int j) { return j >> 2; }
+// packed upper triangle of a symmetric 24x24 matrix (300 entries)
+__host__ __device__ constexpr int sym_pack(int r, int k)
+{
+    return r <= k ? r * 24 - r * (r - 1) / 2 + (k - r) : k * 24 - k * (k - 1) / 2 + (r - k);
+}
+
+template <typename T> struct KeParam { T k[576]; };
+
+// ---------------------------------------------------------------------------
+// Deterministic grid-wide sum: per-block partials, the last block to finish
+// adds them in index order and writes *result.
+template <int NT>
+__device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result)
+{
+    __shared__ double red[NT / 32];
+    __shared__ bool last;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int i = 0; i < NT / 32; ++i) s += red[i];
+        partials[bid] = s;
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double s = 0;
+    for (unsigned i = threadIdx.x; i < nb; i += NT) s += ((volatile double *)partials)[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) red[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int i = 0; i < NT / 32; ++i) t += red[i];
+        *result = t;
+        *counter = 0;
+    }
+}
+
+struct Reduce {             // where a fused dot product goes
+    double *partials; unsigned *counter; double *result;
+};
+
+// ---------------------------------------------------------------------------
+// Inputs of the node kernels: the value of the operand vector at a node.
+template <typename T, typename TV>
+struct VecIn {
+    const TV *u; int64_t cs;
+    __device__ __forceinline__ T operator()(int64_t m, int c) const { return T(u[c * cs + m]); }
+};
+// x = omega * invD .* r  (the Jacobi pre-smoothing step, evaluated on the fly)
+template <typename T, typename TR>
+struct JacobiIn {
+    const TR *r; const T *invD; int64_t cs; T omega;
+    __device__ __forceinline__ T operator()(int64_t m, int c) const { return omega * invD[c * cs + m] * T(r[c * cs + m]); }
+};
+
+// Epilogues: what a node kernel does with y = (K u)(node).
+template <typename T, typename TY>
+struct StoreOut {   // y
+    TY *y; int64_t cs;
+    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
+    { for (int c = 0; c < 3; ++c) y[c * cs + i] = TY(yv[c]); (void)dot; }
+};
+template <typename T, typename TU, typename TY>
+struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
+    TY *y; const TU *u; int64_t cs;
+    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
+    { for (int c = 0; c < 3; ++c) { y[c * cs + i] = TY(yv[c]); dot += double(u[c * cs + i]) * double(yv[c]); } }
+};
+template <typename T, typename TR, typename TD>
+struct ResidOut {   // d = r - y
+    const TR *r; TD *d; int64_t cs;
+    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
+    { for (int c = 0; c < 3; ++c) d[c * cs + i] = TD(T(r[c * cs + i]) - yv[c]); (void)dot; }
+};
+// z = x + omega*invD.*(r - y), optionally dot += z . r  (post-smoothing)
+template <typename T, typename TR, typename TZ>
+struct PostSmoothOut {
+    const T *x; const TR *r; const T *invD; TZ *z; int64_t cs; T omega;
+    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
+    {
+        for (int c = 0; c < 3; ++c) {
+            const int64_t k = c * cs + i;
+            const T zv = x[k] + omega * invD[k] * (T(r[k]) - yv[c]);
+            z[k] = TZ(zv);
+            dot += double(zv) * double(r[k]);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Level 0: y(node) = sum over the 8 incident elements of E_e * Ke(rows of the
+// node) * u_e.  Fixed components: the element matrices have those rows and
+// columns removed and E0/nAdj on the diagonal (TOP_GPU.m:1729-1741), which
+// summed over the node's elements is y = E0*u for a fixed row and u = 0 in
+// every free row -- applied by MASK blocks, the ones whose stencil reaches
+// a fixed node.  Ke comes in as a launch parameter (constant bank).
+template <typename T, bool MASK, class In, class Out>
+__device__ __forceinline__ void l0_node(const KeParam<T> &K, const In &in, const Out &out,
+                                        const T *__restrict__ E, const uint8_t *__restrict__ flags,
+                                        const Geom &g, int64_t idx, bool valid, T E0, double &dot)
+{
+    if (!valid) return;
+    T Ee[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) Ee[i] = E[idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i)];
+    T t[8][3];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i][0] = t[i][1] = t[i][2] = T(0);
+#pragma unroll
+    for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int64_t m = idx + dy + g.PY * dx + g.plane * dz;
+                T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
+                if (MASK) {
+                    const uint8_t fm = flags[m];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) if (fm & (1 << c)) u[c] = T(0);
+                }
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int jy = cdy(i) + dy, jx = cdx(i) + dx, jz = cdz(i) + dz;
+                    if (jy < 0 || jy > 1 || jx < 0 || jx > 1 || jz < 0 || jz > 1) continue;
+                    const int j = corner_of(jy, jx, jz);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) t[i][c] = fma(K.k[(3 * i + c) + 24 * (3 * j + d)], u[d], t[i][c]);
+                }
+            }
+    T y[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        T s = T(0);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s = fma(Ee[i], t[i][c], s);
+        y[c] = s;
+    }
+    if (MASK) {
+        const uint8_t f = flags[idx];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) if (f & (1 << c)) y[c] = E0 * in(idx, c);
+    }
+    out(idx, y, dot);
+}
+
+template <typename T, class In, class Out>
+__global__ void __launch_bounds__(kNodeThreads)
+l0_kernel(const KeParam<T> K, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+          const uint8_t *__restrict__ tileFixed, Geom g, T E0, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    const bool valid = Y < g.NY && X < g.NX;
+    const int64_t idx = g.origin + Y + (int64_t)g.PY * X + g.plane * Z;
+    double dot = 0.0;
+    if (tileFixed[blockIdx.x + (int64_t)g.nbx * Z])
+        l0_node<T, true>(K, in, out, E, flags, g, idx, valid, E0, dot);
+    else
+        l0_node<T, false>(K, in, out, E, flags, g, idx, valid, E0, dot);
+    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
+}
+
+// ---------------------------------------------------------------------------
+// Coarse levels: y(node) = sum over incident elements of the node's three
+// rows of the element's Galerkin matrix Ks (packed upper triangle, entry
+// stride CS) times u_e.
+template <typename T, class In, class Out>
+__global__ void __launch_bounds__(kNodeThreads)
+coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    const bool valid = Y < g.NY && X < g.NX;
+    const int64_t idx = g.origin + Y + (int64_t)g.PY * X + g.plane * Z;
+    double dot = 0.0;
+    if (valid) {
+        T y[3] = {T(0), T(0), T(0)};
+#pragma unroll
+        for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+            for (int dx = -1; dx <= 1; ++dx)
+#pragma unroll
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int64_t m = idx + dy + g.PY * dx + g.plane * dz;
+                    const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) {
+                        const int jy = cdy(i) + dy, jx = cdx(i) + dx, jz = cdz(i) + dz;
+                        if (jy < 0 || jy > 1 || jx < 0 || jx > 1 || jz < 0 || jz > 1) continue;
+                        const int j = corner_of(jy, jx, jz);
+                        const T *ke = Ks + (idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i));
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+#pragma unroll
+                            for (int d = 0; d < 3; ++d)
+                                y[c] = fma(__ldg(ke + g.cs * sym_pack(3 * i + c, 3 * j + d)), u[d], y[c]);
+                    }
+                }
+        out(idx, y, dot);
+    }
+    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
+}
+
+// ---------------------------------------------------------------------------
+// Transfers between level l (fine) and l+1 (coarse), span S.  Prolongation
+// is trilinear interpolation of the coarse field at the fine active nodes;
+// restriction is its transpose.  (TOP_GPU.m:817-878 express the same
+// operators through an intermediate node set with multiplicity weights; for
+// every active node the two coincide.)
+template <typename T, int S>
+__global__ void __launch_bounds__(kNodeThreads)
+restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
+                const uint8_t *__restrict__ flagsC, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int QY = q % gc.PY, QX = q / gc.PY, QZ = blockIdx.y;
+    if (QY >= gc.NY || QX >= gc.NX) return;
+    const int64_t ic = gc.origin + QY + (int64_t)gc.PY * QX + gc.plane * QZ;
+    T acc[3] = {T(0), T(0), T(0)};
+    if (flagsC[ic] & kActive) {
+        for (int oz = -(S - 1); oz <= S - 1; ++oz) {
+            const int Z = S * QZ + oz;
+            if (Z < 0 || Z >= gf.NZ) continue;
+            const T wz = T(S - (oz < 0 ? -oz : oz)) / T(S);
+            for (int ox = -(S - 1); ox <= S - 1; ++ox) {
+                const int X = S * QX + ox;
+                if (X < 0 || X >= gf.NX) continue;
+                const T wzx = wz * (T(S - (ox < 0 ? -ox : ox)) / T(S));
+                const int64_t base = gf.origin + (int64_t)gf.PY * X + gf.plane * Z;
+#pragma unroll
+                for (int oy = -(S - 1); oy <= S - 1; ++oy) {
+                    const int Y = S * QY + oy;
+                    if (Y < 0 || Y >= gf.NY) continue;
+                    const T w = wzx * (T(S - (oy < 0 ? -oy : oy)) / T(S));
+                    const int64_t f = base + Y;
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) acc[c] = fma(w, rf[c * gf.cs + f], acc[c]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
+}
+
+// x_f = base + P x_c, base = omega*invD.*r when r != nullptr (the pre-smoothed
+// iterate of the V-cycle, recomputed instead of stored), 0 otherwise.
+template <typename T, int S, typename TR>
+__global__ void __launch_bounds__(kNodeThreads)
+prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
+               const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
+               const T *__restrict__ invD, T omega, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % gf.PY, X = q / gf.PY, Z = blockIdx.y;
+    if (Y >= gf.NY || X >= gf.NX) return;
+    const int64_t i = gf.origin + Y + (int64_t)gf.PY * X + gf.plane * Z;
+    T v[3] = {T(0), T(0), T(0)};
+    if (flagsF[i] & kActive) {
+        const int qy = Y / S, ry = Y - qy * S, qx = X / S, rx = X - qx * S, qz = Z / S, rz = Z - qz * S;
+        const T wy[2] = {T(S - ry) / T(S), T(ry) / T(S)};
+        const T wx[2] = {T(S - rx) / T(S), T(rx) / T(S)};
+        const T wz[2] = {T(S - rz) / T(S), T(rz) / T(S)};
+#pragma unroll
+        for (int bz = 0; bz < 2; ++bz) {
+            if (bz && rz == 0) continue;
+#pragma unroll
+            for (int bx = 0; bx < 2; ++bx) {
+                if (bx && rx == 0) continue;
+#pragma unroll
+                for (int by = 0; by < 2; ++by) {
+                    if (by && ry == 0) continue;
+                    const T w = wz[bz] * wx[bx] * wy[by];
+                    const int64_t k = gc.origin + (qy + by) + (int64_t)gc.PY * (qx + bx) + gc.plane * (qz + bz);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) v[c] = fma(w, xc[c * gc.cs + k], v[c]);
+                }
+            }
+        }
+        if (r) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] += omega * invD[c * gf.cs + i] * T(r[c * gf.cs + i]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
+}
+
+}  // namespace topgpu

@@ -1,0 +1,1014 @@
+// topgpu_solver.cu -- fused device solver of libtopgpu.so (sm_100a).
+//
+// Replaces, for one voxel model resident in HBM, the reference's
+// Solving_PCG / Solving_Vcycle / Solving_KbyU_MatrixFree /
+// Solving_RestrictResidual / Solving_InterpolationDeviation /
+// Solving_AssembleFEAstencil (TOP_GPU.m:602-878, 1033-1267).
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+#include "topgpu_grid.cuh"
+#include "topgpu_kernels.cuh"
+
+namespace topgpu {
+int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
+                        const double *Pch, const int32_t *mapUnique, const double *uFree,
+                        const double *uFixed, int64_t nElem, int nCh, int64_t nUnique,
+                        double *Qscratch, int32_t *eyeScratch, cudaStream_t st);
+int assemble_higher_f64(double *Ks, const int32_t *upMap, const double *KsPrev, const double *Psub,
+                        int64_t nElem, int nSub, cudaStream_t st);
+
+struct PcgState {
+    double normB, rho, rhoOld, pv, rr, resnorm, tol;
+    int its, maxIT, done, status;
+};
+
+// ---------------------------------------------------------------------------
+// small kernels
+template <typename TI, typename TO>
+__global__ void compact_to_grid_kernel(const TI *__restrict__ v, TO *__restrict__ g,
+                                       const int32_t *__restrict__ nodeGrid, int64_t Nn, int64_t cs)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Nn) return;
+    const int64_t gi = nodeGrid[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c * cs + gi] = TO(v[3 * n + c]);
+}
+template <typename TI, typename TO>
+__global__ void grid_to_compact_kernel(const TI *__restrict__ g, TO *__restrict__ v,
+                                       const int32_t *__restrict__ nodeGrid, int64_t Nn, int64_t cs)
+{
+    const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Nn) return;
+    const int64_t gi = nodeGrid[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[3 * n + c] = TO(g[c * cs + gi]);
+}
+// E (compact, FP64) -> grid slots (FP64 + FP32); SIMP when x != nullptr
+__global__ void modulus_kernel(const double *__restrict__ src, int simp, double E0, double Emin, double p,
+                               double *__restrict__ Ec, double *__restrict__ Eg, float *__restrict__ Eg32,
+                               const int32_t *__restrict__ eleGrid, int64_t Ne)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ne) return;
+    const double v = simp ? Emin + pow(src[e], p) * (E0 - Emin) : src[e];
+    Ec[e] = v;
+    Eg[eleGrid[e]] = v;
+    Eg32[eleGrid[e]] = float(v);
+}
+// Level-0 Jacobi diagonal: sum_e E_e diag(Ke) on free components, E0 on
+// fixed ones (the element matrices of TOP_GPU.m:1184-1188 summed per node).
+__global__ void diag_l0_kernel(const KeParam<double> K, const double *__restrict__ E,
+                               const uint8_t *__restrict__ flags, Geom g, double E0,
+                               double *__restrict__ diag, double *__restrict__ inv64, float *__restrict__ inv32)
+{
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    if (Y >= g.NY || X >= g.NX) return;
+    const int64_t idx = g.origin + Y + (int64_t)g.PY * X + g.plane * Z;
+    const uint8_t f = flags[idx];
+    for (int c = 0; c < 3; ++c) {
+        double d = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d += E[idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i)] * K.k[(3 * i + c) * 25];
+        if (f & (1 << c)) d = E0;
+        const bool on = (f & kActive) && d != 0.0;
+        diag[c * g.cs + idx] = d;
+        inv64[c * g.cs + idx] = on ? 1.0 / d : 0.0;
+        inv32[c * g.cs + idx] = on ? float(1.0 / d) : 0.0f;
+    }
+}
+// Compact element Ks [576 x Ne] -> packed grid slots (FP64 + FP32)
+__global__ void pack_ks_kernel(const double *__restrict__ KsC, const int32_t *__restrict__ eleGrid, int64_t Ne,
+                               double *__restrict__ P64, float *__restrict__ P32, int64_t cs)
+{
+    const int64_t e = blockIdx.x;
+    const int64_t slot = eleGrid[e];
+    for (int r = threadIdx.x; r < 24; r += blockDim.x)
+        for (int k = r; k < 24; ++k) {
+            const double v = KsC[e * 576 + r + 24 * k];
+            const int p = sym_pack(r, k);
+            if (P64) P64[p * cs + slot] = v;
+            if (P32) P32[p * cs + slot] = float(v);
+        }
+}
+__global__ void diag_coarse_kernel(const double *__restrict__ P64, Geom g, const uint8_t *__restrict__ flags,
+                                   double *__restrict__ diag, double *__restrict__ inv64, float *__restrict__ inv32)
+{
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    if (Y >= g.NY || X >= g.NX) return;
+    const int64_t idx = g.origin + Y + (int64_t)g.PY * X + g.plane * Z;
+    for (int c = 0; c < 3; ++c) {
+        double d = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d += P64[g.cs * sym_pack(3 * i + c, 3 * i + c) + idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i)];
+        const bool on = (flags[idx] & kActive) && d != 0.0;
+        diag[c * g.cs + idx] = d;
+        inv64[c * g.cs + idx] = on ? 1.0 / d : 0.0;
+        inv32[c * g.cs + idx] = on ? float(1.0 / d) : 0.0f;
+    }
+}
+// Dense coarsest matrix, one thread per row (compact node n, component c):
+// each thread owns its row, so the sums are race-free and deterministic.
+__global__ void coarsest_assemble_kernel(const double *__restrict__ KsC, const int32_t *__restrict__ nodeGrid,
+                                         const int32_t *__restrict__ eleCompact, const int32_t *__restrict__ nodeCompact,
+                                         Geom g, int64_t Nn, double *__restrict__ A)
+{
+    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= 3 * Nn) return;
+    const int64_t n = row / 3; const int c = int(row % 3);
+    const int64_t nC = 3 * Nn;
+    const int64_t idx = nodeGrid[n];
+    for (int i = 0; i < 8; ++i) {
+        const int64_t slot = idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i);
+        const int32_t e = eleCompact[slot];
+        if (e < 0) continue;
+        for (int j = 0; j < 8; ++j) {
+            const int32_t m = nodeCompact[slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j)];
+            for (int d = 0; d < 3; ++d) A[row + nC * (3 * (int64_t)m + d)] += KsC[(int64_t)e * 576 + (3 * i + c) + 24 * (3 * j + d)];
+        }
+    }
+}
+// ---- dense FP64 Cholesky (lower, col-major, in place), blocked 32 ----
+constexpr int kCb = 32;
+__global__ void chol_diag_kernel(double *A, int64_t n, int64_t k0, int kb, int *status)
+{
+    __shared__ double s[kCb][kCb + 1];
+    const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 32
+    if (tx < kb && ty < kb) s[ty][tx] = A[(k0 + ty) + n * (k0 + tx)];
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        if (tx == 0 && ty == 0) {
+            const double d = s[j][j];
+            if (!(d > 0.0)) { *status = 1; s[j][j] = 1.0; } else s[j][j] = sqrt(d);
+        }
+        __syncthreads();
+        if (tx == 0 && ty > j && ty < kb) s[ty][j] /= s[j][j];
+        __syncthreads();
+        if (ty > j && tx > j && tx <= ty && ty < kb) s[ty][tx] -= s[ty][j] * s[tx][j];
+        __syncthreads();
+    }
+    if (tx < kb && ty < kb && tx <= ty) A[(k0 + ty) + n * (k0 + tx)] = s[ty][tx];
+}
+__global__ void chol_trsm_kernel(double *A, int64_t n, int64_t k0, int kb)
+{   // rows i >= k0+kb: L[i, k0:k0+kb] = A[i, ...] L11^{-T}
+    __shared__ double L11[kCb][kCb + 1];
+    for (int t = threadIdx.x; t < kCb * kCb; t += blockDim.x) {
+        const int r = t % kCb, c = t / kCb;
+        L11[r][c] = (r < kb && c < kb) ? A[(k0 + r) + n * (k0 + c)] : 0.0;
+    }
+    __syncthreads();
+    const int64_t i = k0 + kb + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x[kCb];
+    for (int j = 0; j < kb; ++j) {
+        double a = A[i + n * (k0 + j)];
+        for (int t = 0; t < j; ++t) a -= x[t] * L11[j][t];
+        x[j] = a / L11[j][j];
+    }
+    for (int j = 0; j < kb; ++j) A[i + n * (k0 + j)] = x[j];
+}
+__global__ void chol_syrk_kernel(double *A, int64_t n, int64_t k0, int kb)
+{   // trailing update of the lower triangle
+    const int64_t j = k0 + kb + (int64_t)blockIdx.y * 16 + threadIdx.y;
+    const int64_t i = k0 + kb + (int64_t)blockIdx.x * 16 + threadIdx.x;
+    if (i >= n || j >= n || j > i) return;
+    double s = 0;
+    for (int t = 0; t < kb; ++t) s += A[i + n * (k0 + t)] * A[j + n * (k0 + t)];
+    A[i + n * j] -= s;
+}
+// L^{-1}, one thread per column (lower triangular result in W)
+__global__ void tri_inv_kernel(const double *__restrict__ L, double *__restrict__ W, int64_t n)
+{
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    for (int64_t i = 0; i < j; ++i) W[i + n * j] = 0.0;
+    W[j + n * j] = 1.0 / L[j + n * j];
+    for (int64_t i = j + 1; i < n; ++i) {
+        double s = 0;
+        for (int64_t k = j; k < i; ++k) s += L[i + n * k] * W[k + n * j];
+        W[i + n * j] = -s / L[i + n * i];
+    }
+}
+// A^{-1} = W^T W  (W = L^{-1} lower)
+__global__ void inv_gram_kernel(const double *__restrict__ W, double *__restrict__ Ainv, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * 16 + threadIdx.x, j = (int64_t)blockIdx.y * 16 + threadIdx.y;
+    if (i >= n || j >= n) return;
+    double s = 0;
+    for (int64_t k = (i > j ? i : j); k < n; ++k) s += W[k + n * i] * W[k + n * j];
+    Ainv[i + n * j] = s;
+}
+// coarsest solve: x_grid = Ainv * r (r gathered from the grid in compact order)
+template <typename T>
+__global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const int32_t *__restrict__ nodeGrid,
+                                       int64_t Nn, double *__restrict__ cr, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * Nn) return;
+    cr[t] = double(r[(t % 3) * g.cs + nodeGrid[t / 3]]);
+}
+template <typename T>
+__global__ void coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__ cr, int64_t n,
+                                     T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
+                                     const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double s = 0;
+    for (int64_t j = lane; j < n; j += 32) s += Ainv[j + n * row] * cr[j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) x[(row % 3) * g.cs + nodeGrid[row / 3]] = T(s);
+}
+
+// ---- PCG vector kernels (FP64, level-0 grid arrays) ----
+__global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
+                                  const double *__restrict__ v, int64_t ng, int64_t cs, PcgState *st, Reduce red)
+{
+    if (st->done) return;
+    const double lambda = st->rho / st->pv;
+    double rr = 0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * ng; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = (k / ng) * cs + k % ng;
+        x[i] += lambda * p[i];
+        const double rv = r[i] - lambda * v[i];
+        r[i] = rv;
+        rr += rv * rv;
+    }
+    block_sum_to<256>(rr, red.partials, red.counter, red.result);
+}
+__global__ void pcg_check_kernel(PcgState *st)
+{   // TOP_GPU.m:630-649
+    if (st->done) return;
+    st->its += 1;
+    const double res = sqrt(st->rr) / st->normB;
+    st->resnorm = res;
+    if (!isfinite(res) || !isfinite(st->rho) || !isfinite(st->pv)) { st->status = TOP_ERR_NAN; st->done = 1; return; }
+    if (res < st->tol) { st->done = 1; return; }
+    if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
+    st->rhoOld = st->rho;
+}
+__global__ void pcg_p_kernel(double *__restrict__ p, const double *__restrict__ z, int64_t ng, int64_t cs,
+                             const PcgState *st, int first)
+{
+    if (!first && st->done) return;
+    const double beta = first ? 0.0 : st->rho / st->rhoOld;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * ng; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = (k / ng) * cs + k % ng;
+        p[i] = z[i] + beta * p[i];
+    }
+}
+__global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t ng, int64_t cs, Reduce red)
+{
+    double s = 0;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * ng; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = (k / ng) * cs + k % ng;
+        s += a[i] * b[i];
+    }
+    block_sum_to<256>(s, red.partials, red.counter, red.result);
+}
+// element energies sum_k w_k u_k' Ke u_k (TOP_GPU.m:580-600) on grid vectors
+__global__ void compliance_kernel(const KeParam<double> K, const double *__restrict__ U, int64_t ustride,
+                                  int nLoads, const double *__restrict__ w, const int32_t *__restrict__ eleGrid,
+                                  int64_t Ne, Geom g, double *__restrict__ ce)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ne) return;
+    const int64_t slot = eleGrid[e];
+    double acc = 0;
+    for (int k = 0; k < nLoads; ++k) {
+        const double *u = U + k * ustride;
+        double ue[24];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ue[3 * j + c] = u[c * g.cs + slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j)];
+        double s = 0;
+#pragma unroll
+        for (int a = 0; a < 24; ++a) {
+            double t = 0;
+#pragma unroll
+            for (int b = 0; b < 24; ++b) t = fma(K.k[a + 24 * b], ue[b], t);
+            s = fma(t, ue[a], s);
+        }
+        acc += s * w[k];
+    }
+    ce[e] = acc;
+}
+
+// ---------------------------------------------------------------------------
+struct DevLevel {
+    int ny = 0, nx = 0, nz = 0, span = 0;
+    Geom g{};
+    int64_t Ne = 0, Nn = 0, ng = 0;
+    uint8_t *flags = nullptr;
+    int32_t *nodeGrid = nullptr, *eleGrid = nullptr, *upMap = nullptr;
+    double *KsC = nullptr, *KsP64 = nullptr; float *KsP32 = nullptr;
+    double *diag = nullptr, *invD64 = nullptr; float *invD32 = nullptr;
+    double *r64 = nullptr, *x64 = nullptr, *t64 = nullptr;
+    float *r32 = nullptr, *x32 = nullptr, *t32 = nullptr;
+    uint8_t *tileFixed = nullptr;
+};
+
+}  // namespace topgpu
+
+using namespace topgpu;
+
+struct top_solver {
+    top_solver_params p{};
+    cudaStream_t st = nullptr;
+    int nL = 0, nLoads = 0;
+    std::vector<DevLevel> L;
+    std::vector<void *> allocs;      // raw allocations (freed on destroy)
+    KeParam<double> Ke64{}; KeParam<float> Ke32{};
+    double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
+    double *Ec = nullptr, *Eg64 = nullptr; float *Eg32 = nullptr;
+    int32_t *mapUnique = nullptr; double *uFree = nullptr, *uFixed = nullptr; int64_t nU = 0;
+    double *Qs = nullptr; int32_t *eye = nullptr;
+    double *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *v = nullptr, *tmp = nullptr;
+    double *b = nullptr;             // [nLoads][3 x cs]
+    double *weights = nullptr;
+    PcgState *state = nullptr, *hstate = nullptr;
+    double *partials = nullptr; unsigned *counter = nullptr; int64_t nPartials = 0;
+    double *scal = nullptr;          // device scalars for standalone reductions
+    int *zeroDone = nullptr;
+    int64_t nC = 0; double *Ac = nullptr, *Ainv = nullptr, *Wc = nullptr, *cr = nullptr;
+    int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
+    bool assembled = false;
+    std::vector<double> Fhost; int64_t nd0 = 0;
+
+    template <typename T> T *dalloc(size_t n)
+    {
+        void *ptr = nullptr;
+        if (cudaMalloc(&ptr, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+        cudaMemset(ptr, 0, sizeof(T) * (n ? n : 1));
+        allocs.push_back(ptr);
+        return static_cast<T *>(ptr);
+    }
+    // grid array with margins: ncomp components of stride cs
+    template <typename T> T *galloc(int64_t cs, int ncomp)
+    {
+        T *b = dalloc<T>((size_t)cs * ncomp);
+        return b ? b + kMargin : nullptr;
+    }
+    Reduce red(double *result) const { return Reduce{partials, counter, result}; }
+};
+
+namespace {
+
+inline int nb256(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 1 << 20); }
+inline dim3 node_grid(const Geom &g) { return dim3((unsigned)g.nbx, (unsigned)g.NZ); }
+inline int vec_blocks(int64_t ng) { return (int)std::min<int64_t>((3 * ng + 255) / 256, 4096); }
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e__ = (call);                                                                \
+        if (e__ != cudaSuccess) { set_error("top_solver: CUDA error %d: %s", (int)e__, cudaGetErrorString(e__)); return TOP_ERR_CUDA; } \
+    } while (0)
+#define CKL() CK(cudaGetLastError())
+
+Geom make_geom(int ny, int nx, int nz)
+{
+    Geom g{};
+    g.NY = ny + 1; g.NX = nx + 1; g.NZ = nz + 1;
+    g.PY = (g.NY + 1 + 3) / 4 * 4;
+    const int64_t PX = g.NX + 2, PZ = g.NZ + 2;
+    g.plane = (int64_t)g.PY * PX;
+    const int64_t ng = g.plane * PZ;
+    g.cs = ng + 2 * kMargin;
+    g.origin = g.PY + g.plane;   // (Y=0, X'=1, Z'=1)
+    g.nbx = (int)(((int64_t)g.PY * g.NX + kNodeThreads - 1) / kNodeThreads);
+    return g;
+}
+inline int64_t gidx(const Geom &g, int Y, int X, int Z) { return g.origin + Y + (int64_t)g.PY * X + g.plane * Z; }
+
+// ---- level operators ------------------------------------------------------
+template <typename T> const T *ks_packed(const DevLevel &l);
+template <> const double *ks_packed<double>(const DevLevel &l) { return l.KsP64; }
+template <> const float *ks_packed<float>(const DevLevel &l) { return l.KsP32; }
+template <typename T> const T *invd(const DevLevel &l);
+template <> const double *invd<double>(const DevLevel &l) { return l.invD64; }
+template <> const float *invd<float>(const DevLevel &l) { return l.invD32; }
+template <typename T> T *vr(DevLevel &l);
+template <> double *vr<double>(DevLevel &l) { return l.r64; }
+template <> float *vr<float>(DevLevel &l) { return l.r32; }
+template <typename T> T *vx(DevLevel &l);
+template <> double *vx<double>(DevLevel &l) { return l.x64; }
+template <> float *vx<float>(DevLevel &l) { return l.x32; }
+template <typename T> T *vt(DevLevel &l);
+template <> double *vt<double>(DevLevel &l) { return l.t64; }
+template <> float *vt<float>(DevLevel &l) { return l.t32; }
+template <typename T> const KeParam<T> &keparam(const top_solver *s);
+template <> const KeParam<double> &keparam<double>(const top_solver *s) { return s->Ke64; }
+template <> const KeParam<float> &keparam<float>(const top_solver *s) { return s->Ke32; }
+template <typename T> const T *egrid(const top_solver *s);
+template <> const double *egrid<double>(const top_solver *s) { return s->Eg64; }
+template <> const float *egrid<float>(const top_solver *s) { return s->Eg32; }
+
+// y-epilogue applied to (K_level in)(node) for every node of the level
+template <typename T, class In, class Out>
+void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done)
+{
+    DevLevel &lv = s->L[l];
+    if (l == 0)
+        l0_kernel<T, In, Out><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(
+            keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
+    else
+        coarse_kernel<T, In, Out><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+}
+
+// V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
+// residual r0 (type TR, grid layout); writes z0 (type TZ) and, when zr is
+// set, z0 . r0 into *zr.
+template <typename T, typename TR, typename TZ>
+void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
+{
+    const int nL = s->nL;
+    const T omega = T(s->p.omega);
+    const Reduce none{nullptr, nullptr, nullptr};
+    // restriction leg
+    for (int l = 0; l < nL - 1; ++l) {
+        DevLevel &lv = s->L[l], &lc = s->L[l + 1];
+        T *d = vt<T>(lv);
+        if (l == 0)
+            level_op<T>(s, l, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega}, ResidOut<T, TR, T>{r0, d, lv.g.cs}, none, done);
+        else
+            level_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs}, none, done);
+        if (lc.span == 4)
+            restrict_kernel<T, 4><<<node_grid(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
+        else
+            restrict_kernel<T, 2><<<node_grid(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
+    }
+    // coarsest direct solve, FP64
+    DevLevel &lc = s->L[nL - 1];
+    const int64_t n = 3 * lc.Nn;
+    coarsest_gather_kernel<T><<<nb256(n), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done);
+    coarsest_gemv_kernel<T><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g, lc.nodeGrid, done);
+    // interpolation leg
+    for (int l = nL - 2; l >= 0; --l) {
+        DevLevel &lv = s->L[l], &lcn = s->L[l + 1];
+        const T *xc = vt<T>(lcn);
+        T *x = vx<T>(lv);
+        if (l == 0) {
+            if (lcn.span == 4)
+                prolong_kernel<T, 4, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
+            else
+                prolong_kernel<T, 2, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
+            level_op<T>(s, 0, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega},
+                        zr ? s->red(zr) : none, done);
+        } else {
+            if (lcn.span == 4)
+                prolong_kernel<T, 4, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
+            else
+                prolong_kernel<T, 2, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
+            level_op<T>(s, l, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega}, none, done);
+        }
+    }
+}
+
+void precond(top_solver *s, const double *r0, double *z0, double *zr, const int *done)
+{
+    if (s->p.precision == TOP_PREC_MIXED) vcycle<float, double, double>(s, r0, z0, zr, done);
+    else vcycle<double, double, double>(s, r0, z0, zr, done);
+}
+
+// outer operator v = K0 u on FP64 grid vectors, u.v into *uy.  FP64 unless
+// outerFP32 (the reference's mixed mode runs it in single, TOP_GPU.m:683-684).
+void outer_op(top_solver *s, const double *u, double *y, double *uy, const int *done)
+{
+    DevLevel &l0 = s->L[0];
+    const Reduce red = uy ? s->red(uy) : Reduce{nullptr, nullptr, nullptr};
+    if (s->p.outerFP32)
+        level_op<float>(s, 0, VecIn<float, double>{u, l0.g.cs}, DotStoreOut<float, double, double>{y, u, l0.g.cs}, red, done);
+    else
+        level_op<double>(s, 0, VecIn<double, double>{u, l0.g.cs}, DotStoreOut<double, double, double>{y, u, l0.g.cs}, red, done);
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *p, top_solver **out)
+{
+    if (!mesh || !p || !out) { set_error("top_solver_create: bad arguments"); return TOP_ERR_ARGS; }
+    if (!mesh->hasBC) { set_error("top_solver_create: apply boundary conditions first"); return TOP_ERR_STATE; }
+    if (mesh->superElement) { set_error("top_solver_create: super-element models use top_super_* entry points"); return TOP_ERR_ARGS; }
+    if (p->precision != TOP_PREC_FP64 && p->precision != TOP_PREC_MIXED) { set_error("top_solver_create: bad precision"); return TOP_ERR_ARGS; }
+    top_solver *s = new (std::nothrow) top_solver();
+    if (!s) return TOP_ERR_NOMEM;
+    s->p = *p;
+    s->nL = (int)mesh->L.size();
+    s->nLoads = mesh->nLoads;
+    s->L.resize(s->nL);
+    auto fail = [&](const char *what) { set_error("top_solver_create: %s", what); top_solver_destroy(s); return TOP_ERR_NOMEM; };
+    for (int l = 0; l < s->nL; ++l) {
+        const MeshLevel &M = mesh->L[l];
+        DevLevel &d = s->L[l];
+        d.ny = M.resY; d.nx = M.resX; d.nz = M.resZ; d.span = M.span;
+        d.g = make_geom(d.ny, d.nx, d.nz);
+        d.Ne = M.Ne; d.Nn = M.Nn; d.ng = d.g.cs - 2 * kMargin;
+        const int64_t cs = d.g.cs;
+        // host-side flags, node and element maps
+        std::vector<uint8_t> fl(cs, 0);
+        std::vector<int32_t> ng(M.Nn), eg(M.Ne);
+        {   // nodes of this level in its own grid numbering: invert nodMapForward
+            const int NY = d.ny + 1, NX = d.nx + 1;
+            for (int64_t t = 0; t < (int64_t)M.nodMapForward.size(); ++t) {
+                const int32_t c = M.nodMapForward[t];
+                if (!c) continue;
+                const int Y = int(t % NY), X = int((t / NY) % NX), Z = int(t / ((int64_t)NY * NX));
+                const int64_t gi = gidx(d.g, Y, X, Z);
+                ng[c - 1] = (int32_t)gi;
+                fl[gi + kMargin] = kActive | (l == 0 ? mesh->nodeFixed[c - 1] : 0);
+            }
+            for (int64_t e = 0; e < M.Ne; ++e) {
+                const int64_t gE = M.eleMapBack[e] - 1;
+                const int ey = int(gE % d.ny), ex = int((gE / d.ny) % d.nx), ez = int(gE / ((int64_t)d.ny * d.nx));
+                eg[e] = (int32_t)gidx(d.g, ey, ex, ez);
+            }
+        }
+        d.flags = s->dalloc<uint8_t>(cs);
+        d.nodeGrid = s->dalloc<int32_t>(M.Nn);
+        d.eleGrid = s->dalloc<int32_t>(M.Ne);
+        if (!d.flags || !d.nodeGrid || !d.eleGrid) return fail("out of device memory");
+        cudaMemcpy(d.flags, fl.data(), cs, cudaMemcpyHostToDevice);
+        d.flags += kMargin;
+        cudaMemcpy(d.nodeGrid, ng.data(), sizeof(int32_t) * M.Nn, cudaMemcpyHostToDevice);
+        cudaMemcpy(d.eleGrid, eg.data(), sizeof(int32_t) * M.Ne, cudaMemcpyHostToDevice);
+        d.diag = s->galloc<double>(cs, 3);
+        d.invD64 = s->galloc<double>(cs, 3);
+        d.invD32 = s->galloc<float>(cs, 3);
+        d.x64 = s->galloc<double>(cs, 3); d.t64 = s->galloc<double>(cs, 3);
+        d.x32 = s->galloc<float>(cs, 3); d.t32 = s->galloc<float>(cs, 3);
+        if (l > 0) {
+            d.r64 = s->galloc<double>(cs, 3); d.r32 = s->galloc<float>(cs, 3);
+            const int nch = M.span * M.span * M.span;
+            d.upMap = s->dalloc<int32_t>((size_t)M.Ne * nch);
+            d.KsC = s->dalloc<double>((size_t)M.Ne * 576);
+            if (!d.upMap || !d.KsC) return fail("out of device memory");
+            cudaMemcpy(d.upMap, M.elementUpwardMap.data(), sizeof(int32_t) * M.Ne * nch, cudaMemcpyHostToDevice);
+            if (l < s->nL - 1) {
+                d.KsP64 = s->galloc<double>(cs, 300);
+                d.KsP32 = s->galloc<float>(cs, 300);
+                if (!d.KsP64 || !d.KsP32) return fail("out of device memory");
+            }
+        }
+        if (!d.diag || !d.invD64 || !d.invD32 || !d.x64 || !d.t64 || !d.x32 || !d.t32) return fail("out of device memory");
+        if (l == 0) {
+            // blocks whose stencil touches a fixed node take the masked path
+            std::vector<uint8_t> tf((size_t)d.g.nbx * d.g.NZ, 0);
+            const int NY = d.ny + 1, NX = d.nx + 1, NZ = d.nz + 1;
+            for (int64_t n = 0; n < M.Nn; ++n) {
+                if (!mesh->nodeFixed[n]) continue;
+                const int64_t t = M.nodMapBack[n] - 1;
+                const int Y = int(t % NY), X = int((t / NY) % NX), Z = int(t / ((int64_t)NY * NX));
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dx = -1; dx <= 1; ++dx)
+                        for (int dy = -1; dy <= 1; ++dy) {
+                            const int y = Y + dy, x = X + dx, z = Z + dz;
+                            if (y < 0 || y >= NY || x < 0 || x >= NX || z < 0 || z >= NZ) continue;
+                            const int64_t qq = y + (int64_t)d.g.PY * x;
+                            tf[(size_t)(qq / kNodeThreads) + (size_t)d.g.nbx * z] = 1;
+                        }
+            }
+            d.tileFixed = s->dalloc<uint8_t>(tf.size());
+            if (!d.tileFixed) return fail("out of device memory");
+            cudaMemcpy(d.tileFixed, tf.data(), tf.size(), cudaMemcpyHostToDevice);
+        }
+    }
+    // level-0 data
+    DevLevel &l0 = s->L[0];
+    const MeshLevel &M0 = mesh->L[0];
+    for (int t = 0; t < 576; ++t) { s->Ke64.k[t] = M0.Ke[t]; s->Ke32.k[t] = float(M0.Ke[t]); }
+    s->KeDev = s->dalloc<double>(576);
+    s->Ec = s->dalloc<double>(M0.Ne);
+    s->Eg64 = s->galloc<double>(l0.g.cs, 1);
+    s->Eg32 = s->galloc<float>(l0.g.cs, 1);
+    s->nU = (int64_t)mesh->eleWithFixedDOFs.size();
+    s->mapUnique = s->dalloc<int32_t>(M0.Ne);
+    s->uFree = s->dalloc<double>((size_t)576 * s->nU);
+    s->uFixed = s->dalloc<double>((size_t)576 * s->nU);
+    s->P4 = s->dalloc<double>((size_t)576 * 64);
+    s->P2 = s->dalloc<double>((size_t)576 * 8);
+    s->Qs = s->dalloc<double>((size_t)576 * 64);
+    s->eye = s->dalloc<int32_t>(64 * 64 + 4);
+    if (!s->KeDev || !s->Ec || !s->Eg64 || !s->Eg32 || !s->mapUnique || !s->uFree || !s->uFixed || !s->P4 || !s->P2 || !s->Qs || !s->eye)
+        return fail("out of device memory");
+    cudaMemcpy(s->KeDev, M0.Ke, sizeof(double) * 576, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->mapUnique, mesh->mapUniqueKes.data(), sizeof(int32_t) * M0.Ne, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->uFree, mesh->uniqueKesFree.data(), sizeof(double) * 576 * s->nU, cudaMemcpyHostToDevice);
+    {
+        std::vector<double> fx(mesh->uniqueKesFixed);
+        for (auto &v : fx) v *= p->E0;     // uniqueKesFixed_ * modulus_ (TOP_GPU.m:1614)
+        cudaMemcpy(s->uFixed, fx.data(), sizeof(double) * 576 * s->nU, cudaMemcpyHostToDevice);
+    }
+    {
+        std::vector<double> P((size_t)576 * 64);
+        for (int q = 0; q < 64; ++q) child_prolongation(4, q, &P[(size_t)576 * q]);
+        cudaMemcpy(s->P4, P.data(), sizeof(double) * 576 * 64, cudaMemcpyHostToDevice);
+        for (int q = 0; q < 8; ++q) child_prolongation(2, q, &P[(size_t)576 * q]);
+        cudaMemcpy(s->P2, P.data(), sizeof(double) * 576 * 8, cudaMemcpyHostToDevice);
+    }
+    // PCG vectors
+    const int64_t cs0 = l0.g.cs;
+    s->x = s->galloc<double>(cs0, 3); s->r = s->galloc<double>(cs0, 3); s->z = s->galloc<double>(cs0, 3);
+    s->pv = s->galloc<double>(cs0, 3); s->v = s->galloc<double>(cs0, 3); s->tmp = s->galloc<double>(cs0, 3);
+    s->b = s->galloc<double>(cs0, 3 * std::max(1, s->nLoads));
+    s->weights = s->dalloc<double>(std::max(1, s->nLoads));
+    if (!s->x || !s->r || !s->z || !s->pv || !s->v || !s->tmp || !s->b || !s->weights) return fail("out of device memory");
+    cudaMemcpy(s->weights, mesh->weights.data(), sizeof(double) * s->nLoads, cudaMemcpyHostToDevice);
+    s->nd0 = 3 * M0.Nn;
+    {
+        double *Fd = s->dalloc<double>((size_t)s->nd0 * s->nLoads);
+        if (!Fd) return fail("out of device memory");
+        cudaMemcpy(Fd, mesh->F.data(), sizeof(double) * s->nd0 * s->nLoads, cudaMemcpyHostToDevice);
+        for (int k = 0; k < s->nLoads; ++k)
+            compact_to_grid_kernel<double, double><<<nb256(M0.Nn), 256>>>(Fd + (size_t)k * s->nd0, s->b + (size_t)k * 3 * cs0, l0.nodeGrid, M0.Nn, cs0);
+    }
+    // reduction scratch
+    int64_t maxBlocks = 4096;
+    for (auto &d : s->L) maxBlocks = std::max<int64_t>(maxBlocks, (int64_t)d.g.nbx * d.g.NZ);
+    s->nPartials = maxBlocks;
+    s->partials = s->dalloc<double>(maxBlocks);
+    s->counter = s->dalloc<unsigned>(4);
+    s->scal = s->dalloc<double>(16);
+    s->zeroDone = s->dalloc<int>(4);
+    s->state = s->dalloc<PcgState>(1);
+    if (cudaMallocHost(&s->hstate, sizeof(PcgState)) != cudaSuccess) s->hstate = nullptr;
+    if (!s->partials || !s->counter || !s->scal || !s->zeroDone || !s->state || !s->hstate) return fail("out of memory");
+    // coarsest level maps
+    {
+        DevLevel &lc = s->L[s->nL - 1];
+        const MeshLevel &MC = mesh->L[s->nL - 1];
+        s->nC = 3 * MC.Nn;
+        if (s->nC > 16384) {
+            set_error("top_solver_create: coarsest level has %lld DOFs (> 16384); lower coarsestResolutionControl", (long long)s->nC);
+            top_solver_destroy(s);
+            return TOP_ERR_SHAPE;
+        }
+        std::vector<int32_t> ec(lc.g.cs, -1), nc(lc.g.cs, -1);
+        const int NY = lc.ny + 1, NX = lc.nx + 1;
+        for (int64_t t = 0; t < (int64_t)MC.nodMapForward.size(); ++t) {
+            const int32_t c = MC.nodMapForward[t];
+            if (!c) continue;
+            const int Y = int(t % NY), X = int((t / NY) % NX), Z = int(t / ((int64_t)NY * NX));
+            nc[gidx(lc.g, Y, X, Z) + kMargin] = c - 1;
+        }
+        for (int64_t e = 0; e < MC.Ne; ++e) {
+            const int64_t gE = MC.eleMapBack[e] - 1;
+            const int ey = int(gE % lc.ny), ex = int((gE / lc.ny) % lc.nx), ez = int(gE / ((int64_t)lc.ny * lc.nx));
+            ec[gidx(lc.g, ey, ex, ez) + kMargin] = (int32_t)e;
+        }
+        s->eleCompactC = s->dalloc<int32_t>(lc.g.cs);
+        s->nodeCompactC = s->dalloc<int32_t>(lc.g.cs);
+        s->Ac = s->dalloc<double>((size_t)s->nC * s->nC);
+        s->Ainv = s->dalloc<double>((size_t)s->nC * s->nC);
+        s->Wc = s->dalloc<double>((size_t)s->nC * s->nC);
+        s->cr = s->dalloc<double>((size_t)s->nC);
+        if (!s->eleCompactC || !s->nodeCompactC || !s->Ac || !s->Ainv || !s->Wc || !s->cr) return fail("out of device memory");
+        cudaMemcpy(s->eleCompactC, ec.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
+        cudaMemcpy(s->nodeCompactC, nc.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
+        s->eleCompactC += kMargin; s->nodeCompactC += kMargin;
+    }
+    cudaError_t err = cudaDeviceSynchronize();
+    if (err != cudaSuccess) { set_error("top_solver_create: %s", cudaGetErrorString(err)); top_solver_destroy(s); return TOP_ERR_CUDA; }
+    *out = s;
+    return TOP_OK;
+}
+
+extern "C" int top_solver_destroy(top_solver *s)
+{
+    if (!s) return TOP_OK;
+    for (void *p : s->allocs) cudaFree(p);
+    if (s->hstate) cudaFreeHost(s->hstate);
+    delete s;
+    return TOP_OK;
+}
+
+extern "C" int top_solver_set_stream(top_solver *s, void *stream)
+{
+    if (!s) return TOP_ERR_ARGS;
+    s->st = reinterpret_cast<cudaStream_t>(stream);
+    return TOP_OK;
+}
+
+extern "C" int top_solver_sizes(const top_solver *s, int64_t *out3)
+{
+    if (!s || !out3) return TOP_ERR_ARGS;
+    out3[0] = s->nL; out3[1] = s->nLoads; out3[2] = s->nd0;
+    return TOP_OK;
+}
+
+static int set_E(top_solver *s, const double *src, int where, int simp)
+{
+    if (!s || !src) return TOP_ERR_ARGS;
+    const int64_t Ne = s->L[0].Ne;
+    const double *d = src;
+    if (where == 0) {
+        CK(cudaMemcpyAsync(s->tmp, src, sizeof(double) * Ne, cudaMemcpyHostToDevice, s->st));
+        d = s->tmp;
+    }
+    modulus_kernel<<<nb256(Ne), 256, 0, s->st>>>(d, simp, s->p.E0, s->p.Emin, s->p.penal, s->Ec, s->Eg64, s->Eg32, s->L[0].eleGrid, Ne);
+    CKL();
+    s->assembled = false;
+    return TOP_OK;
+}
+extern "C" int top_solver_set_modulus(top_solver *s, const double *E, int where) { return set_E(s, E, where, 0); }
+extern "C" int top_solver_set_density(top_solver *s, const double *x, int where) { return set_E(s, x, where, 1); }
+
+extern "C" int top_solver_assemble(top_solver *s)
+{
+    if (!s) return TOP_ERR_ARGS;
+    cudaStream_t st = s->st;
+    // Galerkin Ks (TOP_GPU.m:1054-1147)
+    for (int l = 1; l < s->nL; ++l) {
+        DevLevel &d = s->L[l];
+        int rc;
+        if (l == 1)
+            rc = assemble_level2_f64(d.KsC, d.upMap, s->Ec, s->KeDev, s->P4, s->mapUnique, s->uFree, s->uFixed,
+                                     d.Ne, 64, s->nU, s->Qs, s->eye, st);
+        else
+            rc = assemble_higher_f64(d.KsC, d.upMap, s->L[l - 1].KsC, s->P2, d.Ne, 8, st);
+        if (rc) { set_error("top_solver_assemble: Galerkin kernel failed"); return rc; }
+        if (l < s->nL - 1) {
+            pack_ks_kernel<<<(unsigned)d.Ne, 32, 0, st>>>(d.KsC, d.eleGrid, d.Ne, d.KsP64, d.KsP32, d.g.cs);
+            diag_coarse_kernel<<<node_grid(d.g), kNodeThreads, 0, st>>>(d.KsP64, d.g, d.flags, d.diag, d.invD64, d.invD32);
+        }
+    }
+    DevLevel &l0 = s->L[0];
+    diag_l0_kernel<<<node_grid(l0.g), kNodeThreads, 0, st>>>(s->Ke64, s->Eg64, l0.flags, l0.g, s->p.E0, l0.diag, l0.invD64, l0.invD32);
+    CKL();
+    // coarsest matrix, Cholesky, inverse (TOP_GPU.m:1240-1255)
+    DevLevel &lc = s->L[s->nL - 1];
+    const int64_t n = s->nC;
+    CK(cudaMemsetAsync(s->Ac, 0, sizeof(double) * n * n, st));
+    coarsest_assemble_kernel<<<nb256(n), 256, 0, st>>>(lc.KsC, lc.nodeGrid, s->eleCompactC, s->nodeCompactC, lc.g, lc.Nn, s->Ac);
+    CK(cudaMemsetAsync(s->zeroDone, 0, sizeof(int) * 4, st));
+    for (int64_t k0 = 0; k0 < n; k0 += kCb) {
+        const int kb = (int)std::min<int64_t>(kCb, n - k0);
+        chol_diag_kernel<<<1, dim3(kCb, kCb), 0, st>>>(s->Ac, n, k0, kb, s->zeroDone + 1);
+        const int64_t rest = n - k0 - kb;
+        if (rest > 0) {
+            chol_trsm_kernel<<<(unsigned)((rest + 127) / 128), 128, 0, st>>>(s->Ac, n, k0, kb);
+            dim3 gs((unsigned)((rest + 15) / 16), (unsigned)((rest + 15) / 16));
+            chol_syrk_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Ac, n, k0, kb);
+        }
+    }
+    tri_inv_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(s->Ac, s->Wc, n);
+    {
+        dim3 gs((unsigned)((n + 15) / 16), (unsigned)((n + 15) / 16));
+        inv_gram_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Wc, s->Ainv, n);
+    }
+    CKL();
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, s->zeroDone + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (flag) { set_error("top_solver_assemble: coarsest matrix is not positive definite"); return TOP_ERR_NAN; }
+    s->assembled = true;
+    return TOP_OK;
+}
+
+// ---- standalone operators on compact vectors ------------------------------
+extern "C" int top_solver_matvec(top_solver *s, int level, const double *u, double *y, int fp32)
+{
+    if (!s || !u || !y || level < 0 || level >= s->nL) { set_error("top_solver_matvec: bad arguments"); return TOP_ERR_ARGS; }
+    if (level > 0 && !s->assembled) { set_error("top_solver_matvec: assemble first"); return TOP_ERR_STATE; }
+    if (level == s->nL - 1 && level > 0) { set_error("top_solver_matvec: the coarsest level is solved directly"); return TOP_ERR_ARGS; }
+    DevLevel &d = s->L[level];
+    const Reduce none{nullptr, nullptr, nullptr};
+    CK(cudaMemsetAsync(d.x64 - kMargin, 0, sizeof(double) * 3 * d.g.cs, s->st));
+    compact_to_grid_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(u, d.x64, d.nodeGrid, d.Nn, d.g.cs);
+    if (fp32) {
+        level_op<float>(s, level, VecIn<float, double>{d.x64, d.g.cs}, StoreOut<float, double>{d.t64, d.g.cs}, none, nullptr);
+    } else {
+        level_op<double>(s, level, VecIn<double, double>{d.x64, d.g.cs}, StoreOut<double, double>{d.t64, d.g.cs}, none, nullptr);
+    }
+    grid_to_compact_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(d.t64, y, d.nodeGrid, d.Nn, d.g.cs);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_vcycle(top_solver *s, const double *r, double *z)
+{
+    if (!s || !r || !z) return TOP_ERR_ARGS;
+    if (!s->assembled) { set_error("top_solver_vcycle: assemble first"); return TOP_ERR_STATE; }
+    DevLevel &l0 = s->L[0];
+    CK(cudaMemsetAsync(s->tmp - kMargin, 0, sizeof(double) * 3 * l0.g.cs, s->st));
+    compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(r, s->tmp, l0.nodeGrid, l0.Nn, l0.g.cs);
+    precond(s, s->tmp, s->z, nullptr, s->zeroDone);
+    grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(s->z, z, l0.nodeGrid, l0.Nn, l0.g.cs);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_restrict(top_solver *s, int ii, const double *rF, double *rC)
+{
+    if (!s || ii < 1 || ii >= s->nL) return TOP_ERR_ARGS;
+    DevLevel &f = s->L[ii - 1], &c = s->L[ii];
+    CK(cudaMemsetAsync(f.x64 - kMargin, 0, sizeof(double) * 3 * f.g.cs, s->st));
+    compact_to_grid_kernel<double, double><<<nb256(f.Nn), 256, 0, s->st>>>(rF, f.x64, f.nodeGrid, f.Nn, f.g.cs);
+    if (c.span == 4) restrict_kernel<double, 4><<<node_grid(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
+    else restrict_kernel<double, 2><<<node_grid(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
+    grid_to_compact_kernel<double, double><<<nb256(c.Nn), 256, 0, s->st>>>(c.t64, rC, c.nodeGrid, c.Nn, c.g.cs);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_interpolate(top_solver *s, int ii, const double *xC, double *xF)
+{
+    if (!s || ii < 1 || ii >= s->nL) return TOP_ERR_ARGS;
+    DevLevel &f = s->L[ii - 1], &c = s->L[ii];
+    CK(cudaMemsetAsync(c.x64 - kMargin, 0, sizeof(double) * 3 * c.g.cs, s->st));
+    compact_to_grid_kernel<double, double><<<nb256(c.Nn), 256, 0, s->st>>>(xC, c.x64, c.nodeGrid, c.Nn, c.g.cs);
+    if (c.span == 4)
+        prolong_kernel<double, 4, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.x64, c.g, f.t64, f.g, f.flags, nullptr, nullptr, 0.0, nullptr);
+    else
+        prolong_kernel<double, 2, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.x64, c.g, f.t64, f.g, f.flags, nullptr, nullptr, 0.0, nullptr);
+    grid_to_compact_kernel<double, double><<<nb256(f.Nn), 256, 0, s->st>>>(f.t64, xF, f.nodeGrid, f.Nn, f.g.cs);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_get_diag(top_solver *s, int level, double *diag)
+{
+    if (!s || !diag || level < 0 || level >= s->nL - (s->nL > 1 ? 1 : 0)) return TOP_ERR_ARGS;
+    if (!s->assembled) { set_error("top_solver_get_diag: assemble first"); return TOP_ERR_STATE; }
+    DevLevel &d = s->L[level];
+    grid_to_compact_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(d.diag, diag, d.nodeGrid, d.Nn, d.g.cs);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_get_ks(top_solver *s, int level, double *Ks)
+{
+    if (!s || !Ks || level < 1 || level >= s->nL) return TOP_ERR_ARGS;
+    if (!s->assembled) { set_error("top_solver_get_ks: assemble first"); return TOP_ERR_STATE; }
+    DevLevel &d = s->L[level];
+    CK(cudaMemcpyAsync(Ks, d.KsC, sizeof(double) * 576 * d.Ne, cudaMemcpyDeviceToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+// ---- PCG (Solving_PCG, TOP_GPU.m:602-667) ---------------------------------
+static int pcg_run(top_solver *s, const double *bGrid, double *U, int warm, int *itsOut, double *resOut)
+{
+    if (!s->assembled) { set_error("top_solver_pcg: assemble first"); return TOP_ERR_STATE; }
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs, ng = l0.ng;
+    cudaStream_t st = s->st;
+    const int VB = vec_blocks(ng);
+    // state
+    PcgState h{};
+    h.tol = s->p.tol; h.maxIT = s->p.maxIT;
+    CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+    int *done = &s->state->done;
+    // normB
+    dot_kernel<<<VB, 256, 0, st>>>(bGrid, bGrid, ng, cs, s->red(s->scal));
+    // x0
+    CK(cudaMemsetAsync(s->x - kMargin, 0, sizeof(double) * 3 * cs, st));
+    if (warm) compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, st>>>(U, s->x, l0.nodeGrid, l0.Nn, cs);
+    // r = b - A x
+    if (s->p.outerFP32)
+        level_op<float>(s, 0, VecIn<float, double>{s->x, cs}, ResidOut<float, double, double>{bGrid, s->r, cs},
+                        Reduce{nullptr, nullptr, nullptr}, nullptr);
+    else
+        level_op<double>(s, 0, VecIn<double, double>{s->x, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
+                         Reduce{nullptr, nullptr, nullptr}, nullptr);
+    CKL();
+    // copy ||b||^2 from scal[0] and set up the loop state on the device
+    CK(cudaStreamSynchronize(st));
+    double nb2 = 0;
+    CK(cudaMemcpy(&nb2, s->scal, sizeof(double), cudaMemcpyDeviceToHost));
+    h.normB = std::sqrt(nb2);
+    h.done = 0; h.its = 0; h.status = 0;
+    if (h.normB == 0.0) {
+        CK(cudaMemsetAsync(U, 0, sizeof(double) * s->nd0, st));
+        if (itsOut) *itsOut = 0;
+        if (resOut) *resOut = 0.0;
+        CK(cudaStreamSynchronize(st));
+        return TOP_OK;
+    }
+    CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+    // z = M r ; rho = z . r ; p = z
+    precond(s, s->r, s->z, &s->state->rho, nullptr);
+    pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 1);
+    CKL();
+    static const bool trace = std::getenv("TOPGPU_PCG_TRACE") != nullptr;
+    if (trace) {
+        CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        std::fprintf(stderr, "pcg init normB %.6e rho %.6e\n", s->hstate->normB, s->hstate->rho);
+    }
+    const int chunk = trace ? 1 : 4;
+    for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
+        for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
+            outer_op(s, s->pv, s->v, &s->state->pv, done);                                   // v = A p, p.v
+            pcg_update_kernel<<<VB, 256, 0, st>>>(s->x, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
+            pcg_check_kernel<<<1, 1, 0, st>>>(s->state);
+            precond(s, s->r, s->z, &s->state->rho, done);                                     // z = M r, z.r
+            pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 0);              // p = z + beta p
+        }
+        CKL();
+        CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (trace && it0 < 12)
+            std::fprintf(stderr, "pcg it %d rho %.6e rhoOld %.6e pv %.6e rr %.6e res %.6e done %d\n", s->hstate->its,
+                         s->hstate->rho, s->hstate->rhoOld, s->hstate->pv, s->hstate->rr, s->hstate->resnorm, s->hstate->done);
+        if (s->hstate->done) break;
+    }
+    const PcgState &f = *s->hstate;
+    grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, st>>>(s->x, U, l0.nodeGrid, l0.Nn, cs);
+    CKL();
+    CK(cudaStreamSynchronize(st));
+    if (itsOut) *itsOut = f.its;
+    if (resOut) *resOut = f.resnorm;
+    if (f.status == TOP_ERR_NAN) { set_error("top_solver_pcg: non-finite PCG scalar at iteration %d", f.its); return TOP_ERR_NAN; }
+    if (f.status == TOP_ERR_NOT_CONVERGED) { set_error("Exceed the maximum iterate numbers (residual %.4e)", f.resnorm); return TOP_ERR_NOT_CONVERGED; }
+    return TOP_OK;
+}
+
+extern "C" int top_solver_pcg(top_solver *s, int loadCase, double *U, int warm, int *its, double *relres)
+{
+    if (!s || !U || loadCase < 0 || loadCase >= s->nLoads) { set_error("top_solver_pcg: bad arguments"); return TOP_ERR_ARGS; }
+    return pcg_run(s, s->b + (size_t)loadCase * 3 * s->L[0].g.cs, U, warm, its, relres);
+}
+
+extern "C" int top_solver_pcg_rhs(top_solver *s, const double *b, double *U, int warm, int *its, double *relres)
+{
+    if (!s || !b || !U) return TOP_ERR_ARGS;
+    DevLevel &l0 = s->L[0];
+    CK(cudaMemsetAsync(s->tmp - kMargin, 0, sizeof(double) * 3 * l0.g.cs, s->st));
+    compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(b, s->tmp, l0.nodeGrid, l0.Nn, l0.g.cs);
+    CKL();
+    return pcg_run(s, s->tmp, U, warm, its, relres);
+}
+
+extern "C" int top_solver_unit_compliance(top_solver *s, const double *U, double *ce)
+{
+    if (!s || !U || !ce) return TOP_ERR_ARGS;
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs;
+    // U compact [3Nn x nLoads] -> grid; the b array has room for nLoads grid vectors
+    double *Ug = s->b;   // overwritten below, so re-upload afterwards would be needed: use tmp for 1 load
+    if (s->nLoads != 1) { set_error("top_solver_unit_compliance: multiple load cases not supported in this call"); return TOP_ERR_ARGS; }
+    Ug = s->tmp;
+    CK(cudaMemsetAsync(Ug - kMargin, 0, sizeof(double) * 3 * cs, s->st));
+    compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U, Ug, l0.nodeGrid, l0.Nn, cs);
+    compliance_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(s->Ke64, Ug, 3 * cs, 1, s->weights, l0.eleGrid, l0.Ne, l0.g, ce);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+// ---- kernel timing (CUDA events on the solver's stream) -------------------
+// which: 0 = level-0 K*u FP64 (the outer PCG operator), 1 = level-0 K*u FP32
+// (the V-cycle smoother operator), 2 = one V-cycle, 3 = level-1 K*u FP32.
+// Each launch is preceded by a write of flushBytes to evict L2 (0 = none);
+// *msPerLaunch receives the mean event time of the launches alone.
+extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushBytes, double *msPerLaunch)
+{
+    if (!s || nrep < 1 || !msPerLaunch) return TOP_ERR_ARGS;
+    if (which != 0 && !s->assembled) { set_error("top_solver_time_kernel: assemble first"); return TOP_ERR_STATE; }
+    DevLevel &l0 = s->L[0];
+    const Reduce none{nullptr, nullptr, nullptr};
+    void *flush = nullptr;
+    if (flushBytes > 0) CK(cudaMalloc(&flush, (size_t)flushBytes));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a)); CK(cudaEventCreate(&b));
+    double total = 0;
+    for (int k = 0; k < nrep; ++k) {
+        if (flush) CK(cudaMemsetAsync(flush, k & 0xff, (size_t)flushBytes, s->st));
+        CK(cudaEventRecord(a, s->st));
+        switch (which) {
+        case 0: level_op<double>(s, 0, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr); break;
+        case 1: level_op<float>(s, 0, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr); break;
+        case 2: precond(s, s->r, s->z, nullptr, s->zeroDone); break;
+        case 3: if (s->nL > 2) level_op<float>(s, 1, VecIn<float, float>{s->L[1].x32, s->L[1].g.cs}, StoreOut<float, float>{s->L[1].t32, s->L[1].g.cs}, none, nullptr); break;
+        default: set_error("top_solver_time_kernel: unknown kernel %d", which); return TOP_ERR_ARGS;
+        }
+        CK(cudaEventRecord(b, s->st));
+        CK(cudaEventSynchronize(b));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        total += ms;
+    }
+    cudaEventDestroy(a); cudaEventDestroy(b);
+    if (flush) cudaFree(flush);
+    CKL();
+    *msPerLaunch = total / nrep;
+    return TOP_OK;
+}

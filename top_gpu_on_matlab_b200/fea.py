@@ -1,0 +1,211 @@
+"""Host-side mirror of TOP_GPU's FEA model and solver over libtopgpu.so.
+
+``Mesh`` is CreateVoxelFEAmodel / FEA_VoxelBasedDiscretization /
+Solving_BuildingMeshHierarchy / FEA_ApplyBoundaryCondition /
+Solving_SetupKeWithFixedDOFs (TOP_GPU.m:403-536, 1276-1442, 1505-1727), built
+on the host by the library (no GPU needed).  ``Solver`` holds one model on the
+GPU and provides Solving_AssembleFEAstencil, Solving_KbyU_MatrixFree,
+Solving_Vcycle and Solving_PCG (TOP_GPU.m:602-878, 1033-1267).
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from ._lib import (SolverParams, TOP_ERR_NOT_CONVERGED, TOP_OK, TOP_PREC_FP64, TOP_PREC_MIXED,
+                   TopGpuError, check, last_error, lib)
+
+_INT_ARRAYS = {"eleMapBack", "eleMapForward", "eNodMat", "nodMapBack", "nodMapForward", "nodesOnBoundary",
+               "elementsOnBoundary", "elementUpwardMap", "transferMat", "solidNodeMapCoarser2Finer",
+               "mapUniqueKes", "eleWithFixedDOFs", "fixingCond"}
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Mesh:
+    """Voxel FEA model: mesh hierarchy, element matrices, boundary conditions."""
+
+    def __init__(self, mask, control=20000, nu=0.3, cell=None, super_element=0):
+        mask = np.asarray(mask, dtype=bool)
+        if mask.ndim != 3:
+            raise ValueError("mask must be a 3-D logical array (nely x nelx x nelz)")
+        ny, nx, nz = mask.shape
+        self.shape = (ny, nx, nz)
+        if cell is None:
+            cell = 1.0 / nx      # logical-array models: cellSize_ = 1/nelx (TOP_GPU.m:61, 392)
+        self._mask = np.asfortranarray(mask.astype(np.uint8))
+        h = C.c_void_p()
+        check(lib().top_mesh_create(_p(self._mask), ny, nx, nz, control, nu, cell, super_element, C.byref(h)),
+              "top_mesh_create")
+        self._h = h
+        self.super_element = super_element
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().top_mesh_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        out = np.zeros(1 + 8 * 16, dtype=np.int64)
+        check(lib().top_mesh_info(self._h, _p(out), out.size), "top_mesh_info")
+        nl = int(out[0])
+        levels = []
+        for l in range(nl):
+            v = out[1 + 8 * l: 9 + 8 * l]
+            levels.append(dict(resX=int(v[0]), resY=int(v[1]), resZ=int(v[2]), spanWidth=int(v[3]),
+                               numElements=int(v[4]), numNodes=int(v[5]), intermediateNumNodes=int(v[6]),
+                               nUnique=int(v[7])))
+        return levels
+
+    @property
+    def numLevels(self):
+        return len(self.info())
+
+    def get(self, level, name):
+        n = C.c_int64()
+        check(lib().top_mesh_get(self._h, level, name.encode(), None, 0, C.byref(n)), "top_mesh_get")
+        dt = np.int32 if name in _INT_ARRAYS else np.float64
+        a = np.zeros(n.value, dtype=dt)
+        check(lib().top_mesh_get(self._h, level, name.encode(), _p(a), a.size, None), "top_mesh_get")
+        return a
+
+    def apply_optcase(self, opt):
+        check(lib().top_mesh_apply_optcase(self._h, opt), "top_mesh_apply_optcase")
+
+    def apply_bc(self, fixing, loads, weights=None):
+        fixing = np.ascontiguousarray(fixing, dtype=np.float64)
+        loads = [np.ascontiguousarray(l, dtype=np.float64) for l in loads]
+        n = np.array([len(l) for l in loads], dtype=np.int64)
+        ptrs = (C.c_void_p * len(loads))(*[l.ctypes.data for l in loads])
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        check(lib().top_mesh_apply_bc(self._h, len(fixing), _p(fixing), len(loads), _p(n), ptrs,
+                                      None if w is None else _p(w)), "top_mesh_apply_bc")
+
+
+class Solver:
+    """One voxel model resident on the GPU (current CUDA device)."""
+
+    def __init__(self, mesh: Mesh, E0=1.0, Emin=1e-6, penal=3.0, tol=1e-3, maxIT=800, omega=0.6,
+                 mixed=False, outer_fp32=False):
+        self.mesh = mesh
+        p = SolverParams(E0=E0, Emin=Emin, penal=penal, tol=tol, maxIT=maxIT, omega=omega,
+                         precision=TOP_PREC_MIXED if mixed else TOP_PREC_FP64, outerFP32=int(bool(outer_fp32)))
+        self.params = p
+        torch.cuda.init()
+        h = C.c_void_p()
+        check(lib().top_solver_create(mesh.handle, C.byref(p), C.byref(h)), "top_solver_create")
+        self._h = h
+        sz = np.zeros(3, dtype=np.int64)
+        check(lib().top_solver_sizes(self._h, _p(sz)), "top_solver_sizes")
+        self.numLevels, self.nLoads, self.numDOFs = (int(v) for v in sz)
+        self.levels = mesh.info()
+        self.set_stream(torch.cuda.current_stream())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().top_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        check(lib().top_solver_set_stream(self._h, C.c_void_p(stream.cuda_stream)), "top_solver_set_stream")
+
+    @staticmethod
+    def _dev(t, n=None, dtype=torch.float64):
+        if not isinstance(t, torch.Tensor):
+            t = torch.as_tensor(np.asarray(t), dtype=dtype)
+        t = t.to(device="cuda", dtype=dtype).contiguous()
+        if n is not None and t.numel() != n:
+            raise ValueError("expected %d entries, got %d" % (n, t.numel()))
+        return t
+
+    def set_modulus(self, E):
+        E = self._dev(E, self.levels[0]["numElements"])
+        check(lib().top_solver_set_modulus(self._h, E.data_ptr(), 1), "top_solver_set_modulus")
+
+    def set_density(self, x):
+        x = self._dev(x, self.levels[0]["numElements"])
+        check(lib().top_solver_set_density(self._h, x.data_ptr(), 1), "top_solver_set_density")
+
+    def assemble(self):
+        check(lib().top_solver_assemble(self._h), "top_solver_assemble")
+
+    def matvec(self, level, u, fp32=False):
+        n = 3 * self.levels[level]["numNodes"]
+        u = self._dev(u, n)
+        y = torch.zeros(n, dtype=torch.float64, device="cuda")
+        check(lib().top_solver_matvec(self._h, level, u.data_ptr(), y.data_ptr(), int(fp32)), "top_solver_matvec")
+        return y
+
+    def vcycle(self, r):
+        r = self._dev(r, self.numDOFs)
+        z = torch.zeros_like(r)
+        check(lib().top_solver_vcycle(self._h, r.data_ptr(), z.data_ptr()), "top_solver_vcycle")
+        return z
+
+    def restrict(self, ii, r):
+        r = self._dev(r, 3 * self.levels[ii - 1]["numNodes"])
+        out = torch.zeros(3 * self.levels[ii]["numNodes"], dtype=torch.float64, device="cuda")
+        check(lib().top_solver_restrict(self._h, ii, r.data_ptr(), out.data_ptr()), "top_solver_restrict")
+        return out
+
+    def interpolate(self, ii, x):
+        x = self._dev(x, 3 * self.levels[ii]["numNodes"])
+        out = torch.zeros(3 * self.levels[ii - 1]["numNodes"], dtype=torch.float64, device="cuda")
+        check(lib().top_solver_interpolate(self._h, ii, x.data_ptr(), out.data_ptr()), "top_solver_interpolate")
+        return out
+
+    def diag(self, level):
+        out = torch.zeros(3 * self.levels[level]["numNodes"], dtype=torch.float64, device="cuda")
+        check(lib().top_solver_get_diag(self._h, level, out.data_ptr()), "top_solver_get_diag")
+        return out
+
+    def Ks(self, level):
+        ne = self.levels[level]["numElements"]
+        out = torch.zeros(576 * ne, dtype=torch.float64, device="cuda")
+        check(lib().top_solver_get_ks(self._h, level, out.data_ptr()), "top_solver_get_ks")
+        return out
+
+    def pcg(self, load_case=0, U=None, b=None, raise_on_maxit=False):
+        """Solving_PCG on load case k (or an explicit rhs b); U is the warm start.
+
+        Returns (U, its, relres).  Reaching maxIT prints the reference's warning
+        (TOP_GPU.m:656-659) unless raise_on_maxit is set.
+        """
+        warm = U is not None
+        U = torch.zeros(self.numDOFs, dtype=torch.float64, device="cuda") if U is None else self._dev(U, self.numDOFs).clone()
+        its, res = C.c_int(0), C.c_double(0)
+        if b is None:
+            st = lib().top_solver_pcg(self._h, load_case, U.data_ptr(), int(warm), C.byref(its), C.byref(res))
+        else:
+            b = self._dev(b, self.numDOFs)
+            st = lib().top_solver_pcg_rhs(self._h, b.data_ptr(), U.data_ptr(), int(warm), C.byref(its), C.byref(res))
+        if st == TOP_ERR_NOT_CONVERGED and not raise_on_maxit:
+            print("Warning: Exceed the maximum iterate numbers")
+            print("The iterative process stops at residual = %10.4f" % res.value)
+        elif st != TOP_OK:
+            raise TopGpuError(st, "Solving_PCG", last_error())
+        return U, its.value, res.value
+
+    def unit_compliance(self, U):
+        U = self._dev(U, self.numDOFs)
+        ce = torch.zeros(self.levels[0]["numElements"], dtype=torch.float64, device="cuda")
+        check(lib().top_solver_unit_compliance(self._h, U.data_ptr(), ce.data_ptr()), "top_solver_unit_compliance")
+        return ce
