@@ -78,6 +78,21 @@ int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void *eleModulu
                            int64_t nElem, int nCh, int64_t nFine, int64_t nUnique,
                            int dtype, void *stream);
 
+/* Allocation-free top_assemble_ks_level2 (no counterpart in the reference):
+ * same arguments and results, but it never calls cudaMalloc/cudaFree.  For
+ * callers that cannot let a library allocate device memory mid-call -- a MEX
+ * gateway under MATLAB's gpuArray memory pool, or an application that
+ * reserves its memory up front and must avoid the device synchronisation of
+ * cudaMalloc/cudaFree.  Its FP64 scratch is a fixed device array (~311 KB per
+ * GPU, held until exit); nCh is limited to 64 (TOP_ERR_SHAPE above that).
+ * The first call on a device resolves the array's address (make it before
+ * any stream capture); concurrent calls on one device race -- serialise them. */
+int top_assemble_ks_level2_noalloc(void *Ks, const int32_t *upMap, const void *eleModulus,
+                                   const void *K0, const void *Pch, const int32_t *mapUnique,
+                                   const void *uniqueFree, const void *uniqueFixed,
+                                   int64_t nElem, int nCh, int64_t nFine, int64_t nUnique,
+                                   int dtype, void *stream);
+
 /* assembleKs_higherLevel_inplace(d_Ks, d_upMap, d_KsPrev, d_Psub)
  *   (assembleKs_higherLevel_inplace.cu:134-217) */
 int top_assemble_ks_higher(void *Ks, const int32_t *upMap, const void *KsPrev,

@@ -61,6 +61,7 @@ SIGNATURES = {
     "top_scatter": (_int, [_vp, _vp, _vp, _i64, _i64, _int, _vp]),
     "top_scatter_accum3": (_int, [_vp, _vp, _i64, _vp, _i64, _int, _vp]),
     "top_assemble_ks_level2": (_int, [_vp] * 8 + [_i64, _int, _i64, _i64, _int, _vp]),
+    "top_assemble_ks_level2_noalloc": (_int, [_vp] * 8 + [_i64, _int, _i64, _i64, _int, _vp]),
     "top_assemble_ks_higher": (_int, [_vp] * 4 + [_i64, _int, _i64, _int, _vp]),
     "top_assemble_ks_level2_super": (_int, [_vp] * 8 + [_i64, _int, _i64, _i64, _int, _vp]),
     "top_mesh_create": (_int, [_vp, _int, _int, _int, _int, _dbl, _dbl, _int, _vp]),

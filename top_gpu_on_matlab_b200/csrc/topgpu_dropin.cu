@@ -3,6 +3,7 @@
 // gateways (see include/topgpu.h for the file:line each one replaces).
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 #include "topgpu_kernels.cuh"
 
 using namespace topgpu;
@@ -307,5 +308,96 @@ extern "C" int top_assemble_ks_level2_super(void *Ks, const int32_t *upMap, cons
                               (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed}, NoSkip{}, 0);
     TOP_CUDA_CHECK(cudaGetLastError(), N);
     TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // ..._superEle_inplace.cu:313
+    return TOP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of top_assemble_ks_level2.
+//
+// Some callers cannot let this library allocate device memory during a
+// call: a MEX gateway running inside MATLAB, whose gpuArray pool keeps most
+// of the device memory and expects to be the only allocator, and
+// applications that reserve their memory once up front and must not pay the
+// implicit device synchronisation of cudaMalloc/cudaFree inside an
+// optimisation loop.  This entry point takes its scratch (the child matrices
+// Q_s = P_s' K0 P_s and the slot map of the level-2 Galerkin GEMM) from the
+// fixed device arrays below, which every GPU that loads the library holds
+// until the process exits (about 311 KB per device).
+//
+// Limits and behaviour:
+//  * at most kNoAllocMaxChildren (64) children per coarse element -- the
+//    level-2 case of the reference (span 4); larger nCh is rejected with
+//    TOP_ERR_SHAPE before anything runs;
+//  * the first call on a device resolves the arrays' device addresses with
+//    cudaGetSymbolAddress (with that device current); make that first call
+//    before any stream capture on that device;
+//  * all calls share the arrays and each call clears the part it reads, so
+//    calls that run concurrently on the GPU (different streams or threads)
+//    race -- serialise them.
+namespace {
+constexpr int kNoAllocMaxChildren = 64;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_noalloc_Q[576 * kNoAllocMaxChildren];
+static __device__ __align__(256) int32_t g_noalloc_eye[kNoAllocMaxChildren * kNoAllocMaxChildren];
+
+struct NoAllocScratch { double *Q = nullptr; int32_t *eye = nullptr; };
+std::mutex g_noalloc_mu;
+NoAllocScratch g_noalloc_dev[kNoAllocMaxDevices];
+bool g_noalloc_ready[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch(NoAllocScratch *out, const char *N)
+{
+    int dev = 0;
+    TOP_CUDA_CHECK(cudaGetDevice(&dev), N);
+    if (dev < 0 || dev >= kNoAllocMaxDevices) { set_error("%s:CUDA device %d out of range", N, dev); return TOP_ERR_CUDA; }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ready[dev]) {
+        NoAllocScratch s;
+        TOP_CUDA_CHECK(cudaGetSymbolAddress((void **)&s.Q, g_noalloc_Q), N);
+        TOP_CUDA_CHECK(cudaGetSymbolAddress((void **)&s.eye, g_noalloc_eye), N);
+        g_noalloc_dev[dev] = s;
+        g_noalloc_ready[dev] = true;
+    }
+    *out = g_noalloc_dev[dev];
+    return TOP_OK;
+}
+}  // namespace
+
+extern "C" int top_assemble_ks_level2_noalloc(void *Ks, const int32_t *upMap, const void *eleModulus,
+                                              const void *K0, const void *Pch, const int32_t *mapUnique,
+                                              const void *uniqueFree, const void *uniqueFixed,
+                                              int64_t nElem, int nCh, int64_t nFine, int64_t nUnique,
+                                              int dtype, void *stream)
+{
+    const char *N = "assembleKs_level2_inplace";
+    if (dtype != TOP_F32 && dtype != TOP_F64) { set_error("%s:Type d_Ks must be single/double gpuArray.", N); return TOP_ERR_TYPE; }
+    if (nElem < 0 || nCh < 0 || nFine < 0 || nUnique < 0) { set_error("%s:Shape negative size", N); return TOP_ERR_SHAPE; }
+    if (nCh > kNoAllocMaxChildren) {
+        set_error("%s:Shape %d children per coarse element exceed the allocation-free limit of %d", N, nCh, kNoAllocMaxChildren);
+        return TOP_ERR_SHAPE;
+    }
+    if (nElem == 0) return TOP_OK;
+    if (!Ks || !upMap || !eleModulus || !K0 || !Pch) { set_error("%s:Input null pointer", N); return TOP_ERR_ARGS; }
+    const int hasFixed = (nUnique > 0 && mapUnique && uniqueFree && uniqueFixed) ? 1 : 0;
+    cudaStream_t st = S(stream);
+    if (dtype == TOP_F64) {
+        NoAllocScratch sc;
+        int rc = noalloc_scratch(&sc, N);
+        if (rc) return rc;
+        // rows of Q beyond nCh are read by the GEMM (times zero weights): clear all 64
+        TOP_CUDA_CHECK(cudaMemsetAsync(sc.Q, 0, sizeof(double) * 576 * kNoAllocMaxChildren, st), N);
+        rc = assemble_level2_f64((double *)Ks, upMap, (const double *)eleModulus, (const double *)K0,
+                                 (const double *)Pch, mapUnique, (const double *)uniqueFree,
+                                 (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, sc.Q, sc.eye, st);
+        if (rc) { set_error("%s:CUDA launch failed: %s", N, cudaGetErrorString(cudaGetLastError())); return rc; }
+    } else {
+        ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+            (float *)Ks, upMap, nElem, nCh, (const float *)Pch,
+            Level2Child<float>{(const float *)eleModulus, (const float *)K0, mapUnique,
+                               (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed},
+            NoSkip{}, 0);
+    }
+    TOP_CUDA_CHECK(cudaGetLastError(), N);
+    TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);
     return TOP_OK;
 }
