@@ -295,6 +295,28 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_kernels_only(args):
+    """Build the workload's mixed solver, assemble, time a few launches of the
+    level-0 stiffness products (FP64 outer, FP32 smoother) and one V-cycle.
+    Few launches: the command the ncu captures of those kernels run."""
+    import ctypes as C
+    import torch
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    from top_gpu_on_matlab_b200._lib import check, lib
+    mesh = Mesh(np.ones(SHAPE, bool), control=CONTROL)
+    mesh.apply_optcase(1)
+    s = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=True)
+    ne = mesh.info()[0]["numElements"]
+    s.set_density(torch.full((ne,), V0, dtype=torch.float64, device="cuda"))
+    s.assemble()
+    out = {}
+    for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32")):
+        ms = C.c_double(0)
+        check(lib().top_solver_time_kernel(s._h, which, args.steps, 0, C.byref(ms)), "time_kernel")
+        out[key] = ms.value
+    print(json.dumps({"kernels_only": out, "workload": WORKLOAD}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -302,11 +324,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--ref-its", type=int, default=60, help="FP64 iteration count used to scale the CPU sample")
+    ap.add_argument("--ref-its", type=int, default=20, help="FP64 iteration count used to scale the CPU sample")
+    ap.add_argument("--kernels-only", action="store_true", help="time a few launches of the level-0 kernels (profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.kernels_only:
+        run_kernels_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

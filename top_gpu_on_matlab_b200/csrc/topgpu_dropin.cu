@@ -187,14 +187,15 @@ namespace topgpu {
 int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
                         const double *Pch, const int32_t *mapUnique, const double *uFree,
                         const double *uFixed, int64_t nElem, int nCh, int64_t nUnique,
-                        double *Qscratch, int32_t *eyeScratch, cudaStream_t st)
+                        double *Qscratch, int32_t *eyeScratch, cudaStream_t st,
+                        const int32_t *bndList, int64_t nBnd)
 {
     const int hasFixed = (nUnique > 0 && mapUnique && uFree && uFixed) ? 1 : 0;
     // Q_s = P_s^T K0 P_s, one CTA per child slot
     if (nCh > 0) {
         eye_upmap_kernel<<<(nCh * nCh + 255) / 256, 256, 0, st>>>(eyeScratch, nCh);
         ptkp_kernel<double><<<nCh, kPtkpThreads, 0, st>>>(Qscratch, eyeScratch, nCh, nCh, Pch,
-                                                          K0Child<double>{K0}, NoSkip{}, 0);
+                                                          K0Child<double>{K0}, NoSkip{}, 0, nullptr);
     }
     if (nElem == 0) return TOP_OK;
     if (nCh <= kGemmK) {
@@ -204,14 +205,16 @@ int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const
         // exist: Qscratch is sized for 64 slots
         dgemm_k64_kernel<<<grid, 128, kGemmSmem, st>>>(Ks, nElem, 576, 576, Qscratch, 576,
                                                        Level2Row{upMap, E, mapUnique, nElem, nCh, hasFixed});
-        if (hasFixed)
-            ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
+        // children with fixed DOFs: full triple products, accumulated; only the
+        // coarse cells in bndList when the caller knows them (-1: all cells)
+        if (hasFixed && nBnd != 0)
+            ptkp_kernel<double><<<(unsigned)(nBnd > 0 ? nBnd : nElem), kPtkpThreads, 0, st>>>(
                 Ks, upMap, nElem, nCh, Pch,
                 Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed},
-                RegularChild{mapUnique, hasFixed, 1}, 1);
+                RegularChild{mapUnique, hasFixed, 1}, 1, nBnd > 0 ? bndList : nullptr);
     } else {
         ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
-            Ks, upMap, nElem, nCh, Pch, Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed}, NoSkip{}, 0);
+            Ks, upMap, nElem, nCh, Pch, Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed}, NoSkip{}, 0, nullptr);
     }
     return cudaGetLastError() == cudaSuccess ? TOP_OK : TOP_ERR_CUDA;
 }
@@ -221,7 +224,7 @@ int assemble_higher_f64(double *Ks, const int32_t *upMap, const double *KsPrev, 
 {
     if (nElem == 0) return TOP_OK;
     ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(Ks, upMap, nElem, nSub, Psub,
-                                                                  PrevChild<double>{KsPrev}, NoSkip{}, 0);
+                                                                  PrevChild<double>{KsPrev}, NoSkip{}, 0, nullptr);
     return cudaGetLastError() == cudaSuccess ? TOP_OK : TOP_ERR_CUDA;
 }
 }  // namespace topgpu
@@ -247,7 +250,7 @@ extern "C" int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void
         TOP_CUDA_CHECK(cudaMallocAsync(&one, sizeof(int32_t) * (size_t)nCh * nCh + 4, st), N);
         int rc = assemble_level2_f64((double *)Ks, upMap, (const double *)eleModulus, (const double *)K0,
                                      (const double *)Pch, mapUnique, (const double *)uniqueFree,
-                                     (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, Q, one, st);
+                                     (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, Q, one, st, nullptr, -1);
         cudaFreeAsync(Q, st); cudaFreeAsync(one, st);
         if (rc) { set_error("%s:CUDA launch failed: %s", N, cudaGetErrorString(cudaGetLastError())); return rc; }
     } else {
@@ -255,7 +258,7 @@ extern "C" int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void
             (float *)Ks, upMap, nElem, nCh, (const float *)Pch,
             Level2Child<float>{(const float *)eleModulus, (const float *)K0, mapUnique,
                                (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed},
-            NoSkip{}, 0);
+            NoSkip{}, 0, nullptr);
     }
     TOP_CUDA_CHECK(cudaGetLastError(), N);
     TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // assembleKs_level2_inplace.cu:272
@@ -274,10 +277,10 @@ extern "C" int top_assemble_ks_higher(void *Ks, const int32_t *upMap, const void
     cudaStream_t st = S(stream);
     if (dtype == TOP_F64)
         ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>((double *)Ks, upMap, nElem, nSub, (const double *)Psub,
-                                                                      PrevChild<double>{(const double *)KsPrev}, NoSkip{}, 0);
+                                                                      PrevChild<double>{(const double *)KsPrev}, NoSkip{}, 0, nullptr);
     else
         ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>((float *)Ks, upMap, nElem, nSub, (const float *)Psub,
-                                                                     PrevChild<float>{(const float *)KsPrev}, NoSkip{}, 0);
+                                                                     PrevChild<float>{(const float *)KsPrev}, NoSkip{}, 0, nullptr);
     TOP_CUDA_CHECK(cudaGetLastError(), N);
     TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // assembleKs_higherLevel_inplace.cu:209
     return TOP_OK;
@@ -300,12 +303,12 @@ extern "C" int top_assemble_ks_level2_super(void *Ks, const int32_t *upMap, cons
         ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
             (double *)Ks, upMap, nElem, nSub, (const double *)Psub,
             SuperChild<double>{(const double *)Ks0, mapUnique, (const double *)eleModulus,
-                               (const double *)uniqueFree, (const double *)uniqueFixed, hasFixed}, NoSkip{}, 0);
+                               (const double *)uniqueFree, (const double *)uniqueFixed, hasFixed}, NoSkip{}, 0, nullptr);
     else
         ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
             (float *)Ks, upMap, nElem, nSub, (const float *)Psub,
             SuperChild<float>{(const float *)Ks0, mapUnique, (const float *)eleModulus,
-                              (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed}, NoSkip{}, 0);
+                              (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed}, NoSkip{}, 0, nullptr);
     TOP_CUDA_CHECK(cudaGetLastError(), N);
     TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);   // ..._superEle_inplace.cu:313
     return TOP_OK;
@@ -388,14 +391,14 @@ extern "C" int top_assemble_ks_level2_noalloc(void *Ks, const int32_t *upMap, co
         TOP_CUDA_CHECK(cudaMemsetAsync(sc.Q, 0, sizeof(double) * 576 * kNoAllocMaxChildren, st), N);
         rc = assemble_level2_f64((double *)Ks, upMap, (const double *)eleModulus, (const double *)K0,
                                  (const double *)Pch, mapUnique, (const double *)uniqueFree,
-                                 (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, sc.Q, sc.eye, st);
+                                 (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, sc.Q, sc.eye, st, nullptr, -1);
         if (rc) { set_error("%s:CUDA launch failed: %s", N, cudaGetErrorString(cudaGetLastError())); return rc; }
     } else {
         ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
             (float *)Ks, upMap, nElem, nCh, (const float *)Pch,
             Level2Child<float>{(const float *)eleModulus, (const float *)K0, mapUnique,
                                (const float *)uniqueFree, (const float *)uniqueFixed, hasFixed},
-            NoSkip{}, 0);
+            NoSkip{}, 0, nullptr);
     }
     TOP_CUDA_CHECK(cudaGetLastError(), N);
     TOP_CUDA_CHECK(cudaStreamSynchronize(st), N);

@@ -87,48 +87,64 @@ struct Reduce {             // where a fused dot product goes
 
 // ---------------------------------------------------------------------------
 // Inputs of the node kernels: the value of the operand vector at a node.
+// Functors carry one base pointer per component (set on the host), so device
+// code indexes each component with 32-bit in-array offsets.
+template <typename P> struct Comp3 {
+    P p0, p1, p2;
+    Comp3() = default;
+    Comp3(P base, int64_t cs) : p0(base), p1(base + cs), p2(base + 2 * cs) {}
+    __device__ __forceinline__ P operator[](int c) const { return c == 0 ? p0 : (c == 1 ? p1 : p2); }
+};
+
 template <typename T, typename TV>
 struct VecIn {
-    const TV *u; int64_t cs;
-    __device__ __forceinline__ T operator()(int64_t m, int c) const { return T(u[c * cs + m]); }
+    Comp3<const TV *> u;
+    VecIn(const TV *base, int64_t cs) : u(base, cs) {}
+    __device__ __forceinline__ T operator()(int m, int c) const { return T(u[c][m]); }
 };
 // x = omega * invD .* r  (the Jacobi pre-smoothing step, evaluated on the fly)
 template <typename T, typename TR>
 struct JacobiIn {
-    const TR *r; const T *invD; int64_t cs; T omega;
-    __device__ __forceinline__ T operator()(int64_t m, int c) const { return omega * invD[c * cs + m] * T(r[c * cs + m]); }
+    Comp3<const TR *> r; Comp3<const T *> invD; T omega;
+    JacobiIn(const TR *rb, const T *ib, int64_t cs, T om) : r(rb, cs), invD(ib, cs), omega(om) {}
+    __device__ __forceinline__ T operator()(int m, int c) const { return omega * invD[c][m] * T(r[c][m]); }
 };
 
 // Epilogues: what a node kernel does with y = (K u)(node).
 template <typename T, typename TY>
 struct StoreOut {   // y
-    TY *y; int64_t cs;
-    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) y[c * cs + i] = TY(yv[c]); (void)dot; }
+    Comp3<TY *> y;
+    StoreOut(TY *yb, int64_t cs) : y(yb, cs) {}
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
+    { for (int c = 0; c < 3; ++c) y[c][i] = TY(yv[c]); (void)dot; }
 };
 template <typename T, typename TU, typename TY>
 struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
-    TY *y; const TU *u; int64_t cs;
-    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) { y[c * cs + i] = TY(yv[c]); dot += double(u[c * cs + i]) * double(yv[c]); } }
+    Comp3<TY *> y; Comp3<const TU *> u;
+    DotStoreOut(TY *yb, const TU *ub, int64_t cs) : y(yb, cs), u(ub, cs) {}
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
+    { for (int c = 0; c < 3; ++c) { y[c][i] = TY(yv[c]); dot += double(u[c][i]) * double(yv[c]); } }
 };
 template <typename T, typename TR, typename TD>
 struct ResidOut {   // d = r - y
-    const TR *r; TD *d; int64_t cs;
-    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) d[c * cs + i] = TD(T(r[c * cs + i]) - yv[c]); (void)dot; }
+    Comp3<const TR *> r; Comp3<TD *> d;
+    ResidOut(const TR *rb, TD *db, int64_t cs) : r(rb, cs), d(db, cs) {}
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
+    { for (int c = 0; c < 3; ++c) d[c][i] = TD(T(r[c][i]) - yv[c]); (void)dot; }
 };
 // z = x + omega*invD.*(r - y), optionally dot += z . r  (post-smoothing)
 template <typename T, typename TR, typename TZ>
 struct PostSmoothOut {
-    const T *x; const TR *r; const T *invD; TZ *z; int64_t cs; T omega;
-    __device__ __forceinline__ void operator()(int64_t i, const T yv[3], double &dot) const
+    Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega;
+    PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om)
+        : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om) {}
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     {
         for (int c = 0; c < 3; ++c) {
-            const int64_t k = c * cs + i;
-            const T zv = x[k] + omega * invD[k] * (T(r[k]) - yv[c]);
-            z[k] = TZ(zv);
-            dot += double(zv) * double(r[k]);
+            const T rv = T(r[c][i]);
+            const T zv = x[c][i] + omega * invD[c][i] * (rv - yv[c]);
+            z[c][i] = TZ(zv);
+            dot += double(zv) * double(r[c][i]);
         }
     }
 };
@@ -143,12 +159,13 @@ struct PostSmoothOut {
 template <typename T, bool MASK, class In, class Out>
 __device__ __forceinline__ void l0_node(const KeParam<T> &K, const In &in, const Out &out,
                                         const T *__restrict__ E, const uint8_t *__restrict__ flags,
-                                        const Geom &g, int64_t idx, bool valid, T E0, double &dot)
+                                        const Geom &g, int idx, bool valid, T E0, double &dot)
 {
     if (!valid) return;
+    const int PY = g.PY, PL = (int)g.plane;
     T Ee[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) Ee[i] = E[idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i)];
+    for (int i = 0; i < 8; ++i) Ee[i] = E[idx - cdy(i) - PY * cdx(i) - PL * cdz(i)];
     T t[8][3];
 #pragma unroll
     for (int i = 0; i < 8; ++i) t[i][0] = t[i][1] = t[i][2] = T(0);
@@ -158,7 +175,7 @@ __device__ __forceinline__ void l0_node(const KeParam<T> &K, const In &in, const
         for (int dx = -1; dx <= 1; ++dx)
 #pragma unroll
             for (int dy = -1; dy <= 1; ++dy) {
-                const int64_t m = idx + dy + g.PY * dx + g.plane * dz;
+                const int m = idx + dy + PY * dx + PL * dz;
                 T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
                 if (MASK) {
                     const uint8_t fm = flags[m];
@@ -201,7 +218,7 @@ l0_kernel(const KeParam<T> K, In in, Out out, const T *__restrict__ E, const uin
     const int q = blockIdx.x * kNodeThreads + threadIdx.x;
     const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
     const bool valid = Y < g.NY && X < g.NX;
-    const int64_t idx = g.origin + Y + (int64_t)g.PY * X + g.plane * Z;
+    const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
     double dot = 0.0;
     if (tileFixed[blockIdx.x + (int64_t)g.nbx * Z])
         l0_node<T, true>(K, in, out, E, flags, g, idx, valid, E0, dot);
@@ -213,43 +230,52 @@ l0_kernel(const KeParam<T> K, In in, Out out, const T *__restrict__ E, const uin
 // ---------------------------------------------------------------------------
 // Coarse levels: y(node) = sum over incident elements of the node's three
 // rows of the element's Galerkin matrix Ks (packed upper triangle, entry
-// stride CS) times u_e.
+// stride CS) times u_e.  Eight lanes per node, lane i taking incident
+// element i (the node is its local corner i); a shuffle tree adds them up.
+constexpr int kCoarseLanes = 8;
+
 template <typename T, class In, class Out>
 __global__ void __launch_bounds__(kNodeThreads)
 coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, const int *__restrict__ done)
 {
     if (done && *done) return;
-    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
-    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
-    const bool valid = Y < g.NY && X < g.NX;
+    const int64_t gt = (int64_t)blockIdx.x * kNodeThreads + threadIdx.x;
+    const int64_t node = gt / kCoarseLanes;
+    const int i = int(gt % kCoarseLanes);
+    const int64_t nq = (int64_t)g.PY * g.NX * g.NZ;
+    const int64_t nq2 = node < nq ? node : 0;
+    const int Y = int(nq2 % g.PY), X = int((nq2 / g.PY) % g.NX), Z = int(nq2 / ((int64_t)g.PY * g.NX));
+    const bool valid = node < nq && Y < g.NY;
     const int64_t idx = g.origin + Y + (int64_t)g.PY * X + g.plane * Z;
-    double dot = 0.0;
+    T y[3] = {T(0), T(0), T(0)};
     if (valid) {
-        T y[3] = {T(0), T(0), T(0)};
+        const int64_t slot = idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i);
+        const T *ke = Ks + slot;
+        if (ke[g.cs * sym_pack(3 * i, 3 * i)] != T(0)) {       // void element: all zero
 #pragma unroll
-        for (int dz = -1; dz <= 1; ++dz)
+            for (int j = 0; j < 8; ++j) {
+                const int m = (int)(slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j));
+                const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
 #pragma unroll
-            for (int dx = -1; dx <= 1; ++dx)
+                for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int dy = -1; dy <= 1; ++dy) {
-                    const int64_t m = idx + dy + g.PY * dx + g.plane * dz;
-                    const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int jy = cdy(i) + dy, jx = cdx(i) + dx, jz = cdz(i) + dz;
-                        if (jy < 0 || jy > 1 || jx < 0 || jx > 1 || jz < 0 || jz > 1) continue;
-                        const int j = corner_of(jy, jx, jz);
-                        const T *ke = Ks + (idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i));
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-#pragma unroll
-                            for (int d = 0; d < 3; ++d)
-                                y[c] = fma(__ldg(ke + g.cs * sym_pack(3 * i + c, 3 * j + d)), u[d], y[c]);
-                    }
-                }
-        out(idx, y, dot);
+                    for (int d = 0; d < 3; ++d)
+                        y[c] = fma(__ldg(ke + g.cs * sym_pack(3 * i + c, 3 * j + d)), u[d], y[c]);
+            }
+        }
     }
+#pragma unroll
+    for (int o = kCoarseLanes / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[c] += __shfl_down_sync(0xffffffffu, y[c], o, kCoarseLanes);
+    double dot = 0.0;
+    if (valid && i == 0) out((int)idx, y, dot);
     if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
+}
+inline unsigned coarse_blocks(const Geom &g)
+{
+    const int64_t threads = (int64_t)g.PY * g.NX * g.NZ * kCoarseLanes;
+    return (unsigned)((threads + kNodeThreads - 1) / kNodeThreads);
 }
 
 // ---------------------------------------------------------------------------
@@ -258,41 +284,59 @@ coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, cons
 // restriction is its transpose.  (TOP_GPU.m:817-878 express the same
 // operators through an intermediate node set with multiplicity weights; for
 // every active node the two coincide.)
+// One lane group per coarse node (32 lanes for span 4, 8 for span 2): the
+// (2S-1)^2 (z, x) tap columns are dealt out over the group, each lane runs
+// its columns' 2S-1 y taps, the group adds up with shuffles.
+template <int S> struct RestrictLanes { static constexpr int value = (S >= 4) ? 32 : 8; };
+
 template <typename T, int S>
 __global__ void __launch_bounds__(kNodeThreads)
 restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
                 const uint8_t *__restrict__ flagsC, const int *__restrict__ done)
 {
     if (done && *done) return;
-    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
-    const int QY = q % gc.PY, QX = q / gc.PY, QZ = blockIdx.y;
-    if (QY >= gc.NY || QX >= gc.NX) return;
+    constexpr int LPN = RestrictLanes<S>::value, W = 2 * S - 1;
+    const int64_t gt = (int64_t)blockIdx.x * kNodeThreads + threadIdx.x;
+    const int64_t node = gt / LPN;
+    const int lane = int(gt % LPN);
+    const int64_t nq = (int64_t)gc.PY * gc.NX * gc.NZ;
+    const bool inRange = node < nq;
+    const int64_t nq2 = inRange ? node : 0;
+    const int QY = int(nq2 % gc.PY), QX = int((nq2 / gc.PY) % gc.NX), QZ = int(nq2 / ((int64_t)gc.PY * gc.NX));
+    const bool valid = inRange && QY < gc.NY;
     const int64_t ic = gc.origin + QY + (int64_t)gc.PY * QX + gc.plane * QZ;
     T acc[3] = {T(0), T(0), T(0)};
-    if (flagsC[ic] & kActive) {
-        for (int oz = -(S - 1); oz <= S - 1; ++oz) {
-            const int Z = S * QZ + oz;
-            if (Z < 0 || Z >= gf.NZ) continue;
-            const T wz = T(S - (oz < 0 ? -oz : oz)) / T(S);
-            for (int ox = -(S - 1); ox <= S - 1; ++ox) {
-                const int X = S * QX + ox;
-                if (X < 0 || X >= gf.NX) continue;
-                const T wzx = wz * (T(S - (ox < 0 ? -ox : ox)) / T(S));
-                const int64_t base = gf.origin + (int64_t)gf.PY * X + gf.plane * Z;
+    if (valid && (flagsC[ic] & kActive)) {
+        for (int pr = lane; pr < W * W; pr += LPN) {
+            const int oz = pr / W - (S - 1), ox = pr % W - (S - 1);
+            const int Z = S * QZ + oz, X = S * QX + ox;
+            if (Z < 0 || Z >= gf.NZ || X < 0 || X >= gf.NX) continue;
+            const T wzx = (T(S - (oz < 0 ? -oz : oz)) / T(S)) * (T(S - (ox < 0 ? -ox : ox)) / T(S));
+            const int64_t base = gf.origin + (int64_t)gf.PY * X + gf.plane * Z;
 #pragma unroll
-                for (int oy = -(S - 1); oy <= S - 1; ++oy) {
-                    const int Y = S * QY + oy;
-                    if (Y < 0 || Y >= gf.NY) continue;
-                    const T w = wzx * (T(S - (oy < 0 ? -oy : oy)) / T(S));
-                    const int64_t f = base + Y;
+            for (int oy = -(S - 1); oy <= S - 1; ++oy) {
+                const int Y = S * QY + oy;
+                if (Y < 0 || Y >= gf.NY) continue;
+                const T w = wzx * (T(S - (oy < 0 ? -oy : oy)) / T(S));
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) acc[c] = fma(w, rf[c * gf.cs + f], acc[c]);
-                }
+                for (int c = 0; c < 3; ++c) acc[c] = fma(w, rf[c * gf.cs + base + Y], acc[c]);
             }
         }
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
+    for (int o = LPN / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] += __shfl_down_sync(0xffffffffu, acc[c], o, LPN);
+    if (valid && lane == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
+    }
+}
+template <int S>
+inline unsigned restrict_blocks(const Geom &gc)
+{
+    const int64_t threads = (int64_t)gc.PY * gc.NX * gc.NZ * RestrictLanes<S>::value;
+    return (unsigned)((threads + kNodeThreads - 1) / kNodeThreads);
 }
 
 // x_f = base + P x_c, base = omega*invD.*r when r != nullptr (the pre-smoothed

@@ -29,10 +29,11 @@ constexpr int kPtkpThreads = 64;
 template <typename T, class ChildK, class Skip>
 __global__ void __launch_bounds__(kPtkpThreads)
 ptkp_kernel(T *__restrict__ Ks, const int32_t *__restrict__ upMap, int64_t nElem, int nCh,
-            const T *__restrict__ P, ChildK childK, Skip skip, int accumulate)
+            const T *__restrict__ P, ChildK childK, Skip skip, int accumulate,
+            const int32_t *__restrict__ elist)
 {
     __shared__ T sK[576], sP[576], sT[576];
-    const int64_t e = blockIdx.x;
+    const int64_t e = elist ? (int64_t)elist[blockIdx.x] : (int64_t)blockIdx.x;   // optional subset of elements
     const int t = threadIdx.x, rb = (t % 8) * 3, cb = (t / 8) * 3;
     T acc[3][3];
 #pragma unroll

@@ -19,7 +19,8 @@ namespace topgpu {
 int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
                         const double *Pch, const int32_t *mapUnique, const double *uFree,
                         const double *uFixed, int64_t nElem, int nCh, int64_t nUnique,
-                        double *Qscratch, int32_t *eyeScratch, cudaStream_t st);
+                        double *Qscratch, int32_t *eyeScratch, cudaStream_t st,
+                        const int32_t *bndList, int64_t nBnd);
 int assemble_higher_f64(double *Ks, const int32_t *upMap, const double *KsPrev, const double *Psub,
                         int64_t nElem, int nSub, cudaStream_t st);
 
@@ -84,19 +85,29 @@ __global__ void diag_l0_kernel(const KeParam<double> K, const double *__restrict
         inv32[c * g.cs + idx] = on ? float(1.0 / d) : 0.0f;
     }
 }
-// Compact element Ks [576 x Ne] -> packed grid slots (FP64 + FP32)
+// Compact element Ks [576 x Ne] -> packed grid slots (FP64 + FP32), 8
+// elements per block staged through shared memory (coalesced both ways)
+constexpr int kPackE = 8;
 __global__ void pack_ks_kernel(const double *__restrict__ KsC, const int32_t *__restrict__ eleGrid, int64_t Ne,
                                double *__restrict__ P64, float *__restrict__ P32, int64_t cs)
 {
-    const int64_t e = blockIdx.x;
-    const int64_t slot = eleGrid[e];
-    for (int r = threadIdx.x; r < 24; r += blockDim.x)
-        for (int k = r; k < 24; ++k) {
-            const double v = KsC[e * 576 + r + 24 * k];
-            const int p = sym_pack(r, k);
-            if (P64) P64[p * cs + slot] = v;
-            if (P32) P32[p * cs + slot] = float(v);
-        }
+    __shared__ double sK[kPackE * 576];
+    __shared__ int64_t sSlot[kPackE];
+    const int64_t e0 = (int64_t)blockIdx.x * kPackE;
+    const int ne = (int)((Ne - e0) < kPackE ? (Ne - e0) : kPackE);
+    for (int t = threadIdx.x; t < ne * 576; t += blockDim.x) sK[t] = KsC[e0 * 576 + t];
+    if (threadIdx.x < ne) sSlot[threadIdx.x] = eleGrid[e0 + threadIdx.x];
+    __syncthreads();
+    for (int t = threadIdx.x; t < 300 * kPackE; t += blockDim.x) {
+        const int el = t % kPackE, p = t / kPackE;
+        if (el >= ne) continue;
+        int r = 0, base = 0;           // packed index p -> (r, k), r <= k
+        while (base + (24 - r) <= p) { base += 24 - r; ++r; }
+        const int k = r + (p - base);
+        const double v = sK[el * 576 + r + 24 * k];
+        P64[(int64_t)p * cs + sSlot[el]] = v;
+        P32[(int64_t)p * cs + sSlot[el]] = float(v);
+    }
 }
 __global__ void diag_coarse_kernel(const double *__restrict__ P64, Geom g, const uint8_t *__restrict__ flags,
                                    double *__restrict__ diag, double *__restrict__ inv64, float *__restrict__ inv32)
@@ -184,27 +195,42 @@ __global__ void chol_syrk_kernel(double *A, int64_t n, int64_t k0, int kb)
     for (int t = 0; t < kb; ++t) s += A[i + n * (k0 + t)] * A[j + n * (k0 + t)];
     A[i + n * j] -= s;
 }
-// L^{-1}, one thread per column (lower triangular result in W)
+// W = L^{-1}: one CTA per column j, forward substitution in axpy form on a
+// shared-memory copy of the column (each step: w_i /= L_ii, then the rows
+// below subtract L(:,i) w_i -- coalesced column reads of L).
 __global__ void tri_inv_kernel(const double *__restrict__ L, double *__restrict__ W, int64_t n)
 {
-    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    for (int64_t i = 0; i < j; ++i) W[i + n * j] = 0.0;
-    W[j + n * j] = 1.0 / L[j + n * j];
-    for (int64_t i = j + 1; i < n; ++i) {
-        double s = 0;
-        for (int64_t k = j; k < i; ++k) s += L[i + n * k] * W[k + n * j];
-        W[i + n * j] = -s / L[i + n * i];
+    extern __shared__ double w[];
+    const int64_t j = blockIdx.x;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = (i == j) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int64_t i = j; i < n; ++i) {
+        const double wi = w[i] / L[i + n * i];
+        __syncthreads();
+        for (int64_t r = i + 1 + threadIdx.x; r < n; r += blockDim.x) w[r] -= L[r + n * i] * wi;
+        if (threadIdx.x == 0) w[i] = wi;
+        __syncthreads();
     }
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) W[i + n * j] = w[i];
 }
-// A^{-1} = W^T W  (W = L^{-1} lower)
+// A^{-1} = W^T W (W = L^{-1} lower), 16x16 output tiles, coalesced column reads
 __global__ void inv_gram_kernel(const double *__restrict__ W, double *__restrict__ Ainv, int64_t n)
 {
-    const int64_t i = (int64_t)blockIdx.x * 16 + threadIdx.x, j = (int64_t)blockIdx.y * 16 + threadIdx.y;
-    if (i >= n || j >= n) return;
-    double s = 0;
-    for (int64_t k = (i > j ? i : j); k < n; ++k) s += W[k + n * i] * W[k + n * j];
-    Ainv[i + n * j] = s;
+    __shared__ double sA[16][17], sB[16][17];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int64_t i0 = (int64_t)blockIdx.x * 16, j0 = (int64_t)blockIdx.y * 16;
+    double acc = 0;
+    const int64_t k0 = i0 > j0 ? i0 : j0;          // W[k,i] = 0 for k < i
+    for (int64_t kb = k0; kb < n; kb += 16) {
+        const int64_t k = kb + tx;
+        sA[ty][tx] = (k < n && i0 + ty < n) ? W[k + n * (i0 + ty)] : 0.0;
+        sB[ty][tx] = (k < n && j0 + ty < n) ? W[k + n * (j0 + ty)] : 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int t = 0; t < 16; ++t) acc += sA[tx][t] * sB[ty][t];
+        __syncthreads();
+    }
+    if (i0 + tx < n && j0 + ty < n) Ainv[(i0 + tx) + n * (j0 + ty)] = acc;
 }
 // coarsest solve: x_grid = Ainv * r (r gathered from the grid in compact order)
 template <typename T>
@@ -335,6 +361,7 @@ struct top_solver {
     double *Ec = nullptr, *Eg64 = nullptr; float *Eg32 = nullptr;
     int32_t *mapUnique = nullptr; double *uFree = nullptr, *uFixed = nullptr; int64_t nU = 0;
     double *Qs = nullptr; int32_t *eye = nullptr;
+    int32_t *bndList = nullptr; int64_t nBnd = 0;   // level-1 cells with fixed-DOF children
     double *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *v = nullptr, *tmp = nullptr;
     double *b = nullptr;             // [nLoads][3 x cs]
     double *weights = nullptr;
@@ -424,7 +451,7 @@ void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, co
         l0_kernel<T, In, Out><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(
             keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
     else
-        coarse_kernel<T, In, Out><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+        coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
 }
 
 // V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
@@ -445,9 +472,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
         else
             level_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs}, none, done);
         if (lc.span == 4)
-            restrict_kernel<T, 4><<<node_grid(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
+            restrict_kernel<T, 4><<<restrict_blocks<4>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
         else
-            restrict_kernel<T, 2><<<node_grid(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
+            restrict_kernel<T, 2><<<restrict_blocks<2>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
     }
     // coarsest direct solve, FP64
     DevLevel &lc = s->L[nL - 1];
@@ -517,6 +544,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         d.g = make_geom(d.ny, d.nx, d.nz);
         d.Ne = M.Ne; d.Nn = M.Nn; d.ng = d.g.cs - 2 * kMargin;
         const int64_t cs = d.g.cs;
+        if (cs >= (int64_t(1) << 31) - 1) { set_error("top_solver_create: level %d grid too large for 32-bit in-array indices", l); top_solver_destroy(s); return TOP_ERR_SHAPE; }
         // host-side flags, node and element maps
         std::vector<uint8_t> fl(cs, 0);
         std::vector<int32_t> ng(M.Nn), eg(M.Ne);
@@ -604,6 +632,21 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     if (!s->KeDev || !s->Ec || !s->Eg64 || !s->Eg32 || !s->mapUnique || !s->uFree || !s->uFixed || !s->P4 || !s->P2 || !s->Qs || !s->eye)
         return fail("out of device memory");
     cudaMemcpy(s->KeDev, M0.Ke, sizeof(double) * 576, cudaMemcpyHostToDevice);
+    if (s->nL > 1) {   // coarse level-1 cells that own a child with fixed DOFs
+        const MeshLevel &M1 = mesh->L[1];
+        std::vector<int32_t> bl;
+        for (int64_t e = 0; e < M1.Ne; ++e)
+            for (int c = 0; c < 64; ++c) {
+                const int32_t f = M1.elementUpwardMap[e + M1.Ne * c];
+                if (f > 0 && mesh->mapUniqueKes[f - 1] > 0) { bl.push_back(int32_t(e)); break; }
+            }
+        s->nBnd = (int64_t)bl.size();
+        if (s->nBnd) {
+            s->bndList = s->dalloc<int32_t>(bl.size());
+            if (!s->bndList) return fail("out of device memory");
+            cudaMemcpy(s->bndList, bl.data(), sizeof(int32_t) * bl.size(), cudaMemcpyHostToDevice);
+        }
+    }
     cudaMemcpy(s->mapUnique, mesh->mapUniqueKes.data(), sizeof(int32_t) * M0.Ne, cudaMemcpyHostToDevice);
     cudaMemcpy(s->uFree, mesh->uniqueKesFree.data(), sizeof(double) * 576 * s->nU, cudaMemcpyHostToDevice);
     {
@@ -735,12 +778,12 @@ extern "C" int top_solver_assemble(top_solver *s)
         int rc;
         if (l == 1)
             rc = assemble_level2_f64(d.KsC, d.upMap, s->Ec, s->KeDev, s->P4, s->mapUnique, s->uFree, s->uFixed,
-                                     d.Ne, 64, s->nU, s->Qs, s->eye, st);
+                                     d.Ne, 64, s->nU, s->Qs, s->eye, st, s->bndList, s->nBnd);
         else
             rc = assemble_higher_f64(d.KsC, d.upMap, s->L[l - 1].KsC, s->P2, d.Ne, 8, st);
         if (rc) { set_error("top_solver_assemble: Galerkin kernel failed"); return rc; }
         if (l < s->nL - 1) {
-            pack_ks_kernel<<<(unsigned)d.Ne, 32, 0, st>>>(d.KsC, d.eleGrid, d.Ne, d.KsP64, d.KsP32, d.g.cs);
+            pack_ks_kernel<<<(unsigned)((d.Ne + kPackE - 1) / kPackE), 256, 0, st>>>(d.KsC, d.eleGrid, d.Ne, d.KsP64, d.KsP32, d.g.cs);
             diag_coarse_kernel<<<node_grid(d.g), kNodeThreads, 0, st>>>(d.KsP64, d.g, d.flags, d.diag, d.invD64, d.invD32);
         }
     }
@@ -763,7 +806,11 @@ extern "C" int top_solver_assemble(top_solver *s)
             chol_syrk_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Ac, n, k0, kb);
         }
     }
-    tri_inv_kernel<<<(unsigned)((n + 63) / 64), 64, 0, st>>>(s->Ac, s->Wc, n);
+    {
+        const size_t sm = sizeof(double) * (size_t)n;   // one column of W per CTA
+        if (sm > 48 * 1024) cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        tri_inv_kernel<<<(unsigned)n, 256, sm, st>>>(s->Ac, s->Wc, n);
+    }
     {
         dim3 gs((unsigned)((n + 15) / 16), (unsigned)((n + 15) / 16));
         inv_gram_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Wc, s->Ainv, n);
@@ -818,8 +865,8 @@ extern "C" int top_solver_restrict(top_solver *s, int ii, const double *rF, doub
     DevLevel &f = s->L[ii - 1], &c = s->L[ii];
     CK(cudaMemsetAsync(f.x64 - kMargin, 0, sizeof(double) * 3 * f.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(f.Nn), 256, 0, s->st>>>(rF, f.x64, f.nodeGrid, f.Nn, f.g.cs);
-    if (c.span == 4) restrict_kernel<double, 4><<<node_grid(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
-    else restrict_kernel<double, 2><<<node_grid(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
+    if (c.span == 4) restrict_kernel<double, 4><<<restrict_blocks<4>(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
+    else restrict_kernel<double, 2><<<restrict_blocks<2>(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
     grid_to_compact_kernel<double, double><<<nb256(c.Nn), 256, 0, s->st>>>(c.t64, rC, c.nodeGrid, c.Nn, c.g.cs);
     CKL();
     CK(cudaStreamSynchronize(s->st));
