@@ -206,6 +206,36 @@ int top_solver_pcg_rhs(top_solver *s, const double *b, double *U, int warm, int 
  * (TopOpti_ComputeUnitCompliance, TOP_GPU.m:580-600), U device [3Nn x nLoads]. */
 int top_solver_unit_compliance(top_solver *s, const double *U, double *ce);
 
+/* ---- the optimisation steps around the solve (device resident) ---- */
+typedef struct {
+    double V0;       /* target volume fraction                                */
+    double rMin;     /* filter radius in cells                                */
+    int    nLoop;    /* maximum optimisation iterations                       */
+    int    ft;       /* 0 none, 1 sensitivity filter, 2 PDE density filter    */
+} top_opt_params;
+typedef struct {     /* one optimisation iteration (TOP_GPU.m:279-291)         */
+    double c, vol, sharp, cons, change;
+    int    pcgIts;
+    double msAssemble, msSolve, msOpt, msFilter, msTotal;   /* tHist columns */
+} top_opt_record;
+
+/* PDE (Helmholtz) filter of TOP_GPU.m:880-1031 on element vectors (device,
+ * compact element order): nodal 8x8 kernel, Jacobi-preconditioned CG to
+ * tol/10; its may be NULL. */
+int top_solver_filter_setup(top_solver *s, double rMin);
+int top_solver_filter(top_solver *s, const double *src, double *tar, int *its);
+/* The optimisation loop of TOP_GPU.m:141-292 on the device: opt_begin runs
+ * the fully solid solve (cSolid) and sets x = xPhys = V0; each opt_step is
+ * one iteration (SIMP, assembly, warm-started PCG per load case,
+ * sensitivities, filter, OC bisection, xPhys); optimize loops until
+ * nLoop / change <= 1e-4 / sharpness <= 0.01.  Designs are device arrays. */
+int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, double *cSolid);
+int top_solver_opt_step(top_solver *s, top_opt_record *rec);
+int top_solver_opt_state(top_solver *s, int *loop, double *change, double *sharpness);
+int top_solver_get_design(top_solver *s, double *xPhys, double *x);
+int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysOut,
+                        top_opt_record *hist, int *nIter, double *cSolid);
+
 /* Kernel timing with CUDA events on the solver's stream (no host copies):
  * which = 0 level-0 K*u FP64, 1 level-0 K*u FP32, 2 one V-cycle,
  * 3 level-1 K*u FP32; L2 is flushed by writing flushBytes before each launch.

@@ -52,6 +52,16 @@ class SolverParams(C.Structure):
     ]
 
 
+class OptParams(C.Structure):
+    _fields_ = [("V0", C.c_double), ("rMin", C.c_double), ("nLoop", C.c_int), ("ft", C.c_int)]
+
+
+class OptRecord(C.Structure):
+    _fields_ = [("c", C.c_double), ("vol", C.c_double), ("sharp", C.c_double), ("cons", C.c_double),
+                ("change", C.c_double), ("pcgIts", C.c_int), ("msAssemble", C.c_double), ("msSolve", C.c_double),
+                ("msOpt", C.c_double), ("msFilter", C.c_double), ("msTotal", C.c_double)]
+
+
 _vp, _i32p, _i64, _int, _dbl = C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_double
 
 SIGNATURES = {
@@ -87,6 +97,13 @@ SIGNATURES = {
     "top_solver_unit_compliance": (_int, [_vp, _vp, _vp]),
     "top_solver_sizes": (_int, [_vp, _vp]),
     "top_solver_time_kernel": (_int, [_vp, _int, _int, _i64, _vp]),
+    "top_solver_filter_setup": (_int, [_vp, _dbl]),
+    "top_solver_filter": (_int, [_vp, _vp, _vp, _vp]),
+    "top_solver_opt_begin": (_int, [_vp, _vp, _vp]),
+    "top_solver_opt_step": (_int, [_vp, _vp]),
+    "top_solver_opt_state": (_int, [_vp, _vp, _vp, _vp]),
+    "top_solver_get_design": (_int, [_vp, _vp, _vp]),
+    "top_solver_optimize": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _LIB = None

@@ -1,0 +1,661 @@
+// topgpu_opt.cu -- the optimisation steps either side of the FEA solve, on
+// the device: element energies and sensitivities (TOP_GPU.m:580-600,
+// 168-209), the PDE density/sensitivity filter (880-1031), the OC update
+// with bisection (232-253) and the loop that ties them to the solver
+// (141-292).
+#include <cuda_runtime.h>
+#include <cooperative_groups.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+#include "topgpu_kernels.cuh"
+#include "topgpu_solver_impl.cuh"
+
+namespace cg = cooperative_groups;
+using namespace topgpu;
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e__ = (call);                                                                \
+        if (e__ != cudaSuccess) { set_error("top_opt: CUDA error %d: %s", (int)e__, cudaGetErrorString(e__)); return TOP_ERR_CUDA; } \
+    } while (0)
+
+namespace topgpu {
+
+struct OptScalars {          // device-side scalars of one optimisation iteration
+    double cObj, vol, sharp, change, lmid, sumE, fval, pad;
+};
+
+struct FilterState {
+    bool ready = false;
+    double rMin = 0;
+    KeParam<double> KEF{};   // 8x8 in k[0..63], col-major
+    double *act = nullptr;   // element activity on the level-0 element slots (1/0)
+    double *invD = nullptr;  // Jacobi of the filter operator, node grid
+    double *rhs = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *v = nullptr, *eg = nullptr;
+    PcgState *st = nullptr;
+};
+
+struct OptState {
+    bool begun = false;
+    top_opt_params prm{};
+    double cSolid = 0;
+    int loop = 0;
+    double change = 1.0, sharp = 1.0;
+    double *xd = nullptr, *xPhys = nullptr, *xnew = nullptr, *dc = nullptr, *dv = nullptr, *ce = nullptr, *tmp = nullptr;
+    double *U = nullptr;     // [nLoads][3 x cs] grid displacement fields (warm starts)
+    OptScalars *sc = nullptr, *hsc = nullptr;
+    double *ocPartials = nullptr; int ocBlocks = 0;
+};
+
+}  // namespace topgpu
+
+namespace {
+
+inline int vb(int64_t n) { return (int)((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096); }
+
+// ---- PDE filter --------------------------------------------------------------
+// Nodal Helmholtz kernel of the reference (TOP_GPU.m:888-920): KEF0 sums the
+// products of the natural-coordinate shape derivatives over the 2x2x2 Gauss
+// points (no Jacobian, unit weights), KEF1 is the lumped-weight mass
+// (weights 1/8); iKEF = (rMin/(2*sqrt 3))^2 KEF0 + KEF1.  Local node order
+// (s,t,p) = (-1,-1,-1),(1,-1,-1),(1,1,-1),(-1,1,-1), then p = +1.
+void filter_kernel_matrix(double rMin, double *K)
+{
+    static const int sg[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1}, {-1, -1, 1}, {1, -1, 1}, {1, 1, 1}, {-1, 1, 1}};
+    const double g = 1.0 / std::sqrt(3.0);
+    double K0[64] = {0}, K1[64] = {0};
+    for (int q = 0; q < 8; ++q) {
+        const double pt[3] = {sg[q][0] * g, sg[q][1] * g, sg[q][2] * g};
+        double N[8], dN[8][3];
+        for (int a = 0; a < 8; ++a) {
+            double f[3], df[3];
+            for (int k = 0; k < 3; ++k) { f[k] = 1.0 + sg[a][k] * pt[k]; df[k] = sg[a][k]; }
+            N[a] = 0.125 * f[0] * f[1] * f[2];
+            dN[a][0] = 0.125 * df[0] * f[1] * f[2];
+            dN[a][1] = 0.125 * f[0] * df[1] * f[2];
+            dN[a][2] = 0.125 * f[0] * f[1] * df[2];
+        }
+        for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b) {
+                K0[a + 8 * b] += dN[a][0] * dN[b][0] + dN[a][1] * dN[b][1] + dN[a][2] * dN[b][2];
+                K1[a + 8 * b] += N[a] * (1.0 / 8.0) * N[b];
+            }
+    }
+    const double iR = rMin / 2.0 / std::sqrt(3.0);    // element size 1 (TOP_GPU.m:918)
+    for (int t = 0; t < 64; ++t) K[t] = iR * iR * K0[t] + K1[t];
+}
+
+// The filter's local node a sits at (s,t,p); the solver's element corner j at
+// (dy,dx,dz).  Both are the same eight nodes of the voxel (TOP_GPU.m:2031-2040
+// numbering); the filter reuses the element node order of eNodMat.
+__global__ void filter_activity_kernel(const int32_t *__restrict__ eleGrid, int64_t Ne, double *__restrict__ act)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < Ne) act[eleGrid[e]] = 1.0;
+}
+__global__ void filter_diag_kernel(const KeParam<double> K, const double *__restrict__ act, Geom g,
+                                   const uint8_t *__restrict__ flags, double *__restrict__ invD)
+{
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    if (Y >= g.NY || X >= g.NX) return;
+    const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
+    double d = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) d += act[idx - cdy(i) - g.PY * cdx(i) - (int)g.plane * cdz(i)] * K.k[9 * i];
+    invD[idx] = (flags[idx] & kActive) && d != 0.0 ? 1.0 / d : 0.0;
+}
+// y = A_filter x (+ dot x.y), node-centric over the 8 incident elements
+__global__ void __launch_bounds__(kNodeThreads)
+filter_apply_kernel(const KeParam<double> K, const double *__restrict__ act, const double *__restrict__ x,
+                    double *__restrict__ y, Geom g, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    const bool valid = Y < g.NY && X < g.NX;
+    const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
+    const int PY = g.PY, PL = (int)g.plane;
+    double dot = 0.0;
+    if (valid) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int slot = idx - cdy(i) - PY * cdx(i) - PL * cdz(i);
+            const double a = act[slot];
+            double t = 0.0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) t = fma(K.k[i + 8 * j], x[slot + cdy(j) + PY * cdx(j) + PL * cdz(j)], t);
+            s = fma(a, t, s);
+        }
+        y[idx] = s;
+        dot = x[idx] * s;
+    }
+    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
+}
+// element values (compact) -> element slots
+__global__ void elem_to_slots_kernel(const double *__restrict__ src, const int32_t *__restrict__ eleGrid,
+                                     int64_t Ne, double scale, double *__restrict__ dst)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < Ne) dst[eleGrid[e]] = src[e] * scale;
+}
+// nodal rhs: sum of the (pre-scaled) values of the incident elements (TOP_GPU.m:975-996)
+__global__ void slots_to_nodes_kernel(const double *__restrict__ eg, Geom g, const uint8_t *__restrict__ flags,
+                                      double *__restrict__ rhs)
+{
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    if (Y >= g.NY || X >= g.NX) return;
+    const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
+    double s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += eg[idx - cdy(i) - g.PY * cdx(i) - (int)g.plane * cdz(i)];
+    rhs[idx] = (flags[idx] & kActive) ? s : 0.0;
+}
+// node -> element mean (TOP_GPU.m:1004-1005)
+__global__ void nodes_to_elem_kernel(const double *__restrict__ xn, const int32_t *__restrict__ eleGrid, Geom g,
+                                     int64_t Ne, double *__restrict__ out)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ne) return;
+    const int slot = eleGrid[e];
+    double s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) s += xn[slot + cdy(j) + g.PY * cdx(j) + (int)g.plane * cdz(j)];
+    out[e] = s * (1.0 / 8.0);
+}
+// scalar PCG pieces (one component)
+__global__ void fpcg_init_kernel(const double *__restrict__ b, double *__restrict__ x, double *__restrict__ r,
+                                 double *__restrict__ z, double *__restrict__ p, const double *__restrict__ invD,
+                                 int64_t n, Reduce bb)
+{   // x = 0, r = b, z = M r, p = z; ||b||^2
+    double s1 = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double bi = b[i], zi = invD[i] * bi;
+        x[i] = 0.0; r[i] = bi; z[i] = zi; p[i] = zi;
+        s1 += bi * bi;
+    }
+    block_sum_to<256>(s1, bb.partials, bb.counter, bb.result);
+}
+__global__ void fpcg_update_kernel(double *__restrict__ x, double *__restrict__ r, double *__restrict__ z,
+                                   const double *__restrict__ p, const double *__restrict__ v,
+                                   const double *__restrict__ invD, int64_t n, PcgState *st, Reduce rr)
+{   // x += l p ; r -= l v ; z = M r ; ||r||^2 (rho from z.r in a second pass)
+    if (st->done) return;
+    const double l = st->rho / st->pv;
+    double s = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += l * p[i];
+        const double ri = r[i] - l * v[i];
+        r[i] = ri;
+        z[i] = invD[i] * ri;
+        s += ri * ri;
+    }
+    block_sum_to<256>(s, rr.partials, rr.counter, rr.result);
+}
+__global__ void fpcg_zr_kernel(const double *__restrict__ z, const double *__restrict__ r, int64_t n, PcgState *st, Reduce red)
+{
+    if (st->done) return;
+    double s = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += z[i] * r[i];
+    block_sum_to<256>(s, red.partials, red.counter, red.result);
+}
+__global__ void fpcg_check_kernel(PcgState *st)
+{   // same stopping rule as Solving_PCG (TOP_GPU.m:637-649)
+    if (st->done) return;
+    st->its += 1;
+    const double res = sqrt(st->rr) / st->normB;
+    st->resnorm = res;
+    if (!isfinite(res)) { st->status = TOP_ERR_NAN; st->done = 1; return; }
+    if (res < st->tol) { st->done = 1; return; }
+    if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
+    st->rhoOld = st->rho;
+}
+__global__ void fpcg_p_kernel(double *__restrict__ p, const double *__restrict__ z, int64_t n, const PcgState *st)
+{
+    if (st->done) return;
+    const double beta = st->rho / st->rhoOld;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+__global__ void fpcg_start_kernel(PcgState *st, double tol, int maxIT)
+{
+    st->normB = sqrt(st->normB);
+    st->tol = tol; st->maxIT = maxIT; st->its = 0; st->status = 0;
+    st->done = st->normB == 0.0 ? 1 : 0;
+}
+
+// ---- sensitivities ----------------------------------------------------------
+// ce_e = sum_k w_k u_ke' Ke u_ke; dc = -p (E0-Emin) x^(p-1) ce / cSolid; dv = 1;
+// sums: cObj = sum E_e ce_e / cSolid, sumX = sum xPhys (TOP_GPU.m:191-199)
+__global__ void sensitivity_kernel(const KeParam<double> K, const double *__restrict__ U, int64_t ustride, int nLoads,
+                                   const double *__restrict__ w, const int32_t *__restrict__ eleGrid, int64_t Ne, Geom g,
+                                   const double *__restrict__ xPhys, const double *__restrict__ Ec,
+                                   double E0, double Emin, double penal, double cSolid,
+                                   double *__restrict__ ce, double *__restrict__ dc, double *__restrict__ dv,
+                                   Reduce redC)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double cpart = 0;
+    if (e < Ne) {
+        const int slot = eleGrid[e];
+        double acc = 0;
+        for (int k = 0; k < nLoads; ++k) {
+            const double *u = U + k * ustride;
+            double ue[24];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) ue[3 * j + c] = u[c * g.cs + slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j)];
+            double s = 0;
+#pragma unroll
+            for (int a = 0; a < 24; ++a) {
+                double t = 0;
+#pragma unroll
+                for (int b = 0; b < 24; ++b) t = fma(K.k[a + 24 * b], ue[b], t);
+                s = fma(t, ue[a], s);
+            }
+            acc += s * w[k];
+        }
+        if (ce) ce[e] = acc;
+        const double cn = cSolid > 0 ? acc / cSolid : acc;
+        if (dc) {
+            const double x = xPhys[e];
+            dc[e] = -(penal * (E0 - Emin) * pow(x, penal - 1.0)) * cn;
+            dv[e] = 1.0;
+        }
+        cpart = Ec[e] * cn;
+    }
+    if (redC.result) block_sum_to<256>(cpart, redC.partials, redC.counter, redC.result);
+}
+__global__ void sum_kernel(const double *__restrict__ a, int64_t n, int mode, Reduce red)
+{   // mode 0: sum a ; mode 1: sum a(1-a)
+    double s = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += mode ? a[i] * (1.0 - a[i]) : a[i];
+    block_sum_to<256>(s, red.partials, red.counter, red.result);
+}
+__global__ void mul_kernel(const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ c, int64_t n)
+{ for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) c[i] = a[i] * b[i]; }
+__global__ void div_floor_kernel(const double *__restrict__ a, const double *__restrict__ x, double *__restrict__ c, int64_t n)
+{ for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) c[i] = a[i] / fmax(1e-3, x[i]); }
+
+// ---- OC update: bisection on the Lagrange multiplier (TOP_GPU.m:233-253) ----
+// One cooperative launch; every block reduces the same per-block partials in
+// the same order, so all blocks take identical branches without a broadcast.
+__device__ __forceinline__ double oc_new(double x, double dc, double dv, double lmid, double move)
+{
+    const double cand = x * sqrt(-dc / dv / lmid);
+    // MATLAB's max/min ignore NaN like fmax/fmin
+    return fmax(0.0, fmax(x - move, fmin(1.0, fmin(x + move, cand))));
+}
+__global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc, const double *__restrict__ dv,
+                          int64_t n, double *__restrict__ partials, OptScalars *sc, double move, int maxSteps)
+{
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double red[8];
+    const double fval = sc->fval;
+    double l1 = 0.0, l2 = 1e9, lmid = 0.5 * (l1 + l2);
+    const unsigned nb = gridDim.x;
+    auto block_reduce = [&](double v, bool isMax) -> double {
+        for (int o = 16; o > 0; o >>= 1) {
+            const double w = __shfl_down_sync(0xffffffffu, v, o);
+            v = isMax ? fmax(v, w) : v + w;
+        }
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+        __syncthreads();
+        double t = isMax ? 0.0 : 0.0;
+        if (threadIdx.x == 0) {
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t = isMax ? fmax(t, red[i]) : t + red[i];
+            red[0] = t;
+        }
+        __syncthreads();
+        t = red[0];
+        __syncthreads();
+        return t;
+    };
+    int step = 0;
+    while ((l2 - l1) / (l1 + l2) > 1e-6 && step < maxSteps) {
+        lmid = 0.5 * (l2 + l1);
+        double s = 0;
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)nb * blockDim.x)
+            s += oc_new(x[i], dc[i], dv[i], lmid, move) - x[i];
+        const double bs = block_reduce(s, false);
+        if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+        grid.sync();
+        double tot = 0;
+        for (unsigned b = 0; b < nb; ++b) tot += partials[b];   // same order in every block
+        const double gt = fval + tot / (double)n;
+        if (gt > 0) l1 = lmid; else l2 = lmid;
+        ++step;
+        grid.sync();
+    }
+    // xnew from the last multiplier; change = max|xnew - x|; x = xnew
+    double mx = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)nb * blockDim.x) {
+        const double xn = oc_new(x[i], dc[i], dv[i], lmid, move);
+        mx = fmax(mx, fabs(xn - x[i]));
+        x[i] = xn;
+    }
+    const double bm = block_reduce(mx, true);
+    if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+    grid.sync();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double c = 0;
+        for (unsigned b = 0; b < nb; ++b) c = fmax(c, partials[b]);
+        sc->change = c;
+        sc->lmid = lmid;
+        sc->pad = (double)step;
+    }
+}
+
+__global__ void copy_kernel(const double *__restrict__ a, double *__restrict__ b, int64_t n)
+{ for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i]; }
+__global__ void fill_kernel(double *__restrict__ a, double v, int64_t n)
+{ for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) a[i] = v; }
+
+}  // namespace
+
+// ============================================================================
+// solver-attached state
+namespace {
+FilterState &filt(top_solver *s) { return *reinterpret_cast<FilterState *>(s->filterState); }
+OptState &opt(top_solver *s) { return *reinterpret_cast<OptState *>(s->optState); }
+
+int ensure_state(top_solver *s)
+{
+    if (!s->filterState) s->filterState = new FilterState();
+    if (!s->optState) s->optState = new OptState();
+    return TOP_OK;
+}
+}  // namespace
+
+void topgpu::free_opt_state(top_solver *s)
+{
+    delete reinterpret_cast<FilterState *>(s->filterState);
+    delete reinterpret_cast<OptState *>(s->optState);
+    s->filterState = s->optState = nullptr;
+}
+
+extern "C" int top_solver_filter_setup(top_solver *s, double rMin)
+{
+    if (!s || !(rMin > 0)) { set_error("top_solver_filter_setup: bad arguments"); return TOP_ERR_ARGS; }
+    ensure_state(s);
+    FilterState &f = filt(s);
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs;
+    if (!f.act) {
+        f.act = s->galloc<double>(cs, 1); f.invD = s->galloc<double>(cs, 1);
+        f.rhs = s->galloc<double>(cs, 1); f.x = s->galloc<double>(cs, 1); f.r = s->galloc<double>(cs, 1);
+        f.z = s->galloc<double>(cs, 1); f.p = s->galloc<double>(cs, 1); f.v = s->galloc<double>(cs, 1);
+        f.eg = s->galloc<double>(cs, 1);
+        f.st = s->dalloc<PcgState>(1);
+        if (!f.act || !f.invD || !f.rhs || !f.x || !f.r || !f.z || !f.p || !f.v || !f.eg || !f.st) {
+            set_error("top_solver_filter_setup: out of device memory"); return TOP_ERR_NOMEM;
+        }
+    }
+    filter_kernel_matrix(rMin, f.KEF.k);
+    filter_activity_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(l0.eleGrid, l0.Ne, f.act);
+    filter_diag_kernel<<<dim3(l0.g.nbx, l0.g.NZ), kNodeThreads, 0, s->st>>>(f.KEF, f.act, l0.g, l0.flags, f.invD);
+    CK(cudaGetLastError());
+    f.rMin = rMin;
+    f.ready = true;
+    return TOP_OK;
+}
+
+// tar = PDE-filter(src), element vectors (device, compact) -- TOP_GPU.m:959-1006
+static int filter_apply(top_solver *s, const double *src, double *tar, int *itsOut)
+{
+    FilterState &f = filt(s);
+    DevLevel &l0 = s->L[0];
+    const Geom &g = l0.g;
+    const int64_t cs = g.cs, ng = l0.ng;
+    cudaStream_t st = s->st;
+    // nodal rhs: each element adds src/8 to its nodes
+    CK(cudaMemsetAsync(f.eg - kMargin, 0, sizeof(double) * cs, st));
+    elem_to_slots_kernel<<<nb256(l0.Ne), 256, 0, st>>>(src, l0.eleGrid, l0.Ne, 1.0 / 8.0, f.eg);
+    slots_to_nodes_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, st>>>(f.eg, g, l0.flags, f.rhs);
+    // PCG with the filter operator and Jacobi, tol_/10, maxIT_ (TOP_GPU.m:999-1001)
+    const int VB = vb(ng);
+    fpcg_init_kernel<<<VB, 256, 0, st>>>(f.rhs, f.x, f.r, f.z, f.p, f.invD, ng, s->red(&f.st->normB));
+    fpcg_start_kernel<<<1, 1, 0, st>>>(f.st, s->p.tol / 10.0, s->p.maxIT);
+    fpcg_zr_kernel<<<VB, 256, 0, st>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
+    const int *done = &f.st->done;
+    const int chunk = 8;
+    PcgState h{};
+    for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
+        for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
+            filter_apply_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, st>>>(f.KEF, f.act, f.p, f.v, g, s->red(&f.st->pv), done);
+            fpcg_update_kernel<<<VB, 256, 0, st>>>(f.x, f.r, f.z, f.p, f.v, f.invD, ng, f.st, s->red(&f.st->rr));
+            fpcg_check_kernel<<<1, 1, 0, st>>>(f.st);
+            fpcg_zr_kernel<<<VB, 256, 0, st>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
+            fpcg_p_kernel<<<VB, 256, 0, st>>>(f.p, f.z, ng, f.st);
+        }
+        CK(cudaMemcpyAsync(&h, f.st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (h.done) break;
+    }
+    nodes_to_elem_kernel<<<nb256(l0.Ne), 256, 0, st>>>(f.x, l0.eleGrid, g, l0.Ne, tar);
+    CK(cudaGetLastError());
+    if (itsOut) *itsOut = h.its;
+    if (h.status == TOP_ERR_NAN) { set_error("PDE filter: non-finite PCG scalar"); return TOP_ERR_NAN; }
+    return TOP_OK;
+}
+
+extern "C" int top_solver_filter(top_solver *s, const double *src, double *tar, int *its)
+{
+    if (!s || !src || !tar) return TOP_ERR_ARGS;
+    if (!s->filterState || !filt(s).ready) { set_error("top_solver_filter: call top_solver_filter_setup first"); return TOP_ERR_STATE; }
+    const int rc = filter_apply(s, src, tar, its);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+// ---- the optimisation loop ---------------------------------------------------
+static int solve_all(top_solver *s, int warm, int *itsTotal)
+{
+    OptState &o = opt(s);
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs;
+    int tot = 0;
+    for (int k = 0; k < s->nLoads; ++k) {
+        int its = 0;
+        const int rc = pcg_grid(s, s->b + (size_t)k * 3 * cs, o.U + (size_t)k * 3 * cs, warm, &its, nullptr);
+        tot += its;
+        if (rc != TOP_OK && rc != TOP_ERR_NOT_CONVERGED) return rc;
+        if (rc == TOP_ERR_NOT_CONVERGED) std::fprintf(stderr, "Warning: Exceed the maximum iterate numbers\n");
+    }
+    if (itsTotal) *itsTotal = tot;
+    return TOP_OK;
+}
+
+static int sensitivities(top_solver *s, int withGrad)
+{
+    OptState &o = opt(s);
+    DevLevel &l0 = s->L[0];
+    sensitivity_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(
+        s->Ke64, o.U, 3 * l0.g.cs, s->nLoads, s->weights, l0.eleGrid, l0.Ne, l0.g, o.xPhys, s->Ec,
+        s->p.E0, s->p.Emin, s->p.penal, withGrad ? o.cSolid : 0.0, o.ce, withGrad ? o.dc : nullptr, o.dv,
+        s->red(&o.sc->cObj));
+    CK(cudaGetLastError());
+    return TOP_OK;
+}
+
+extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, double *cSolidOut)
+{
+    if (!s || !prm || prm->nLoop < 0 || !(prm->V0 > 0) || (prm->ft != 0 && prm->ft != 1 && prm->ft != 2)) {
+        set_error("top_solver_opt_begin: bad arguments"); return TOP_ERR_ARGS;
+    }
+    ensure_state(s);
+    OptState &o = opt(s);
+    DevLevel &l0 = s->L[0];
+    const int64_t Ne = l0.Ne, cs = l0.g.cs;
+    if (!o.xd) {
+        o.xd = s->dalloc<double>(Ne); o.xPhys = s->dalloc<double>(Ne); o.xnew = s->dalloc<double>(Ne);
+        o.dc = s->dalloc<double>(Ne); o.dv = s->dalloc<double>(Ne); o.ce = s->dalloc<double>(Ne); o.tmp = s->dalloc<double>(Ne);
+        o.U = s->galloc<double>(cs, 3 * s->nLoads);
+        o.sc = s->dalloc<OptScalars>(1);
+        if (cudaMallocHost(&o.hsc, sizeof(OptScalars)) != cudaSuccess) o.hsc = nullptr;
+        int dev = 0, nsm = 0, perSM = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, oc_kernel, 256, 0);
+        o.ocBlocks = std::max(1, std::min<int>(nsm * std::max(1, perSM), (int)((Ne + 255) / 256)));
+        o.ocPartials = s->dalloc<double>(o.ocBlocks);
+        if (!o.xd || !o.xPhys || !o.xnew || !o.dc || !o.dv || !o.ce || !o.tmp || !o.U || !o.sc || !o.hsc || !o.ocPartials) {
+            set_error("top_solver_opt_begin: out of memory"); return TOP_ERR_NOMEM;
+        }
+    }
+    o.prm = *prm;
+    if (prm->ft != 0) { const int rc = top_solver_filter_setup(s, prm->rMin); if (rc) return rc; }
+    // fully solid solve and its compliance (TOP_GPU.m:142-165)
+    fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.tmp, s->p.E0, Ne);
+    int rc = set_modulus_dev(s, o.tmp, 1, 0);
+    if (rc) return rc;
+    rc = top_solver_assemble(s);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(o.U - kMargin, 0, sizeof(double) * 3 * cs * s->nLoads, s->st));
+    rc = solve_all(s, 0, nullptr);
+    if (rc) return rc;
+    o.cSolid = 0;
+    rc = sensitivities(s, 0);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(o.hsc, o.sc, sizeof(OptScalars), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    o.cSolid = o.hsc->cObj;       // cSolid = E0 * sum(ceList) with E = E0
+    fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.xd, prm->V0, Ne);
+    fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.xPhys, prm->V0, Ne);
+    CK(cudaGetLastError());
+    o.loop = 0; o.change = 1.0; o.sharp = 1.0;
+    o.begun = true;
+    if (cSolidOut) *cSolidOut = o.cSolid;
+    return TOP_OK;
+}
+
+extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
+{
+    if (!s || !s->optState || !opt(s).begun) { set_error("top_solver_opt_step: call top_solver_opt_begin first"); return TOP_ERR_STATE; }
+    OptState &o = opt(s);
+    DevLevel &l0 = s->L[0];
+    const int64_t Ne = l0.Ne;
+    cudaStream_t st = s->st;
+    const int VB = vb(Ne);
+    cudaEvent_t ev[7];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    CK(cudaEventRecord(ev[0], st));
+    // 5.1 SIMP moduli and stencil assembly
+    int rc = set_modulus_dev(s, o.xPhys, 1, 1);
+    if (!rc) rc = top_solver_assemble(s);
+    if (rc) return rc;
+    CK(cudaEventRecord(ev[1], st));
+    // 5.2 state solves, warm-started
+    int its = 0;
+    rc = solve_all(s, 1, &its);
+    if (rc) return rc;
+    CK(cudaEventRecord(ev[2], st));
+    // objective and sensitivities, volume
+    rc = sensitivities(s, 1);
+    if (rc) return rc;
+    sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 0, s->red(&o.sc->sumE));
+    CK(cudaEventRecord(ev[3], st));
+    // 5.3 filtering of the sensitivities
+    int fits = 0;
+    if (o.prm.ft == 1) {
+        mul_kernel<<<VB, 256, 0, st>>>(o.xd, o.dc, o.tmp, Ne);
+        rc = filter_apply(s, o.tmp, o.dc, &fits);
+        if (rc) return rc;
+        div_floor_kernel<<<VB, 256, 0, st>>>(o.dc, o.xd, o.dc, Ne);
+    } else if (o.prm.ft == 2) {
+        rc = filter_apply(s, o.dc, o.tmp, &fits);
+        if (!rc) { copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dc, Ne); rc = filter_apply(s, o.dv, o.tmp, &fits); }
+        if (rc) return rc;
+        copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dv, Ne);
+    }
+    CK(cudaEventRecord(ev[4], st));
+    // 5.4 OC update; fval = mean(xPhys) - V0
+    CK(cudaMemcpyAsync(o.hsc, o.sc, sizeof(OptScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double cObj = o.hsc->cObj, vol = o.hsc->sumE / (double)Ne;
+    OptScalars h = *o.hsc;
+    h.fval = vol - o.prm.V0;
+    CK(cudaMemcpyAsync(o.sc, &h, sizeof(OptScalars), cudaMemcpyHostToDevice, st));
+    {
+        double move = 0.2;
+        int maxSteps = 256;
+        int64_t n = Ne;
+        double *xa = o.xd; const double *dca = o.dc, *dva = o.dv; double *pa = o.ocPartials; OptScalars *sca = o.sc;
+        void *args[] = {&xa, &dca, &dva, &n, &pa, &sca, &move, &maxSteps};
+        CK(cudaLaunchCooperativeKernel((const void *)oc_kernel, dim3(o.ocBlocks), dim3(256), args, 0, st));
+    }
+    CK(cudaEventRecord(ev[5], st));
+    // xPhys (TOP_GPU.m:256-267): the new design, or its PDE-filtered version
+    if (o.prm.ft == 2) { rc = filter_apply(s, o.xd, o.xPhys, &fits); if (rc) return rc; }
+    else copy_kernel<<<VB, 256, 0, st>>>(o.xd, o.xPhys, Ne);
+    sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 1, s->red(&o.sc->sharp));
+    CK(cudaEventRecord(ev[6], st));
+    CK(cudaMemcpyAsync(o.hsc, o.sc, sizeof(OptScalars), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    o.loop += 1;
+    o.change = o.hsc->change;
+    o.sharp = 4.0 * o.hsc->sharp / (double)Ne;
+    if (rec) {   // the reference's tHist columns (TOP_GPU.m:283)
+        float t[6];
+        for (int k = 0; k < 6; ++k) cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]);
+        rec->c = cObj * o.cSolid;
+        rec->vol = vol;
+        rec->sharp = o.sharp;
+        rec->cons = h.fval;
+        rec->change = o.change;
+        rec->pcgIts = its;
+        rec->msAssemble = t[0];
+        rec->msSolve = t[1];
+        rec->msOpt = t[2] + t[4];
+        rec->msFilter = t[3] + t[5];
+        float tot = 0;
+        cudaEventElapsedTime(&tot, ev[0], ev[6]);
+        rec->msTotal = tot;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return TOP_OK;
+}
+
+extern "C" int top_solver_opt_state(top_solver *s, int *loop, double *change, double *sharpness)
+{
+    if (!s || !s->optState || !opt(s).begun) return TOP_ERR_STATE;
+    OptState &o = opt(s);
+    if (loop) *loop = o.loop;
+    if (change) *change = o.change;
+    if (sharpness) *sharpness = o.sharp;
+    return TOP_OK;
+}
+
+extern "C" int top_solver_get_design(top_solver *s, double *xPhys, double *x)
+{
+    if (!s || !s->optState || !opt(s).begun) return TOP_ERR_STATE;
+    OptState &o = opt(s);
+    const int64_t Ne = s->L[0].Ne;
+    if (xPhys) CK(cudaMemcpyAsync(xPhys, o.xPhys, sizeof(double) * Ne, cudaMemcpyDeviceToDevice, s->st));
+    if (x) CK(cudaMemcpyAsync(x, o.xd, sizeof(double) * Ne, cudaMemcpyDeviceToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysOut,
+                                   top_opt_record *hist, int *nIter, double *cSolid)
+{
+    int rc = top_solver_opt_begin(s, prm, cSolid);
+    if (rc) return rc;
+    OptState &o = opt(s);
+    // TOP_GPU.m:176 -- loop < nLoop && change > 1e-4 && sharpness > 0.01
+    while (o.loop < prm->nLoop && o.change > 0.0001 && o.sharp > 0.01) {
+        rc = top_solver_opt_step(s, hist ? hist + o.loop : nullptr);
+        if (rc) return rc;
+    }
+    if (nIter) *nIter = o.loop;
+    if (xPhysOut) return top_solver_get_design(s, xPhysOut, nullptr);
+    return TOP_OK;
+}

@@ -12,8 +12,8 @@
 #include <cstring>
 #include <new>
 #include <vector>
-#include "topgpu_grid.cuh"
 #include "topgpu_kernels.cuh"
+#include "topgpu_solver_impl.cuh"
 
 namespace topgpu {
 int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
@@ -24,10 +24,7 @@ int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const
 int assemble_higher_f64(double *Ks, const int32_t *upMap, const double *KsPrev, const double *Psub,
                         int64_t nElem, int nSub, cudaStream_t st);
 
-struct PcgState {
-    double normB, rho, rhoOld, pv, rr, resnorm, tol;
-    int its, maxIT, done, status;
-};
+
 
 // ---------------------------------------------------------------------------
 // small kernels
@@ -332,68 +329,15 @@ __global__ void compliance_kernel(const KeParam<double> K, const double *__restr
     ce[e] = acc;
 }
 
-// ---------------------------------------------------------------------------
-struct DevLevel {
-    int ny = 0, nx = 0, nz = 0, span = 0;
-    Geom g{};
-    int64_t Ne = 0, Nn = 0, ng = 0;
-    uint8_t *flags = nullptr;
-    int32_t *nodeGrid = nullptr, *eleGrid = nullptr, *upMap = nullptr;
-    double *KsC = nullptr, *KsP64 = nullptr; float *KsP32 = nullptr;
-    double *diag = nullptr, *invD64 = nullptr; float *invD32 = nullptr;
-    double *r64 = nullptr, *x64 = nullptr, *t64 = nullptr;
-    float *r32 = nullptr, *x32 = nullptr, *t32 = nullptr;
-    uint8_t *tileFixed = nullptr;
-};
+
 
 }  // namespace topgpu
 
 using namespace topgpu;
 
-struct top_solver {
-    top_solver_params p{};
-    cudaStream_t st = nullptr;
-    int nL = 0, nLoads = 0;
-    std::vector<DevLevel> L;
-    std::vector<void *> allocs;      // raw allocations (freed on destroy)
-    KeParam<double> Ke64{}; KeParam<float> Ke32{};
-    double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
-    double *Ec = nullptr, *Eg64 = nullptr; float *Eg32 = nullptr;
-    int32_t *mapUnique = nullptr; double *uFree = nullptr, *uFixed = nullptr; int64_t nU = 0;
-    double *Qs = nullptr; int32_t *eye = nullptr;
-    int32_t *bndList = nullptr; int64_t nBnd = 0;   // level-1 cells with fixed-DOF children
-    double *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *v = nullptr, *tmp = nullptr;
-    double *b = nullptr;             // [nLoads][3 x cs]
-    double *weights = nullptr;
-    PcgState *state = nullptr, *hstate = nullptr;
-    double *partials = nullptr; unsigned *counter = nullptr; int64_t nPartials = 0;
-    double *scal = nullptr;          // device scalars for standalone reductions
-    int *zeroDone = nullptr;
-    int64_t nC = 0; double *Ac = nullptr, *Ainv = nullptr, *Wc = nullptr, *cr = nullptr;
-    int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
-    bool assembled = false;
-    std::vector<double> Fhost; int64_t nd0 = 0;
-
-    template <typename T> T *dalloc(size_t n)
-    {
-        void *ptr = nullptr;
-        if (cudaMalloc(&ptr, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
-        cudaMemset(ptr, 0, sizeof(T) * (n ? n : 1));
-        allocs.push_back(ptr);
-        return static_cast<T *>(ptr);
-    }
-    // grid array with margins: ncomp components of stride cs
-    template <typename T> T *galloc(int64_t cs, int ncomp)
-    {
-        T *b = dalloc<T>((size_t)cs * ncomp);
-        return b ? b + kMargin : nullptr;
-    }
-    Reduce red(double *result) const { return Reduce{partials, counter, result}; }
-};
 
 namespace {
 
-inline int nb256(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 1 << 20); }
 inline dim3 node_grid(const Geom &g) { return dim3((unsigned)g.nbx, (unsigned)g.NZ); }
 inline int vec_blocks(int64_t ng) { return (int)std::min<int64_t>((3 * ng + 255) / 256, 4096); }
 
@@ -731,6 +675,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
 extern "C" int top_solver_destroy(top_solver *s)
 {
     if (!s) return TOP_OK;
+    free_opt_state(s);
     for (void *p : s->allocs) cudaFree(p);
     if (s->hstate) cudaFreeHost(s->hstate);
     delete s;
@@ -751,7 +696,7 @@ extern "C" int top_solver_sizes(const top_solver *s, int64_t *out3)
     return TOP_OK;
 }
 
-static int set_E(top_solver *s, const double *src, int where, int simp)
+int topgpu::set_modulus_dev(top_solver *s, const double *src, int where, int simp)
 {
     if (!s || !src) return TOP_ERR_ARGS;
     const int64_t Ne = s->L[0].Ne;
@@ -765,8 +710,8 @@ static int set_E(top_solver *s, const double *src, int where, int simp)
     s->assembled = false;
     return TOP_OK;
 }
-extern "C" int top_solver_set_modulus(top_solver *s, const double *E, int where) { return set_E(s, E, where, 0); }
-extern "C" int top_solver_set_density(top_solver *s, const double *x, int where) { return set_E(s, x, where, 1); }
+extern "C" int top_solver_set_modulus(top_solver *s, const double *E, int where) { return set_modulus_dev(s, E, where, 0); }
+extern "C" int top_solver_set_density(top_solver *s, const double *x, int where) { return set_modulus_dev(s, x, where, 1); }
 
 extern "C" int top_solver_assemble(top_solver *s)
 {
@@ -911,60 +856,43 @@ extern "C" int top_solver_get_ks(top_solver *s, int level, double *Ks)
 }
 
 // ---- PCG (Solving_PCG, TOP_GPU.m:602-667) ---------------------------------
-static int pcg_run(top_solver *s, const double *bGrid, double *U, int warm, int *itsOut, double *resOut)
+__global__ void pcg_init_kernel(PcgState *st)
+{   // ||b|| from the squared norm written by dot_kernel into st->normB
+    st->normB = sqrt(st->normB);
+    if (st->normB == 0.0) st->done = 1;   // zero load: x = 0, no iterations
+}
+
+int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, int *itsOut, double *resOut)
 {
     if (!s->assembled) { set_error("top_solver_pcg: assemble first"); return TOP_ERR_STATE; }
     DevLevel &l0 = s->L[0];
     const int64_t cs = l0.g.cs, ng = l0.ng;
     cudaStream_t st = s->st;
     const int VB = vec_blocks(ng);
-    // state
     PcgState h{};
     h.tol = s->p.tol; h.maxIT = s->p.maxIT;
     CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
     int *done = &s->state->done;
-    // normB
-    dot_kernel<<<VB, 256, 0, st>>>(bGrid, bGrid, ng, cs, s->red(s->scal));
-    // x0
-    CK(cudaMemsetAsync(s->x - kMargin, 0, sizeof(double) * 3 * cs, st));
-    if (warm) compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, st>>>(U, s->x, l0.nodeGrid, l0.Nn, cs);
+    dot_kernel<<<VB, 256, 0, st>>>(bGrid, bGrid, ng, cs, s->red(&s->state->normB));
+    pcg_init_kernel<<<1, 1, 0, st>>>(s->state);
+    if (!warm) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * 3 * cs, st));
     // r = b - A x
     if (s->p.outerFP32)
-        level_op<float>(s, 0, VecIn<float, double>{s->x, cs}, ResidOut<float, double, double>{bGrid, s->r, cs},
-                        Reduce{nullptr, nullptr, nullptr}, nullptr);
+        level_op<float>(s, 0, VecIn<float, double>{xg, cs}, ResidOut<float, double, double>{bGrid, s->r, cs},
+                        Reduce{nullptr, nullptr, nullptr}, done);
     else
-        level_op<double>(s, 0, VecIn<double, double>{s->x, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
-                         Reduce{nullptr, nullptr, nullptr}, nullptr);
-    CKL();
-    // copy ||b||^2 from scal[0] and set up the loop state on the device
-    CK(cudaStreamSynchronize(st));
-    double nb2 = 0;
-    CK(cudaMemcpy(&nb2, s->scal, sizeof(double), cudaMemcpyDeviceToHost));
-    h.normB = std::sqrt(nb2);
-    h.done = 0; h.its = 0; h.status = 0;
-    if (h.normB == 0.0) {
-        CK(cudaMemsetAsync(U, 0, sizeof(double) * s->nd0, st));
-        if (itsOut) *itsOut = 0;
-        if (resOut) *resOut = 0.0;
-        CK(cudaStreamSynchronize(st));
-        return TOP_OK;
-    }
-    CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+        level_op<double>(s, 0, VecIn<double, double>{xg, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
+                         Reduce{nullptr, nullptr, nullptr}, done);
     // z = M r ; rho = z . r ; p = z
-    precond(s, s->r, s->z, &s->state->rho, nullptr);
+    precond(s, s->r, s->z, &s->state->rho, done);
     pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 1);
     CKL();
     static const bool trace = std::getenv("TOPGPU_PCG_TRACE") != nullptr;
-    if (trace) {
-        CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        std::fprintf(stderr, "pcg init normB %.6e rho %.6e\n", s->hstate->normB, s->hstate->rho);
-    }
     const int chunk = trace ? 1 : 4;
     for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
         for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
             outer_op(s, s->pv, s->v, &s->state->pv, done);                                   // v = A p, p.v
-            pcg_update_kernel<<<VB, 256, 0, st>>>(s->x, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
+            pcg_update_kernel<<<VB, 256, 0, st>>>(xg, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
             pcg_check_kernel<<<1, 1, 0, st>>>(s->state);
             precond(s, s->r, s->z, &s->state->rho, done);                                     // z = M r, z.r
             pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 0);              // p = z + beta p
@@ -978,14 +906,27 @@ static int pcg_run(top_solver *s, const double *bGrid, double *U, int warm, int 
         if (s->hstate->done) break;
     }
     const PcgState &f = *s->hstate;
-    grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, st>>>(s->x, U, l0.nodeGrid, l0.Nn, cs);
-    CKL();
-    CK(cudaStreamSynchronize(st));
+    if (f.normB == 0.0) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * 3 * cs, st));
     if (itsOut) *itsOut = f.its;
     if (resOut) *resOut = f.resnorm;
     if (f.status == TOP_ERR_NAN) { set_error("top_solver_pcg: non-finite PCG scalar at iteration %d", f.its); return TOP_ERR_NAN; }
     if (f.status == TOP_ERR_NOT_CONVERGED) { set_error("Exceed the maximum iterate numbers (residual %.4e)", f.resnorm); return TOP_ERR_NOT_CONVERGED; }
     return TOP_OK;
+}
+
+// compact warm start / solution around pcg_grid
+static int pcg_run(top_solver *s, const double *bGrid, double *U, int warm, int *itsOut, double *resOut)
+{
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs;
+    CK(cudaMemsetAsync(s->x - kMargin, 0, sizeof(double) * 3 * cs, s->st));
+    if (warm) compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U, s->x, l0.nodeGrid, l0.Nn, cs);
+    const int rc = pcg_grid(s, bGrid, s->x, 1, itsOut, resOut);
+    if (rc != TOP_OK && rc != TOP_ERR_NOT_CONVERGED) return rc;
+    grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(s->x, U, l0.nodeGrid, l0.Nn, cs);
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return rc;
 }
 
 extern "C" int top_solver_pcg(top_solver *s, int loadCase, double *U, int warm, int *its, double *relres)

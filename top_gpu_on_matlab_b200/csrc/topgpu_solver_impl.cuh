@@ -1,0 +1,91 @@
+// topgpu_solver_impl.cuh -- internal state of the fused solver, shared by
+// topgpu_solver.cu (operators, V-cycle, PCG, assembly) and topgpu_opt.cu
+// (filters, sensitivities, OC loop).
+#pragma once
+#include <cuda_runtime.h>
+#include <vector>
+#include "topgpu_grid.cuh"
+
+namespace topgpu {
+
+struct PcgState {
+    double normB, rho, rhoOld, pv, rr, resnorm, tol;
+    int its, maxIT, done, status;
+};
+
+// ---------------------------------------------------------------------------
+struct DevLevel {
+    int ny = 0, nx = 0, nz = 0, span = 0;
+    Geom g{};
+    int64_t Ne = 0, Nn = 0, ng = 0;
+    uint8_t *flags = nullptr;
+    int32_t *nodeGrid = nullptr, *eleGrid = nullptr, *upMap = nullptr;
+    double *KsC = nullptr, *KsP64 = nullptr; float *KsP32 = nullptr;
+    double *diag = nullptr, *invD64 = nullptr; float *invD32 = nullptr;
+    double *r64 = nullptr, *x64 = nullptr, *t64 = nullptr;
+    float *r32 = nullptr, *x32 = nullptr, *t32 = nullptr;
+    uint8_t *tileFixed = nullptr;
+};
+
+}  // namespace topgpu
+
+struct top_solver {
+    using DevLevel = topgpu::DevLevel;
+    using PcgState = topgpu::PcgState;
+    using Reduce = topgpu::Reduce;
+    top_solver_params p{};
+    cudaStream_t st = nullptr;
+    int nL = 0, nLoads = 0;
+    std::vector<DevLevel> L;
+    std::vector<void *> allocs;      // raw allocations (freed on destroy)
+    topgpu::KeParam<double> Ke64{}; topgpu::KeParam<float> Ke32{};
+    double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
+    double *Ec = nullptr, *Eg64 = nullptr; float *Eg32 = nullptr;
+    int32_t *mapUnique = nullptr; double *uFree = nullptr, *uFixed = nullptr; int64_t nU = 0;
+    double *Qs = nullptr; int32_t *eye = nullptr;
+    int32_t *bndList = nullptr; int64_t nBnd = 0;   // level-1 cells with fixed-DOF children
+    double *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *v = nullptr, *tmp = nullptr;
+    double *b = nullptr;             // [nLoads][3 x cs]
+    double *weights = nullptr;
+    PcgState *state = nullptr, *hstate = nullptr;
+    double *partials = nullptr; unsigned *counter = nullptr; int64_t nPartials = 0;
+    double *scal = nullptr;          // device scalars for standalone reductions
+    int *zeroDone = nullptr;
+    int64_t nC = 0; double *Ac = nullptr, *Ainv = nullptr, *Wc = nullptr, *cr = nullptr;
+    int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
+    bool assembled = false;
+    void *filterState = nullptr, *optState = nullptr;   // topgpu_opt.cu
+    std::vector<double> Fhost; int64_t nd0 = 0;
+
+    template <typename T> T *dalloc(size_t n)
+    {
+        void *ptr = nullptr;
+        if (cudaMalloc(&ptr, sizeof(T) * (n ? n : 1)) != cudaSuccess) return nullptr;
+        cudaMemset(ptr, 0, sizeof(T) * (n ? n : 1));
+        allocs.push_back(ptr);
+        return static_cast<T *>(ptr);
+    }
+    // grid array with margins: ncomp components of stride cs
+    template <typename T> T *galloc(int64_t cs, int ncomp)
+    {
+        T *b = dalloc<T>((size_t)cs * ncomp);
+        return b ? b + topgpu::kMargin : nullptr;
+    }
+    Reduce red(double *result) const { return Reduce{partials, counter, result}; }
+};
+
+namespace topgpu {
+// PCG (TOP_GPU.m:602-667) on level-0 grid vectors: b and x in the solver's
+// SoA grid layout, x holds the warm start when warm != 0 and the solution.
+int pcg_grid(top_solver *s, const double *bGrid, double *xGrid, int warm, int *itsOut, double *resOut);
+void free_opt_state(top_solver *s);
+// element moduli from a compact element vector (SIMP when simp != 0)
+int set_modulus_dev(top_solver *s, const double *src, int where, int simp);
+template <typename TI, typename TO>
+__global__ void compact_to_grid_kernel(const TI *__restrict__ v, TO *__restrict__ g,
+                                       const int32_t *__restrict__ nodeGrid, int64_t Nn, int64_t cs);
+template <typename TI, typename TO>
+__global__ void grid_to_compact_kernel(const TI *__restrict__ g, TO *__restrict__ v,
+                                       const int32_t *__restrict__ nodeGrid, int64_t Nn, int64_t cs);
+inline int nb256(int64_t n) { return (int)((n + 255) / 256 < (1 << 20) ? (n + 255) / 256 : (1 << 20)); }
+}  // namespace topgpu

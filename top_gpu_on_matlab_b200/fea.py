@@ -12,8 +12,8 @@ import ctypes as C
 import numpy as np
 import torch
 
-from ._lib import (SolverParams, TOP_ERR_NOT_CONVERGED, TOP_OK, TOP_PREC_FP64, TOP_PREC_MIXED,
-                   TopGpuError, check, last_error, lib)
+from ._lib import (OptParams, OptRecord, SolverParams, TOP_ERR_NOT_CONVERGED, TOP_OK, TOP_PREC_FP64,
+                   TOP_PREC_MIXED, TopGpuError, check, last_error, lib)
 
 _INT_ARRAYS = {"eleMapBack", "eleMapForward", "eNodMat", "nodMapBack", "nodMapForward", "nodesOnBoundary",
                "elementsOnBoundary", "elementUpwardMap", "transferMat", "solidNodeMapCoarser2Finer",
@@ -209,3 +209,48 @@ class Solver:
         ce = torch.zeros(self.levels[0]["numElements"], dtype=torch.float64, device="cuda")
         check(lib().top_solver_unit_compliance(self._h, U.data_ptr(), ce.data_ptr()), "top_solver_unit_compliance")
         return ce
+
+    # -- optimisation steps (TOP_GPU.m:141-292) --------------------------------
+    def filter_setup(self, rMin):
+        check(lib().top_solver_filter_setup(self._h, float(rMin)), "top_solver_filter_setup")
+
+    def filter(self, src):
+        src = self._dev(src, self.levels[0]["numElements"])
+        out = torch.zeros_like(src)
+        its = C.c_int(0)
+        check(lib().top_solver_filter(self._h, src.data_ptr(), out.data_ptr(), C.byref(its)), "top_solver_filter")
+        return out, its.value
+
+    def opt_begin(self, V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1):
+        self._opt = OptParams(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
+        cs = C.c_double(0)
+        check(lib().top_solver_opt_begin(self._h, C.byref(self._opt), C.byref(cs)), "top_solver_opt_begin")
+        return cs.value
+
+    def opt_step(self):
+        rec = OptRecord()
+        check(lib().top_solver_opt_step(self._h, C.byref(rec)), "top_solver_opt_step")
+        return {k: getattr(rec, k) for k, _ in OptRecord._fields_}
+
+    def opt_state(self):
+        loop, ch, sh = C.c_int(0), C.c_double(0), C.c_double(0)
+        check(lib().top_solver_opt_state(self._h, C.byref(loop), C.byref(ch), C.byref(sh)), "top_solver_opt_state")
+        return loop.value, ch.value, sh.value
+
+    def design(self):
+        ne = self.levels[0]["numElements"]
+        xp = torch.zeros(ne, dtype=torch.float64, device="cuda")
+        x = torch.zeros(ne, dtype=torch.float64, device="cuda")
+        check(lib().top_solver_get_design(self._h, xp.data_ptr(), x.data_ptr()), "top_solver_get_design")
+        return xp, x
+
+    def optimize(self, V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1):
+        """TOP_GPU's optimisation loop on the device; returns (xPhys, history, cSolid)."""
+        prm = OptParams(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
+        hist = (OptRecord * max(1, nLoop))()
+        n, cs = C.c_int(0), C.c_double(0)
+        xp = torch.zeros(self.levels[0]["numElements"], dtype=torch.float64, device="cuda")
+        check(lib().top_solver_optimize(self._h, C.byref(prm), xp.data_ptr(), hist, C.byref(n), C.byref(cs)),
+              "top_solver_optimize")
+        rows = [{k: getattr(hist[i], k) for k, _ in OptRecord._fields_} for i in range(n.value)]
+        return xp, rows, cs.value
