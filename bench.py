@@ -2,21 +2,24 @@
 
 Workload (the metric's configuration): true(96,192,96) voxels (1,769,472
 elements, 5,447,811 DOFs), cantilever BCs (optCase 1), E0 = 1, Emin = 1e-9,
-nu = 0.3, SIMP p = 3, five multigrid levels (coarsestResolutionControl 400;
-192x96x96 -> 48x24x24 -> 24x12x12 -> 12x6x6 -> 6x3x3), damped Jacobi
-omega = 0.6, relative residual 1e-6.  One step = one optimisation
-iteration's FEA: SIMP moduli from the design, Galerkin assembly of every
-coarse level + coarsest Cholesky, and the PCG state solve warm-started from
-the previous iteration (TOP_GPU.m:180-187).  The design and warm start of a
-step are those of optimisation iteration 1 (x = V0 = 0.12 everywhere, U from
-the fully solid solve), so every step does identical work.
+nu = 0.3, SIMP p = 3, V0 = 0.12, rMin = sqrt(3), ft = 1 sensitivity filter,
+five multigrid levels (coarsestResolutionControl 400; 192x96x96 ->
+48x24x24 -> 24x12x12 -> 12x6x6 -> 6x3x3), damped Jacobi omega = 0.6,
+relative residual 1e-6.  One step = one optimisation iteration of
+TOP_GPU.m:176-292 on the device: SIMP moduli, Galerkin assembly of every
+coarse level + coarsest Cholesky, the PCG state solve warm-started from the
+previous iteration, element energies, sensitivity filter and OC update.
+W warm-up iterations run first (iterations 1..W after the fully solid
+solve), then K timed iterations (W+1..W+K).
 
-value = PCG ms per optimisation iteration of the mixed-precision path
+value = mean PCG ms of the timed iterations on the mixed-precision path
 (FP32 V-cycle, FP64 outer recurrence / matvec / coarsest Cholesky), device
-time from CUDA events with inputs resident in HBM.  The same steps run with
-the plain FP64 path for the ratio and the compliance error.  e2e repeats the
-step through the C ABI with the design on the host (pinned) and the
-compliance read back every step.
+time from CUDA events with inputs resident in HBM.  The same iterations run
+on the plain FP64 path for the ratio; the compliance error is the largest
+relative difference of any iteration's compliance between the two paths,
+the density error the max-abs difference of xPhys after the last one.  e2e
+runs the same iterations through the C ABI with the design held on the host
+(pinned): the design goes up before and comes back after every iteration.
 
 --impl reference times the FP64 CPU restatement of the reference (oracle/,
 the MATLAB driver cannot run here) on the host cores on a bounded sample.
@@ -40,7 +43,11 @@ CONTROL = 400
 V0 = 0.12
 E0, EMIN, PENAL, NU = 1.0, 1e-9, 3.0, 0.3
 TOL, MAXIT, OMEGA = 1e-6, 800, 0.6
-WORKLOAD = "cantilever_96x192x96_optiter1"
+RMIN, FT = 3 ** 0.5, 1
+WORKLOAD = "cantilever_96x192x96_ft1_optimisation_iterations"
+# DRAM bytes (read + write) per launch of the level-0 stiffness products from
+# one ncu capture of this workload (profiles/l0_kernel_cantilever_96x192x96.md)
+NCU_TRAFFIC = {"l0_f64": None, "l0_f32": None}
 
 
 def _env_rank():
@@ -166,80 +173,69 @@ def run_ours(args):
     mesh.apply_optcase(1)
     info = mesh.info()
     ne, nn = info[0]["numElements"], info[0]["numNodes"]
-    solvers = {}
-    for name, mixed in (("mixed", True), ("fp64", False)):
-        solvers[name] = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=mixed)
-    # optimisation iteration 0: fully solid solve (TOP_GPU.m:144-155)
-    s64 = solvers["fp64"]
-    s64.set_modulus(torch.full((ne,), E0, dtype=torch.float64, device=dev))
-    s64.assemble()
-    U_solid, its_solid, _ = s64.pcg(0)
-    x = torch.full((ne,), V0, dtype=torch.float64, device=dev)
-    F = torch.from_numpy(mesh.get(0, "F")).to(dev)
     stream = torch.cuda.current_stream()
 
-    def step(s, U0):
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        ev[0].record(stream)
-        s.set_density(x)
-        s.assemble()
-        ev[1].record(stream)
-        U, its, res = s.pcg(0, U=U0)
-        ev[2].record(stream)
-        torch.cuda.synchronize()
-        return U, its, res, ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    def make(mixed):
+        s = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=mixed)
+        c_solid = s.opt_begin(V0=V0, rMin=RMIN, nLoop=1 << 20, ft=FT)
+        return s, c_solid
 
-    results = {}
-    for name in ("fp64", "mixed"):
-        s = solvers[name]
-        for _ in range(args.warmup):
-            step(s, U_solid)
+    def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+
+    results = {}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        s, c_solid = make(mixed)
+        recs = [s.opt_step() for _ in range(args.warmup)]
+        barrier()
         clk = Clocks(local) if name == "mixed" else None
+        n0 = s.launches
         t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        asm, pcg, its_l = [], [], []
-        U = None
-        for _ in range(args.steps):
-            U, its, res, ta, tp = step(s, U_solid)
-            asm.append(ta); pcg.append(tp); its_l.append(its)
+        timed = [s.opt_step() for _ in range(args.steps)]
         t1.record(stream)
-        torch.cuda.synchronize()
-        total = t0.elapsed_time(t1)
+        barrier()
+        launches = s.launches - n0
         clocks = clk.stop() if clk else None
-        vals = torch.tensor([float(np.mean(pcg)), total / args.steps, float(np.mean(asm))], device=dev)
+        total = t0.elapsed_time(t1)
+        vals = torch.tensor([float(np.mean([r["msSolve"] for r in timed])), total / args.steps,
+                             float(np.mean([r["msAssemble"] for r in timed]))], device=dev)
         if world > 1:
             dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-        results[name] = dict(pcg_ms=float(vals[0]), step_ms=float(vals[1]), asm_ms=float(vals[2]), its=its_l[-1],
-                             compliance=float(F @ U), clocks=clocks)
+        xp, _ = s.design()
+        results[name] = dict(solver=s, pcg_ms=float(vals[0]), step_ms=float(vals[1]), asm_ms=float(vals[2]),
+                             its=[r["pcgIts"] for r in timed], c=[r["c"] for r in recs + timed],
+                             rows=timed, launches=launches, clocks=clocks, xPhys=xp, c_solid=c_solid)
     mixed, fp64 = results["mixed"], results["fp64"]
-    comp_err = abs(mixed["compliance"] - fp64["compliance"]) / abs(fp64["compliance"])
+    comp_err = max(abs(a - b) / abs(b) for a, b in zip(mixed["c"], fp64["c"]))
+    dens_err = float((mixed["xPhys"] - fp64["xPhys"]).abs().max())
+    del fp64["solver"]
 
-    # ---- e2e through the C ABI with the design on the host (pinned) ----
-    s = solvers["mixed"]
-    x_host = torch.full((ne,), V0, dtype=torch.float64).pin_memory()
-    c_host = torch.zeros(1, dtype=torch.float64).pin_memory()
-    xd = torch.empty_like(x_host, device=dev)
-    U_dev = U_solid.clone()
+    # ---- e2e: the same optimisation iterations through the C ABI with the
+    # design on the host (pinned): H2D of (xPhys, x) before each iteration,
+    # D2H of the new design after it (the compliance comes back in the record)
+    s, _ = make(True)
+    xp_h = torch.full((ne,), V0, dtype=torch.float64).pin_memory()
+    x_h = torch.full((ne,), V0, dtype=torch.float64).pin_memory()
     e2e = []
     for k in range(args.warmup + args.steps):
-        torch.cuda.synchronize()
+        barrier()
         e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        xd.copy_(x_host, non_blocking=True)
-        s.set_density(xd)
-        s.assemble()
-        U, its, res = s.pcg(0, U=U_dev)
-        c_host.copy_((F @ U).reshape(1), non_blocking=True)
+        s.set_design(xp_h, x_h)
+        s.opt_step()
+        s.get_design_into(xp_h, x_h)
         e1.record(stream)
         torch.cuda.synchronize()
         if k >= args.warmup:
             e2e.append(e0.elapsed_time(e1))
     e2e_ms = float(np.mean(e2e))
+    del s
 
     # ---- kernel roofline: level-0 stiffness products, L2 flushed ----
+    s = mixed["solver"]
     peak, peak_kind = _peaks()
     flush = 512 << 20
     tk = {}
@@ -253,40 +249,48 @@ def run_ours(args):
     # mixed PCG iteration: 1 FP64 outer product + 2 FP32 level-0 smoother products
     share64, share32 = tk["l0_f64"], 2 * tk["l0_f32"]
     if share64 >= share32:
-        dom, t_dom, byt = "l0_kernel<double> (outer K*p)", tk["l0_f64"], bytes64
+        dom, t_dom, byt, traffic = "l0_kernel<double> (outer K*p)", tk["l0_f64"], bytes64, NCU_TRAFFIC["l0_f64"]
     else:
-        dom, t_dom, byt = "l0_kernel<float> (V-cycle smoother K*u)", tk["l0_f32"], bytes32
+        dom, t_dom, byt, traffic = "l0_kernel<float> (V-cycle smoother K*u)", tk["l0_f32"], bytes32, NCU_TRAFFIC["l0_f32"]
     achieved = byt / (t_dom * 1e-3) / 1e9
+    its_m = float(np.mean(mixed["its"]))
+    its_d = float(np.mean(fp64["its"]))
     line = {
         "metric": "PCG ms/opt-iter", "value": mixed["pcg_ms"], "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed["step_ms"],
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
         "config": {"workload": WORKLOAD, "shape": list(SHAPE), "elements": ne, "dofs": 3 * nn, "levels": len(info),
-                   "control": CONTROL, "tol": TOL, "precision": "mixed (FP32 V-cycle, FP64 outer)",
+                   "control": CONTROL, "tol": TOL, "V0": V0, "rMin": RMIN, "ft": FT,
+                   "opt_iters_timed": "%d-%d" % (args.warmup + 1, args.warmup + args.steps),
+                   "precision": "mixed (FP32 V-cycle, FP64 outer)",
                    "l2": "working set > L2 per PCG iteration; kernel timings flush L2",
                    "parallelism": "replicas" if world > 1 else "single"},
-        "pcg_its": mixed["its"], "fp64_pcg_ms": fp64["pcg_ms"], "fp64_pcg_its": fp64["its"],
+        "pcg_its": its_m, "fp64_pcg_ms": fp64["pcg_ms"], "fp64_pcg_its": its_d,
         "mixed_vs_fp64_speedup": fp64["pcg_ms"] / mixed["pcg_ms"],
+        "opt_iter_ms": {"mixed": mixed["step_ms"], "fp64": fp64["step_ms"]},
         "compliance_rel_err_mixed_vs_fp64": comp_err,
+        "density_maxabs_err_mixed_vs_fp64": dens_err,
         "assembly_ms": mixed["asm_ms"], "fp64_assembly_ms": fp64["asm_ms"],
         "kernel_ms": tk,
         "matvec_gbs": {"fp64": bytes64 / (tk["l0_f64"] * 1e-3) / 1e9, "fp32": bytes32 / (tk["l0_f32"] * 1e-3) / 1e9},
         "matvec_tflops": {"fp64": flops / (tk["l0_f64"] * 1e-3) / 1e12, "fp32": flops / (tk["l0_f32"] * 1e-3) / 1e12},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                     "traffic": None},
-        "gpu_launches": None,
-        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": ne * 8, "d2h_bytes_per_step": 8,
-                "includes": "H2D design, SIMP, assembly, PCG, D2H compliance"},
+                     "algorithmic_bytes": byt, "traffic": traffic},
+        "gpu_launches": mixed["launches"],
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * ne * 8, "d2h_bytes_per_step": 2 * ne * 8,
+                "includes": "whole optimisation iteration through the C ABI: H2D design, SIMP, assembly, "
+                            "PCG, sensitivities, filter, OC, D2H design and compliance"},
         "clocks": mixed["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         cs = cpu_sample(iters=2)
-        line["cpu_baseline"] = {"value": cs["ms_per_pcg_iter"] * fp64["its"], "unit": "ms", "cores": cs["cores"],
+        line["cpu_baseline"] = {"value": cs["ms_per_pcg_iter"] * its_d, "unit": "ms", "cores": cs["cores"],
                                 "kind": "port",
                                 "sample": "2 FP64 PCG iterations of the oracle (C + OpenMP) on this problem, "
-                                          "ms/iteration x the FP64 iteration count (%d)" % fp64["its"],
+                                          "ms/iteration x the mean FP64 iteration count of the timed "
+                                          "optimisation iterations (%.1f)" % its_d,
                                 "assemble_ms": cs["assemble_ms"]}
     if rank == 0:
         print(json.dumps(line), flush=True)

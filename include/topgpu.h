@@ -232,7 +232,11 @@ int top_solver_filter(top_solver *s, const double *src, double *tar, int *its);
 int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, double *cSolid);
 int top_solver_opt_step(top_solver *s, top_opt_record *rec);
 int top_solver_opt_state(top_solver *s, int *loop, double *change, double *sharpness);
+/* get/set copy the physical and raw designs (either may be NULL) to/from
+ * device or host memory (any pointer CUDA's unified addressing accepts);
+ * set_design replaces the state the next opt_step starts from. */
 int top_solver_get_design(top_solver *s, double *xPhys, double *x);
+int top_solver_set_design(top_solver *s, const double *xPhys, const double *x);
 int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysOut,
                         top_opt_record *hist, int *nIter, double *cSolid);
 
@@ -241,6 +245,10 @@ int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysO
  * 3 level-1 K*u FP32; L2 is flushed by writing flushBytes before each launch.
  * No counterpart in the reference (its MATLAB driver times with tic/toc). */
 int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushBytes, double *msPerLaunch);
+
+/* Kernels this solver has launched since it was created (every entry point
+ * counts the launches it makes on the solver's stream). */
+int top_solver_launch_count(const top_solver *s, int64_t *count);
 
 /* Number of levels / load cases / DOFs of level 0. */
 int top_solver_sizes(const top_solver *s, int64_t *out3);

@@ -103,6 +103,8 @@ SIGNATURES = {
     "top_solver_opt_step": (_int, [_vp, _vp]),
     "top_solver_opt_state": (_int, [_vp, _vp, _vp, _vp]),
     "top_solver_get_design": (_int, [_vp, _vp, _vp]),
+    "top_solver_set_design": (_int, [_vp, _vp, _vp]),
+    "top_solver_launch_count": (_int, [_vp, _vp]),
     "top_solver_optimize": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
 }
 

@@ -399,7 +399,9 @@ extern "C" int top_solver_filter_setup(top_solver *s, double rMin)
     }
     filter_kernel_matrix(rMin, f.KEF.k);
     filter_activity_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(l0.eleGrid, l0.Ne, f.act);
+    TOPGPU_COUNT_LAUNCH();
     filter_diag_kernel<<<dim3(l0.g.nbx, l0.g.NZ), kNodeThreads, 0, s->st>>>(f.KEF, f.act, l0.g, l0.flags, f.invD);
+    TOPGPU_COUNT_LAUNCH();
     CK(cudaGetLastError());
     f.rMin = rMin;
     f.ready = true;
@@ -417,28 +419,39 @@ static int filter_apply(top_solver *s, const double *src, double *tar, int *itsO
     // nodal rhs: each element adds src/8 to its nodes
     CK(cudaMemsetAsync(f.eg - kMargin, 0, sizeof(double) * cs, st));
     elem_to_slots_kernel<<<nb256(l0.Ne), 256, 0, st>>>(src, l0.eleGrid, l0.Ne, 1.0 / 8.0, f.eg);
+    TOPGPU_COUNT_LAUNCH();
     slots_to_nodes_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, st>>>(f.eg, g, l0.flags, f.rhs);
+    TOPGPU_COUNT_LAUNCH();
     // PCG with the filter operator and Jacobi, tol_/10, maxIT_ (TOP_GPU.m:999-1001)
     const int VB = vb(ng);
     fpcg_init_kernel<<<VB, 256, 0, st>>>(f.rhs, f.x, f.r, f.z, f.p, f.invD, ng, s->red(&f.st->normB));
+    TOPGPU_COUNT_LAUNCH();
     fpcg_start_kernel<<<1, 1, 0, st>>>(f.st, s->p.tol / 10.0, s->p.maxIT);
+    TOPGPU_COUNT_LAUNCH();
     fpcg_zr_kernel<<<VB, 256, 0, st>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
+    TOPGPU_COUNT_LAUNCH();
     const int *done = &f.st->done;
     const int chunk = 8;
     PcgState h{};
     for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
         for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
             filter_apply_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, st>>>(f.KEF, f.act, f.p, f.v, g, s->red(&f.st->pv), done);
+            TOPGPU_COUNT_LAUNCH();
             fpcg_update_kernel<<<VB, 256, 0, st>>>(f.x, f.r, f.z, f.p, f.v, f.invD, ng, f.st, s->red(&f.st->rr));
+            TOPGPU_COUNT_LAUNCH();
             fpcg_check_kernel<<<1, 1, 0, st>>>(f.st);
+            TOPGPU_COUNT_LAUNCH();
             fpcg_zr_kernel<<<VB, 256, 0, st>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
+            TOPGPU_COUNT_LAUNCH();
             fpcg_p_kernel<<<VB, 256, 0, st>>>(f.p, f.z, ng, f.st);
+            TOPGPU_COUNT_LAUNCH();
         }
         CK(cudaMemcpyAsync(&h, f.st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (h.done) break;
     }
     nodes_to_elem_kernel<<<nb256(l0.Ne), 256, 0, st>>>(f.x, l0.eleGrid, g, l0.Ne, tar);
+    TOPGPU_COUNT_LAUNCH();
     CK(cudaGetLastError());
     if (itsOut) *itsOut = h.its;
     if (h.status == TOP_ERR_NAN) { set_error("PDE filter: non-finite PCG scalar"); return TOP_ERR_NAN; }
@@ -481,6 +494,7 @@ static int sensitivities(top_solver *s, int withGrad)
         s->Ke64, o.U, 3 * l0.g.cs, s->nLoads, s->weights, l0.eleGrid, l0.Ne, l0.g, o.xPhys, s->Ec,
         s->p.E0, s->p.Emin, s->p.penal, withGrad ? o.cSolid : 0.0, o.ce, withGrad ? o.dc : nullptr, o.dv,
         s->red(&o.sc->cObj));
+        TOPGPU_COUNT_LAUNCH();
     CK(cudaGetLastError());
     return TOP_OK;
 }
@@ -514,6 +528,7 @@ extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, do
     if (prm->ft != 0) { const int rc = top_solver_filter_setup(s, prm->rMin); if (rc) return rc; }
     // fully solid solve and its compliance (TOP_GPU.m:142-165)
     fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.tmp, s->p.E0, Ne);
+    TOPGPU_COUNT_LAUNCH();
     int rc = set_modulus_dev(s, o.tmp, 1, 0);
     if (rc) return rc;
     rc = top_solver_assemble(s);
@@ -528,7 +543,9 @@ extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, do
     CK(cudaStreamSynchronize(s->st));
     o.cSolid = o.hsc->cObj;       // cSolid = E0 * sum(ceList) with E = E0
     fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.xd, prm->V0, Ne);
+    TOPGPU_COUNT_LAUNCH();
     fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.xPhys, prm->V0, Ne);
+    TOPGPU_COUNT_LAUNCH();
     CK(cudaGetLastError());
     o.loop = 0; o.change = 1.0; o.sharp = 1.0;
     o.begun = true;
@@ -561,19 +578,23 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
     rc = sensitivities(s, 1);
     if (rc) return rc;
     sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 0, s->red(&o.sc->sumE));
+    TOPGPU_COUNT_LAUNCH();
     CK(cudaEventRecord(ev[3], st));
     // 5.3 filtering of the sensitivities
     int fits = 0;
     if (o.prm.ft == 1) {
         mul_kernel<<<VB, 256, 0, st>>>(o.xd, o.dc, o.tmp, Ne);
+        TOPGPU_COUNT_LAUNCH();
         rc = filter_apply(s, o.tmp, o.dc, &fits);
         if (rc) return rc;
         div_floor_kernel<<<VB, 256, 0, st>>>(o.dc, o.xd, o.dc, Ne);
+        TOPGPU_COUNT_LAUNCH();
     } else if (o.prm.ft == 2) {
         rc = filter_apply(s, o.dc, o.tmp, &fits);
-        if (!rc) { copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dc, Ne); rc = filter_apply(s, o.dv, o.tmp, &fits); }
+        if (!rc) { copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dc, Ne); TOPGPU_COUNT_LAUNCH(); rc = filter_apply(s, o.dv, o.tmp, &fits); }
         if (rc) return rc;
         copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dv, Ne);
+        TOPGPU_COUNT_LAUNCH();
     }
     CK(cudaEventRecord(ev[4], st));
     // 5.4 OC update; fval = mean(xPhys) - V0
@@ -590,12 +611,14 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
         double *xa = o.xd; const double *dca = o.dc, *dva = o.dv; double *pa = o.ocPartials; OptScalars *sca = o.sc;
         void *args[] = {&xa, &dca, &dva, &n, &pa, &sca, &move, &maxSteps};
         CK(cudaLaunchCooperativeKernel((const void *)oc_kernel, dim3(o.ocBlocks), dim3(256), args, 0, st));
+        TOPGPU_COUNT_LAUNCH();
     }
     CK(cudaEventRecord(ev[5], st));
     // xPhys (TOP_GPU.m:256-267): the new design, or its PDE-filtered version
     if (o.prm.ft == 2) { rc = filter_apply(s, o.xd, o.xPhys, &fits); if (rc) return rc; }
-    else copy_kernel<<<VB, 256, 0, st>>>(o.xd, o.xPhys, Ne);
+    else { copy_kernel<<<VB, 256, 0, st>>>(o.xd, o.xPhys, Ne); TOPGPU_COUNT_LAUNCH(); }
     sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 1, s->red(&o.sc->sharp));
+    TOPGPU_COUNT_LAUNCH();
     CK(cudaEventRecord(ev[6], st));
     CK(cudaMemcpyAsync(o.hsc, o.sc, sizeof(OptScalars), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -638,9 +661,26 @@ extern "C" int top_solver_get_design(top_solver *s, double *xPhys, double *x)
     if (!s || !s->optState || !opt(s).begun) return TOP_ERR_STATE;
     OptState &o = opt(s);
     const int64_t Ne = s->L[0].Ne;
-    if (xPhys) CK(cudaMemcpyAsync(xPhys, o.xPhys, sizeof(double) * Ne, cudaMemcpyDeviceToDevice, s->st));
-    if (x) CK(cudaMemcpyAsync(x, o.xd, sizeof(double) * Ne, cudaMemcpyDeviceToDevice, s->st));
+    if (xPhys) CK(cudaMemcpyAsync(xPhys, o.xPhys, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
+    if (x) CK(cudaMemcpyAsync(x, o.xd, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
     CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_set_design(top_solver *s, const double *xPhys, const double *x)
+{
+    if (!s || !s->optState || !opt(s).begun) return TOP_ERR_STATE;
+    OptState &o = opt(s);
+    const int64_t Ne = s->L[0].Ne;
+    if (xPhys) CK(cudaMemcpyAsync(o.xPhys, xPhys, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
+    if (x) CK(cudaMemcpyAsync(o.xd, x, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
+    return TOP_OK;
+}
+
+extern "C" int top_solver_launch_count(const top_solver *s, int64_t *count)
+{
+    if (!s || !count) return TOP_ERR_ARGS;
+    *count = s->launches;
     return TOP_OK;
 }
 

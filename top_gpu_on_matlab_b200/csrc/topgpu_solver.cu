@@ -396,6 +396,7 @@ void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, co
             keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
     else
         coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    TOPGPU_COUNT_LAUNCH();
 }
 
 // V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
@@ -419,12 +420,15 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
             restrict_kernel<T, 4><<<restrict_blocks<4>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
         else
             restrict_kernel<T, 2><<<restrict_blocks<2>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
+        TOPGPU_COUNT_LAUNCH();
     }
     // coarsest direct solve, FP64
     DevLevel &lc = s->L[nL - 1];
     const int64_t n = 3 * lc.Nn;
     coarsest_gather_kernel<T><<<nb256(n), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done);
+    TOPGPU_COUNT_LAUNCH();
     coarsest_gemv_kernel<T><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g, lc.nodeGrid, done);
+    TOPGPU_COUNT_LAUNCH();
     // interpolation leg
     for (int l = nL - 2; l >= 0; --l) {
         DevLevel &lv = s->L[l], &lcn = s->L[l + 1];
@@ -435,6 +439,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
                 prolong_kernel<T, 4, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
             else
                 prolong_kernel<T, 2, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
+            TOPGPU_COUNT_LAUNCH();
             level_op<T>(s, 0, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega},
                         zr ? s->red(zr) : none, done);
         } else {
@@ -442,6 +447,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
                 prolong_kernel<T, 4, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
             else
                 prolong_kernel<T, 2, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
+            TOPGPU_COUNT_LAUNCH();
             level_op<T>(s, l, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega}, none, done);
         }
     }
@@ -619,7 +625,10 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         if (!Fd) return fail("out of device memory");
         cudaMemcpy(Fd, mesh->F.data(), sizeof(double) * s->nd0 * s->nLoads, cudaMemcpyHostToDevice);
         for (int k = 0; k < s->nLoads; ++k)
+        {
             compact_to_grid_kernel<double, double><<<nb256(M0.Nn), 256>>>(Fd + (size_t)k * s->nd0, s->b + (size_t)k * 3 * cs0, l0.nodeGrid, M0.Nn, cs0);
+            TOPGPU_COUNT_LAUNCH();
+        }
     }
     // reduction scratch
     int64_t maxBlocks = 4096;
@@ -706,6 +715,7 @@ int topgpu::set_modulus_dev(top_solver *s, const double *src, int where, int sim
         d = s->tmp;
     }
     modulus_kernel<<<nb256(Ne), 256, 0, s->st>>>(d, simp, s->p.E0, s->p.Emin, s->p.penal, s->Ec, s->Eg64, s->Eg32, s->L[0].eleGrid, Ne);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     s->assembled = false;
     return TOP_OK;
@@ -729,36 +739,45 @@ extern "C" int top_solver_assemble(top_solver *s)
         if (rc) { set_error("top_solver_assemble: Galerkin kernel failed"); return rc; }
         if (l < s->nL - 1) {
             pack_ks_kernel<<<(unsigned)((d.Ne + kPackE - 1) / kPackE), 256, 0, st>>>(d.KsC, d.eleGrid, d.Ne, d.KsP64, d.KsP32, d.g.cs);
+            TOPGPU_COUNT_LAUNCH();
             diag_coarse_kernel<<<node_grid(d.g), kNodeThreads, 0, st>>>(d.KsP64, d.g, d.flags, d.diag, d.invD64, d.invD32);
+            TOPGPU_COUNT_LAUNCH();
         }
     }
     DevLevel &l0 = s->L[0];
     diag_l0_kernel<<<node_grid(l0.g), kNodeThreads, 0, st>>>(s->Ke64, s->Eg64, l0.flags, l0.g, s->p.E0, l0.diag, l0.invD64, l0.invD32);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     // coarsest matrix, Cholesky, inverse (TOP_GPU.m:1240-1255)
     DevLevel &lc = s->L[s->nL - 1];
     const int64_t n = s->nC;
     CK(cudaMemsetAsync(s->Ac, 0, sizeof(double) * n * n, st));
     coarsest_assemble_kernel<<<nb256(n), 256, 0, st>>>(lc.KsC, lc.nodeGrid, s->eleCompactC, s->nodeCompactC, lc.g, lc.Nn, s->Ac);
+    TOPGPU_COUNT_LAUNCH();
     CK(cudaMemsetAsync(s->zeroDone, 0, sizeof(int) * 4, st));
     for (int64_t k0 = 0; k0 < n; k0 += kCb) {
         const int kb = (int)std::min<int64_t>(kCb, n - k0);
         chol_diag_kernel<<<1, dim3(kCb, kCb), 0, st>>>(s->Ac, n, k0, kb, s->zeroDone + 1);
+        TOPGPU_COUNT_LAUNCH();
         const int64_t rest = n - k0 - kb;
         if (rest > 0) {
             chol_trsm_kernel<<<(unsigned)((rest + 127) / 128), 128, 0, st>>>(s->Ac, n, k0, kb);
+            TOPGPU_COUNT_LAUNCH();
             dim3 gs((unsigned)((rest + 15) / 16), (unsigned)((rest + 15) / 16));
             chol_syrk_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Ac, n, k0, kb);
+            TOPGPU_COUNT_LAUNCH();
         }
     }
     {
         const size_t sm = sizeof(double) * (size_t)n;   // one column of W per CTA
         if (sm > 48 * 1024) cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         tri_inv_kernel<<<(unsigned)n, 256, sm, st>>>(s->Ac, s->Wc, n);
+        TOPGPU_COUNT_LAUNCH();
     }
     {
         dim3 gs((unsigned)((n + 15) / 16), (unsigned)((n + 15) / 16));
         inv_gram_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Wc, s->Ainv, n);
+        TOPGPU_COUNT_LAUNCH();
     }
     CKL();
     int flag = 0;
@@ -779,12 +798,14 @@ extern "C" int top_solver_matvec(top_solver *s, int level, const double *u, doub
     const Reduce none{nullptr, nullptr, nullptr};
     CK(cudaMemsetAsync(d.x64 - kMargin, 0, sizeof(double) * 3 * d.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(u, d.x64, d.nodeGrid, d.Nn, d.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     if (fp32) {
         level_op<float>(s, level, VecIn<float, double>{d.x64, d.g.cs}, StoreOut<float, double>{d.t64, d.g.cs}, none, nullptr);
     } else {
         level_op<double>(s, level, VecIn<double, double>{d.x64, d.g.cs}, StoreOut<double, double>{d.t64, d.g.cs}, none, nullptr);
     }
     grid_to_compact_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(d.t64, y, d.nodeGrid, d.Nn, d.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return TOP_OK;
@@ -797,8 +818,10 @@ extern "C" int top_solver_vcycle(top_solver *s, const double *r, double *z)
     DevLevel &l0 = s->L[0];
     CK(cudaMemsetAsync(s->tmp - kMargin, 0, sizeof(double) * 3 * l0.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(r, s->tmp, l0.nodeGrid, l0.Nn, l0.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     precond(s, s->tmp, s->z, nullptr, s->zeroDone);
     grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(s->z, z, l0.nodeGrid, l0.Nn, l0.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return TOP_OK;
@@ -810,9 +833,12 @@ extern "C" int top_solver_restrict(top_solver *s, int ii, const double *rF, doub
     DevLevel &f = s->L[ii - 1], &c = s->L[ii];
     CK(cudaMemsetAsync(f.x64 - kMargin, 0, sizeof(double) * 3 * f.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(f.Nn), 256, 0, s->st>>>(rF, f.x64, f.nodeGrid, f.Nn, f.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     if (c.span == 4) restrict_kernel<double, 4><<<restrict_blocks<4>(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
     else restrict_kernel<double, 2><<<restrict_blocks<2>(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
+    TOPGPU_COUNT_LAUNCH();
     grid_to_compact_kernel<double, double><<<nb256(c.Nn), 256, 0, s->st>>>(c.t64, rC, c.nodeGrid, c.Nn, c.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return TOP_OK;
@@ -824,11 +850,14 @@ extern "C" int top_solver_interpolate(top_solver *s, int ii, const double *xC, d
     DevLevel &f = s->L[ii - 1], &c = s->L[ii];
     CK(cudaMemsetAsync(c.x64 - kMargin, 0, sizeof(double) * 3 * c.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(c.Nn), 256, 0, s->st>>>(xC, c.x64, c.nodeGrid, c.Nn, c.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     if (c.span == 4)
         prolong_kernel<double, 4, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.x64, c.g, f.t64, f.g, f.flags, nullptr, nullptr, 0.0, nullptr);
     else
         prolong_kernel<double, 2, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.x64, c.g, f.t64, f.g, f.flags, nullptr, nullptr, 0.0, nullptr);
+    TOPGPU_COUNT_LAUNCH();
     grid_to_compact_kernel<double, double><<<nb256(f.Nn), 256, 0, s->st>>>(f.t64, xF, f.nodeGrid, f.Nn, f.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return TOP_OK;
@@ -840,6 +869,7 @@ extern "C" int top_solver_get_diag(top_solver *s, int level, double *diag)
     if (!s->assembled) { set_error("top_solver_get_diag: assemble first"); return TOP_ERR_STATE; }
     DevLevel &d = s->L[level];
     grid_to_compact_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(d.diag, diag, d.nodeGrid, d.Nn, d.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return TOP_OK;
@@ -874,7 +904,9 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
     CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
     int *done = &s->state->done;
     dot_kernel<<<VB, 256, 0, st>>>(bGrid, bGrid, ng, cs, s->red(&s->state->normB));
+    TOPGPU_COUNT_LAUNCH();
     pcg_init_kernel<<<1, 1, 0, st>>>(s->state);
+    TOPGPU_COUNT_LAUNCH();
     if (!warm) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * 3 * cs, st));
     // r = b - A x
     if (s->p.outerFP32)
@@ -886,6 +918,7 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
     // z = M r ; rho = z . r ; p = z
     precond(s, s->r, s->z, &s->state->rho, done);
     pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 1);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     static const bool trace = std::getenv("TOPGPU_PCG_TRACE") != nullptr;
     const int chunk = trace ? 1 : 4;
@@ -893,11 +926,14 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
         for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
             outer_op(s, s->pv, s->v, &s->state->pv, done);                                   // v = A p, p.v
             pcg_update_kernel<<<VB, 256, 0, st>>>(xg, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
+            TOPGPU_COUNT_LAUNCH();
             pcg_check_kernel<<<1, 1, 0, st>>>(s->state);
+            TOPGPU_COUNT_LAUNCH();
             precond(s, s->r, s->z, &s->state->rho, done);                                     // z = M r, z.r
             pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 0);              // p = z + beta p
         }
         CKL();
+        TOPGPU_COUNT_LAUNCH();
         CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (trace && it0 < 12)
@@ -920,10 +956,14 @@ static int pcg_run(top_solver *s, const double *bGrid, double *U, int warm, int 
     DevLevel &l0 = s->L[0];
     const int64_t cs = l0.g.cs;
     CK(cudaMemsetAsync(s->x - kMargin, 0, sizeof(double) * 3 * cs, s->st));
-    if (warm) compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U, s->x, l0.nodeGrid, l0.Nn, cs);
+    if (warm) {
+        compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U, s->x, l0.nodeGrid, l0.Nn, cs);
+        TOPGPU_COUNT_LAUNCH();
+    }
     const int rc = pcg_grid(s, bGrid, s->x, 1, itsOut, resOut);
     if (rc != TOP_OK && rc != TOP_ERR_NOT_CONVERGED) return rc;
     grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(s->x, U, l0.nodeGrid, l0.Nn, cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return rc;
@@ -941,6 +981,7 @@ extern "C" int top_solver_pcg_rhs(top_solver *s, const double *b, double *U, int
     DevLevel &l0 = s->L[0];
     CK(cudaMemsetAsync(s->tmp - kMargin, 0, sizeof(double) * 3 * l0.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(b, s->tmp, l0.nodeGrid, l0.Nn, l0.g.cs);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     return pcg_run(s, s->tmp, U, warm, its, relres);
 }
@@ -956,7 +997,9 @@ extern "C" int top_solver_unit_compliance(top_solver *s, const double *U, double
     Ug = s->tmp;
     CK(cudaMemsetAsync(Ug - kMargin, 0, sizeof(double) * 3 * cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U, Ug, l0.nodeGrid, l0.Nn, cs);
+    TOPGPU_COUNT_LAUNCH();
     compliance_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(s->Ke64, Ug, 3 * cs, 1, s->weights, l0.eleGrid, l0.Ne, l0.g, ce);
+    TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));
     return TOP_OK;

@@ -54,6 +54,7 @@ struct top_solver {
     int64_t nC = 0; double *Ac = nullptr, *Ainv = nullptr, *Wc = nullptr, *cr = nullptr;
     int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
     bool assembled = false;
+    int64_t launches = 0;            // kernels launched by this solver (all entry points)
     void *filterState = nullptr, *optState = nullptr;   // topgpu_opt.cu
     std::vector<double> Fhost; int64_t nd0 = 0;
 
@@ -73,6 +74,9 @@ struct top_solver {
     }
     Reduce red(double *result) const { return Reduce{partials, counter, result}; }
 };
+
+// every kernel launch of the solver is counted on the solver it serves
+#define TOPGPU_COUNT_LAUNCH() (++s->launches)
 
 namespace topgpu {
 // PCG (TOP_GPU.m:602-667) on level-0 grid vectors: b and x in the solver's

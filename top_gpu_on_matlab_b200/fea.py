@@ -244,6 +244,31 @@ class Solver:
         check(lib().top_solver_get_design(self._h, xp.data_ptr(), x.data_ptr()), "top_solver_get_design")
         return xp, x
 
+    def set_design(self, xPhys=None, x=None):
+        """Replace the design the next opt_step starts from (device or pinned/pageable host tensors)."""
+        ne = self.levels[0]["numElements"]
+        ptrs = []
+        for v in (xPhys, x):
+            if v is None:
+                ptrs.append(None)
+                continue
+            if v.dtype != torch.float64 or v.numel() != ne or not v.is_contiguous():
+                raise ValueError("set_design: contiguous float64 vectors of numElements expected")
+            ptrs.append(v.data_ptr())
+        check(lib().top_solver_set_design(self._h, ptrs[0], ptrs[1]), "top_solver_set_design")
+
+    def get_design_into(self, xPhys=None, x=None):
+        """Copy the current design into given tensors (device or host); blocks until done."""
+        check(lib().top_solver_get_design(self._h, None if xPhys is None else xPhys.data_ptr(),
+                                          None if x is None else x.data_ptr()), "top_solver_get_design")
+
+    @property
+    def launches(self):
+        """Kernels launched by this solver since creation."""
+        n = C.c_int64(0)
+        check(lib().top_solver_launch_count(self._h, C.byref(n)), "top_solver_launch_count")
+        return n.value
+
     def optimize(self, V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1):
         """TOP_GPU's optimisation loop on the device; returns (xPhys, history, cSolid)."""
         prm = OptParams(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
