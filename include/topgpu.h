@@ -246,6 +246,19 @@ int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysO
  * No counterpart in the reference (its MATLAB driver times with tic/toc). */
 int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushBytes, double *msPerLaunch);
 
+/* Level-0 stiffness product kernel, per precision (fp32 = 0: the FP64
+ * products, 1: the FP32 V-cycle products).  kind 0 = node-centric product
+ * with the dense 24x24 Ke; kind 1 = Ke in the Walsh-Hadamard basis of the
+ * cube element (eight 3x3 blocks), z-marching tiles of ty x tx element
+ * columns, each of ctas CTAs marching an equal share of the (tile, z-layer)
+ * work (ctas = 0: as many CTAs as fit on the GPU at once); tile shapes
+ * 16x16 and 16x8.  kind 1 needs Ke with the cube's reflection
+ * symmetry (always the case for the reference's isotropic voxel) and is the
+ * default then.  get returns {kind, ty, tx, ctas}.  No counterpart in the
+ * reference. */
+int top_solver_set_l0_kernel(top_solver *s, int fp32, int kind, int ty, int tx, int ctas);
+int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);
+
 /* Kernels this solver has launched since it was created (every entry point
  * counts the launches it makes on the solver's stream). */
 int top_solver_launch_count(const top_solver *s, int64_t *count);

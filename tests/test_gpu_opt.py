@@ -74,3 +74,26 @@ def test_mixed_precision_loop_tracks_fp64():
     c64, c32 = np.array(res[False][1]), np.array(res[True][1])
     assert np.abs(c32 - c64).max() <= 1e-6 * np.abs(c64).max()
     assert np.abs(res[True][0] - res[False][0]).max() <= 1e-4
+
+
+def test_design_host_round_trip_and_launch_count():
+    """set_design / get_design through pinned host memory: an iteration
+    started from a design that went down and up again equals one started
+    from the device state; every step launches kernels."""
+    _, a = _pair(np.ones((8, 16, 8), bool), 1, 1e-9)
+    _, b = _pair(np.ones((8, 16, 8), bool), 1, 1e-9)
+    a.opt_begin(V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1)
+    b.opt_begin(V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1)
+    ra, rb = a.opt_step(), b.opt_step()
+    ne = a.levels[0]["numElements"]
+    xp = torch.empty(ne, dtype=torch.float64).pin_memory()
+    x = torch.empty(ne, dtype=torch.float64).pin_memory()
+    b.get_design_into(xp, x)
+    b.set_design(xp, x)
+    n0 = b.launches
+    ra, rb = a.opt_step(), b.opt_step()
+    assert b.launches > n0
+    assert ra["c"] == rb["c"]
+    xa, _ = a.design()
+    xb, _ = b.design()
+    assert torch.equal(xa, xb)

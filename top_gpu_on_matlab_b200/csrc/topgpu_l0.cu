@@ -1,0 +1,110 @@
+// topgpu_l0.cu -- level-0 stiffness product dispatch of the fused solver:
+// the node-centric kernel with the dense 24x24 Ke (topgpu_grid.cuh) or the
+// Walsh-basis tile kernel (topgpu_walsh.cuh), per precision, with the
+// operand/epilogue combinations the solver uses instantiated here.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include "topgpu_solver_impl.cuh"
+
+namespace topgpu {
+namespace {
+
+template <typename T> const KeParam<T> &keparam(const top_solver *s);
+template <> const KeParam<double> &keparam<double>(const top_solver *s) { return s->Ke64; }
+template <> const KeParam<float> &keparam<float>(const top_solver *s) { return s->Ke32; }
+template <typename T> const T *egrid(const top_solver *s);
+template <> const double *egrid<double>(const top_solver *s) { return s->Eg64; }
+template <> const float *egrid<float>(const top_solver *s) { return s->Eg32; }
+template <typename T> const WalshParam<T> &walshparam(const top_solver *s);
+template <> const WalshParam<double> &walshparam<double>(const top_solver *s) { return s->W64; }
+template <> const WalshParam<float> &walshparam<float>(const top_solver *s) { return s->W32; }
+template <typename T> constexpr int prec_slot() { return sizeof(T) == 8 ? 0 : 1; }
+
+// tile shapes the Walsh-basis kernel is built for
+#define TOPGPU_WALSH_SHAPES(X) X(16, 16) X(16, 8)
+
+bool walsh_shape_ok(int ty, int tx)
+{
+#define TOPGPU_SHAPE_OK(A, B) if (ty == A && tx == B) return true;
+    TOPGPU_WALSH_SHAPES(TOPGPU_SHAPE_OK)
+#undef TOPGPU_SHAPE_OK
+    return false;
+}
+
+// grid of the Walsh kernel: the configured CTA count (0: the CTAs that fit
+// on the GPU at once), at most one per (tile, layer) work item
+template <typename T, int A, int B, class In, class Out>
+unsigned l0w_ctas(const top_solver *s, const top_solver::L0Kernel &k)
+{
+    static const int occ = [] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0w_kernel<T, A, B, In, Out>, A * B, 0) != cudaSuccess) n = 1;
+        return n > 0 ? n : 1;
+    }();
+    const DevLevel &lv = s->L[0];
+    const int64_t work = (int64_t)walsh_tiles(lv.g, A, B) * lv.g.NZ;
+    int64_t n = k.ctas > 0 ? k.ctas : (int64_t)s->numSMs * occ;
+    n = std::min<int64_t>(std::min<int64_t>(n, work), s->nPartials);
+    return (unsigned)std::max<int64_t>(n, 1);
+}
+
+}  // namespace
+
+template <typename T, class In, class Out>
+void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done)
+{
+    DevLevel &lv = s->L[0];
+    const top_solver::L0Kernel &k = s->l0k[prec_slot<T>()];
+    if (k.kind == 1) {
+#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                     \
+        if (k.ty == A && k.tx == B)                                                                   \
+            l0w_kernel<T, A, B, In, Out><<<l0w_ctas<T, A, B, In, Out>(s, k), A * B, 0, s->st>>>(      \
+                walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
+        TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
+#undef TOPGPU_LAUNCH_SHAPE
+    } else {
+        l0_kernel<T, In, Out><<<dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ), kNodeThreads, 0, s->st>>>(
+            keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
+    }
+    TOPGPU_COUNT_LAUNCH();
+}
+
+int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
+{
+    top_solver::L0Kernel &k = s->l0k[p];
+    if (kind == 0) { k.kind = 0; return TOP_OK; }
+    if (kind != 1 || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0) return TOP_ERR_ARGS;
+    DevLevel &l0 = s->L[0];
+    const int tiles = walsh_tiles(l0.g, ty, tx);
+    if (ctas > s->nPartials) {                         // one reduction partial per CTA
+        double *pp = s->dalloc<double>((size_t)ctas);
+        if (!pp) return TOP_ERR_NOMEM;
+        s->partials = pp; s->nPartials = ctas;
+    }
+    if (k.mask) { cudaFree(k.mask); k.mask = nullptr; }
+    if (cudaMalloc(&k.mask, (size_t)tiles) != cudaSuccess) { k.mask = nullptr; k.kind = 0; return TOP_ERR_NOMEM; }
+#define TOPGPU_MASK_SHAPE(A, B) \
+    if (ty == A && tx == B) walsh_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask);
+    TOPGPU_WALSH_SHAPES(TOPGPU_MASK_SHAPE)
+#undef TOPGPU_MASK_SHAPE
+    TOPGPU_COUNT_LAUNCH();
+    if (cudaGetLastError() != cudaSuccess) return TOP_ERR_CUDA;
+    k.kind = 1; k.ty = ty; k.tx = tx; k.ctas = ctas;
+    return TOP_OK;
+}
+
+// the operand / epilogue pairs of the solver's level-0 products
+using VIdd = VecIn<double, double>;  using VIff = VecIn<float, float>;  using VIfd = VecIn<float, double>;
+using JIdd = JacobiIn<double, double>; using JIfd = JacobiIn<float, double>;
+template void l0_op<double, VIdd, StoreOut<double, double>>(top_solver *, const VIdd &, const StoreOut<double, double> &, Reduce, const int *);
+template void l0_op<double, JIdd, ResidOut<double, double, double>>(top_solver *, const JIdd &, const ResidOut<double, double, double> &, Reduce, const int *);
+template void l0_op<double, VIdd, PostSmoothOut<double, double, double>>(top_solver *, const VIdd &, const PostSmoothOut<double, double, double> &, Reduce, const int *);
+template void l0_op<double, VIdd, DotStoreOut<double, double, double>>(top_solver *, const VIdd &, const DotStoreOut<double, double, double> &, Reduce, const int *);
+template void l0_op<double, VIdd, ResidOut<double, double, double>>(top_solver *, const VIdd &, const ResidOut<double, double, double> &, Reduce, const int *);
+template void l0_op<float, JIfd, ResidOut<float, double, float>>(top_solver *, const JIfd &, const ResidOut<float, double, float> &, Reduce, const int *);
+template void l0_op<float, VIff, PostSmoothOut<float, double, double>>(top_solver *, const VIff &, const PostSmoothOut<float, double, double> &, Reduce, const int *);
+template void l0_op<float, VIfd, DotStoreOut<float, double, double>>(top_solver *, const VIfd &, const DotStoreOut<float, double, double> &, Reduce, const int *);
+template void l0_op<float, VIfd, StoreOut<float, double>>(top_solver *, const VIfd &, const StoreOut<float, double> &, Reduce, const int *);
+template void l0_op<float, VIfd, ResidOut<float, double, double>>(top_solver *, const VIfd &, const ResidOut<float, double, double> &, Reduce, const int *);
+template void l0_op<float, VIff, StoreOut<float, float>>(top_solver *, const VIff &, const StoreOut<float, float> &, Reduce, const int *);
+}  // namespace topgpu

@@ -386,17 +386,20 @@ template <typename T> const T *egrid(const top_solver *s);
 template <> const double *egrid<double>(const top_solver *s) { return s->Eg64; }
 template <> const float *egrid<float>(const top_solver *s) { return s->Eg32; }
 
-// y-epilogue applied to (K_level in)(node) for every node of the level
+// y-epilogue applied to (K_level in)(node) for every node of a coarse level
+template <typename T, class In, class Out>
+void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done)
+{
+    DevLevel &lv = s->L[l];
+    coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    TOPGPU_COUNT_LAUNCH();
+}
+// ... of any level (level 0: the configured level-0 kernel, topgpu_l0.cu)
 template <typename T, class In, class Out>
 void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done)
 {
-    DevLevel &lv = s->L[l];
-    if (l == 0)
-        l0_kernel<T, In, Out><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(
-            keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
-    else
-        coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
-    TOPGPU_COUNT_LAUNCH();
+    if (l == 0) l0_op<T>(s, in, out, red, done);
+    else coarse_op<T>(s, l, in, out, red, done);
 }
 
 // V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
@@ -413,9 +416,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
         if (l == 0)
-            level_op<T>(s, l, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega}, ResidOut<T, TR, T>{r0, d, lv.g.cs}, none, done);
+            l0_op<T>(s, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega}, ResidOut<T, TR, T>{r0, d, lv.g.cs}, none, done);
         else
-            level_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs}, none, done);
+            coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs}, none, done);
         if (lc.span == 4)
             restrict_kernel<T, 4><<<restrict_blocks<4>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
         else
@@ -440,7 +443,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
             else
                 prolong_kernel<T, 2, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
             TOPGPU_COUNT_LAUNCH();
-            level_op<T>(s, 0, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega},
+            l0_op<T>(s, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega},
                         zr ? s->red(zr) : none, done);
         } else {
             if (lcn.span == 4)
@@ -448,7 +451,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
             else
                 prolong_kernel<T, 2, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
             TOPGPU_COUNT_LAUNCH();
-            level_op<T>(s, l, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega}, none, done);
+            coarse_op<T>(s, l, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega}, none, done);
         }
     }
 }
@@ -466,9 +469,9 @@ void outer_op(top_solver *s, const double *u, double *y, double *uy, const int *
     DevLevel &l0 = s->L[0];
     const Reduce red = uy ? s->red(uy) : Reduce{nullptr, nullptr, nullptr};
     if (s->p.outerFP32)
-        level_op<float>(s, 0, VecIn<float, double>{u, l0.g.cs}, DotStoreOut<float, double, double>{y, u, l0.g.cs}, red, done);
+        l0_op<float>(s, VecIn<float, double>{u, l0.g.cs}, DotStoreOut<float, double, double>{y, u, l0.g.cs}, red, done);
     else
-        level_op<double>(s, 0, VecIn<double, double>{u, l0.g.cs}, DotStoreOut<double, double, double>{y, u, l0.g.cs}, red, done);
+        l0_op<double>(s, VecIn<double, double>{u, l0.g.cs}, DotStoreOut<double, double, double>{y, u, l0.g.cs}, red, done);
 }
 
 }  // namespace
@@ -567,6 +570,9 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     DevLevel &l0 = s->L[0];
     const MeshLevel &M0 = mesh->L[0];
     for (int t = 0; t < 576; ++t) { s->Ke64.k[t] = M0.Ke[t]; s->Ke32.k[t] = float(M0.Ke[t]); }
+    s->walshOK = walsh_blocks(M0.Ke, s->W64) < 1e-12;
+    for (int t = 0; t < 8; ++t)
+        for (int k = 0; k < 9; ++k) s->W32.b[t][k] = float(s->W64.b[t][k]);
     s->KeDev = s->dalloc<double>(576);
     s->Ec = s->dalloc<double>(M0.Ne);
     s->Eg64 = s->galloc<double>(l0.g.cs, 1);
@@ -675,6 +681,15 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         cudaMemcpy(s->nodeCompactC, nc.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
         s->eleCompactC += kMargin; s->nodeCompactC += kMargin;
     }
+    {
+        int dev = 0, nsm = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
+            s->numSMs = nsm;
+    }
+    // level-0 products in the Walsh basis where Ke allows it
+    if (s->walshOK)
+        for (int pslot = 0; pslot < 2; ++pslot)
+            if (set_l0_kernel(s, pslot, 1, 16, 8, (pslot ? 12 : 8) * s->numSMs) != TOP_OK) return fail("level-0 kernel setup");
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) { set_error("top_solver_create: %s", cudaGetErrorString(err)); top_solver_destroy(s); return TOP_ERR_CUDA; }
     *out = s;
@@ -685,9 +700,24 @@ extern "C" int top_solver_destroy(top_solver *s)
 {
     if (!s) return TOP_OK;
     free_opt_state(s);
+    for (auto &k : s->l0k) if (k.mask) cudaFree(k.mask);
     for (void *p : s->allocs) cudaFree(p);
     if (s->hstate) cudaFreeHost(s->hstate);
     delete s;
+    return TOP_OK;
+}
+
+extern "C" int top_solver_set_l0_kernel(top_solver *s, int fp32, int kind, int ty, int tx, int ctas)
+{
+    if (!s) return TOP_ERR_ARGS;
+    return set_l0_kernel(s, fp32 ? 1 : 0, kind, ty, tx, ctas);
+}
+
+extern "C" int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4)
+{
+    if (!s || !out4) return TOP_ERR_ARGS;
+    const top_solver::L0Kernel &k = s->l0k[fp32 ? 1 : 0];
+    out4[0] = k.kind; out4[1] = k.ty; out4[2] = k.tx; out4[3] = k.ctas;
     return TOP_OK;
 }
 
@@ -910,10 +940,10 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
     if (!warm) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * 3 * cs, st));
     // r = b - A x
     if (s->p.outerFP32)
-        level_op<float>(s, 0, VecIn<float, double>{xg, cs}, ResidOut<float, double, double>{bGrid, s->r, cs},
+        l0_op<float>(s, VecIn<float, double>{xg, cs}, ResidOut<float, double, double>{bGrid, s->r, cs},
                         Reduce{nullptr, nullptr, nullptr}, done);
     else
-        level_op<double>(s, 0, VecIn<double, double>{xg, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
+        l0_op<double>(s, VecIn<double, double>{xg, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
                          Reduce{nullptr, nullptr, nullptr}, done);
     // z = M r ; rho = z . r ; p = z
     precond(s, s->r, s->z, &s->state->rho, done);
@@ -1025,10 +1055,10 @@ extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_
         if (flush) CK(cudaMemsetAsync(flush, k & 0xff, (size_t)flushBytes, s->st));
         CK(cudaEventRecord(a, s->st));
         switch (which) {
-        case 0: level_op<double>(s, 0, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr); break;
-        case 1: level_op<float>(s, 0, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr); break;
+        case 0: l0_op<double>(s, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr); break;
+        case 1: l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr); break;
         case 2: precond(s, s->r, s->z, nullptr, s->zeroDone); break;
-        case 3: if (s->nL > 2) level_op<float>(s, 1, VecIn<float, float>{s->L[1].x32, s->L[1].g.cs}, StoreOut<float, float>{s->L[1].t32, s->L[1].g.cs}, none, nullptr); break;
+        case 3: if (s->nL > 2) coarse_op<float>(s, 1, VecIn<float, float>{s->L[1].x32, s->L[1].g.cs}, StoreOut<float, float>{s->L[1].t32, s->L[1].g.cs}, none, nullptr); break;
         default: set_error("top_solver_time_kernel: unknown kernel %d", which); return TOP_ERR_ARGS;
         }
         CK(cudaEventRecord(b, s->st));

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <vector>
 #include "topgpu_grid.cuh"
+#include "topgpu_walsh.cuh"
 
 namespace topgpu {
 
@@ -39,6 +40,14 @@ struct top_solver {
     std::vector<DevLevel> L;
     std::vector<void *> allocs;      // raw allocations (freed on destroy)
     topgpu::KeParam<double> Ke64{}; topgpu::KeParam<float> Ke32{};
+    // level-0 product: kind 0 = node-centric dense Ke, 1 = Walsh-basis tiles
+    // of ty x tx element columns on ctas CTAs (0: as many as fit at once);
+    // per precision, set by top_solver_set_l0_kernel or the autotuner
+    struct L0Kernel { int kind = 0, ty = 16, tx = 16, ctas = 0; uint8_t *mask = nullptr; };
+    int numSMs = 148;
+    L0Kernel l0k[2];                 // [0] FP64, [1] FP32
+    bool walshOK = false;            // Ke has the cube's reflection symmetry
+    topgpu::WalshParam<double> W64{}; topgpu::WalshParam<float> W32{};
     double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
     double *Ec = nullptr, *Eg64 = nullptr; float *Eg32 = nullptr;
     int32_t *mapUnique = nullptr; double *uFree = nullptr, *uFixed = nullptr; int64_t nU = 0;
@@ -79,6 +88,12 @@ struct top_solver {
 #define TOPGPU_COUNT_LAUNCH() (++s->launches)
 
 namespace topgpu {
+// y-epilogue applied to (K_0 in)(node) for every level-0 node, with the
+// level-0 kernel configured for precision T (topgpu_l0.cu)
+template <typename T, class In, class Out>
+void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done);
+// configure the level-0 kernel of precision slot p (0 FP64, 1 FP32)
+int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas);
 // PCG (TOP_GPU.m:602-667) on level-0 grid vectors: b and x in the solver's
 // SoA grid layout, x holds the warm start when warm != 0 and the solution.
 int pcg_grid(top_solver *s, const double *bGrid, double *xGrid, int warm, int *itsOut, double *resOut);

@@ -1,0 +1,294 @@
+// topgpu_walsh.cuh -- level-0 stiffness product in the Walsh-Hadamard basis
+// of the voxel element.
+//
+// The 8-node unit-cube element of an isotropic material is invariant under
+// the three axis reflections of the cube (a reflection along axis k swaps the
+// corner pairs across k and flips the sign of displacement component k).
+// Those reflections commute, so they diagonalise together: with the Walsh
+// functions w_s(a) = (-1)^(s_y dy(a) + s_x dx(a) + s_z dz(a)) over the
+// corners a (s = s_y + 2 s_x + 4 s_z), and U[c][s] = sum_a w_s(a) u[a][c],
+//
+//     Ke u = W (B U),   (W V)[a][c] = sum_s w_s(a) V[c][s],
+//
+// where B couples U[c][s] only to U[c'][s'] with s ^ e(c) == s' ^ e(c')
+// (e(c) = the bit of component c's own axis): eight 3x3 blocks, one per
+// character t = s ^ e(c), with 45 nonzero entries in all (the rest vanish
+// by the cube's diagonal symmetries).  The element product then costs two
+// 8-point Walsh transforms per component (add/subtract butterflies) plus
+// 45 multiply-adds, instead of the 576 multiply-adds of the dense 24x24 Ke.
+//
+// The kernel marches along z through a 2-D tile of element columns: each
+// thread owns one element column, keeps the (y, x) Walsh transform of the
+// node layer below it from the previous step (the z butterfly is the only
+// part that needs both layers), and sums the Walsh-domain output of the two
+// elements sharing a node layer before transforming back.  Node sums across
+// the four element columns around a node go through shared memory in a
+// fixed order, so results are deterministic.  Tiles overlap by one column:
+// a tile of TY x TX element columns produces (TY-1) x (TX-1) node columns.
+#pragma once
+#include "topgpu_grid.cuh"
+
+namespace topgpu {
+
+template <typename T> struct WalshParam { T b[8][9]; };   // B_t[c][c'] at b[t][3c+c']
+
+// bit of s along the axis of displacement component c (x -> s_x, y -> s_y, z -> s_z)
+__host__ __device__ constexpr int walsh_axis_bit(int c) { return c == 0 ? 2 : (c == 1 ? 1 : 4); }
+// nonzero entries (bit 3c+c') of block t for the isotropic unit cube
+__host__ __device__ constexpr unsigned walsh_pattern(int t)
+{
+    return t == 0 ? 0x1FFu : t == 1 ? 0x145u : t == 2 ? 0x1B0u : t == 3 ? 0x11Bu
+         : t == 4 ? 0x01Bu : t == 5 ? 0x1B1u : t == 6 ? 0x155u : 0x1FFu;
+}
+__host__ __device__ constexpr int walsh_sign(int s, int a)
+{
+    return ((((s & 1) * cdy(a)) + (((s >> 1) & 1) * cdx(a)) + (((s >> 2) & 1) * cdz(a))) & 1) ? -1 : 1;
+}
+
+// Blocks of Ke (column-major 24x24, corner order of the element node map)
+// in the Walsh basis, scaled by 1/64.  Returns the largest entry of Ke's
+// Walsh form outside the block pattern relative to max |Ke|: zero up to
+// rounding for a cube element of an isotropic material.
+inline double walsh_blocks(const double *Ke, WalshParam<double> &P)
+{
+    double kmax = 0.0, off = 0.0;
+    for (int i = 0; i < 576; ++i) kmax = Ke[i] > kmax ? Ke[i] : (-Ke[i] > kmax ? -Ke[i] : kmax);
+    for (int s = 0; s < 8; ++s)
+        for (int c = 0; c < 3; ++c)
+            for (int s2 = 0; s2 < 8; ++s2)
+                for (int d = 0; d < 3; ++d) {
+                    double m = 0.0;
+                    for (int a = 0; a < 8; ++a)
+                        for (int b = 0; b < 8; ++b)
+                            m += walsh_sign(s, a) * Ke[(3 * a + c) + 24 * (3 * b + d)] * walsh_sign(s2, b);
+                    m /= 64.0;
+                    const int t = s ^ walsh_axis_bit(c);
+                    const bool inBlock = (s2 ^ walsh_axis_bit(d)) == t && ((walsh_pattern(t) >> (3 * c + d)) & 1u);
+                    if (inBlock) P.b[t][3 * c + d] = m;
+                    else off = (m < 0 ? -m : m) > off ? (m < 0 ? -m : m) : off;
+                }
+    for (int t = 0; t < 8; ++t)
+        for (int k = 0; k < 9; ++k)
+            if (!((walsh_pattern(t) >> k) & 1u)) P.b[t][k] = 0.0;
+    return kmax > 0 ? off / kmax : 0.0;
+}
+
+// (y, x) butterfly of four corner values v[by + 2 bx]; its own inverse up to 1/4
+template <typename T>
+__device__ __forceinline__ void walsh2(T v[4])
+{
+    const T p0 = v[0] + v[1], m0 = v[0] - v[1], p1 = v[2] + v[3], m1 = v[2] - v[3];
+    v[0] = p0 + p1; v[1] = m0 + m1; v[2] = p0 - p1; v[3] = m0 - m1;
+}
+
+template <typename T, int TY, int TX> struct WalshTile {
+    static constexpr int NT = TY * TX;                      // threads = element columns
+    static constexpr int NS = (TY + 1) * (TX + 1);          // staged node columns
+    static constexpr int R = (3 * NS + NT - 1) / NT;        // staged values per thread
+    // y stride of a staged column in shared memory, chosen so that the
+    // (ty + by, tx + bx) reads of a warp (of a half-warp for 8-byte values)
+    // fall in distinct banks
+    static constexpr int SY = sizeof(T) == 4 ? (TY < 32 ? TY + 32 : TY + 1) : (TY == 8 ? 24 : TY + 1);
+    static constexpr int SC = SY * (TX + 1);                // one component
+};
+
+__host__ __device__ inline int walsh_tiles(const Geom &g, int TY, int TX)
+{
+    return ((g.NY + TY - 2) / (TY - 1)) * ((g.NX + TX - 2) / (TX - 1));
+}
+
+// one z-range [z0, z1) of node layers of tile (y0, x0): element layers
+// z0-1 .. z1-1 are visited, the first only for its top-layer carry
+template <typename T, int TY, int TX, bool MASK, class In, class Out>
+__device__ __forceinline__ void l0w_march(const WalshParam<T> &B, const In &in, const Out &out,
+                                          const T *__restrict__ E, const uint8_t *__restrict__ flags,
+                                          const Geom &g, int y0, int x0, int z0, int z1, T E0,
+                                          T *su, T *so, double &dot)
+{
+    using Tl = WalshTile<T, TY, TX>;
+    const int tid = threadIdx.x, ty = tid % TY, tx = tid / TY;
+    const int PY = g.PY, PL = (int)g.plane;
+    // staged node columns of this thread: (Y, X) = (y0-1+j, x0-1+i); outside
+    // [-1, NY] x [-1, NX] they are not guard slots and stage as zero
+    int sOff[Tl::R], sComp[Tl::R], sDst[Tl::R];
+    bool sOn[Tl::R];
+#pragma unroll
+    for (int r = 0; r < Tl::R; ++r) {
+        const int k = tid + r * Tl::NT;
+        const int c = k / Tl::NS, q = k % Tl::NS, j = q % (TY + 1), i = q / (TY + 1);
+        const int Y = y0 - 1 + j, X = x0 - 1 + i;
+        sOn[r] = k < 3 * Tl::NS && Y <= g.NY && X <= g.NX;
+        sComp[r] = c < 3 ? c : 0;
+        sDst[r] = k < 3 * Tl::NS ? c * Tl::SC + j + Tl::SY * i : -1;
+        sOff[r] = sOn[r] ? (int)(g.origin + Y + (int64_t)PY * X) : 0;
+    }
+    T pre[Tl::R];
+    auto fetch = [&](int z) {
+#pragma unroll
+        for (int r = 0; r < Tl::R; ++r) {
+            T v = T(0);
+            if (sOn[r]) {
+                const int m = sOff[r] + PL * z;
+                v = in(m, sComp[r]);
+                if (MASK && (flags[m] & (1 << sComp[r]))) v = T(0);
+            }
+            pre[r] = v;
+        }
+    };
+    auto stage = [&]() {
+#pragma unroll
+        for (int r = 0; r < Tl::R; ++r)
+            if (sDst[r] >= 0) su[sDst[r]] = pre[r];
+    };
+    // element column of this thread
+    const int ey = y0 - 1 + ty, ex = x0 - 1 + tx;
+    const bool eOn = ey <= g.NY - 1 && ex <= g.NX - 1;
+    const int eOff = eOn ? (int)(g.origin + ey + (int64_t)PY * ex) : 0;
+    // node of this thread (corner (0,0) of its element column) and whether it is an output
+    const bool nOut = ty >= 1 && tx >= 1 && ey < g.NY && ex < g.NX;
+    auto corners = [&](T h[3][4]) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+            for (int bx = 0; bx < 2; ++bx)
+#pragma unroll
+                for (int by = 0; by < 2; ++by)
+                    h[c][by + 2 * bx] = su[c * Tl::SC + (ty + by) + Tl::SY * (tx + bx)];
+            walsh2(h[c]);
+        }
+    };
+
+    T hb[3][4], gt[3][4];
+    fetch(z0 - 1);
+    __syncthreads();                     // the previous range's reads of su / so are done
+    stage();
+    fetch(z0);
+    T eNext = eOn ? E[eOff + PL * (z0 - 1)] : T(0);
+    __syncthreads();
+    corners(hb);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gt[c][k] = T(0);
+
+    for (int ez = z0 - 1; ez < z1; ++ez) {
+        __syncthreads();                 // every read of su / so of the previous step is done
+        stage();                         // node layer ez + 1
+        if (ez + 2 <= z1) fetch(ez + 2);
+        const T Ee = eNext;
+        if (ez + 1 < z1) eNext = eOn ? E[eOff + PL * (ez + 1)] : T(0);
+        __syncthreads();
+        T ht[3][4];
+        corners(ht);
+        // z butterfly and modulus: U[c][s], s = sxy + 4 sz
+        T U[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                U[c][k] = Ee * (hb[c][k] + ht[c][k]);
+                U[c][k + 4] = Ee * (hb[c][k] - ht[c][k]);
+                hb[c][k] = ht[c][k];
+            }
+        // block products V[c][t ^ e(c)] = sum_c' B_t[c][c'] U[c'][t ^ e(c')]
+        T V[3][8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                T acc = T(0);
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if ((walsh_pattern(t) >> (3 * c + d)) & 1u) acc = fma(B.b[t][3 * c + d], U[d][t ^ walsh_axis_bit(d)], acc);
+                V[c][t ^ walsh_axis_bit(c)] = acc;
+            }
+        // back along z: the bottom layer (ez) is complete with the carry of
+        // element ez-1's top layer; this element's top layer is the new carry
+        T G[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                G[c][k] = gt[c][k] + (V[c][k] + V[c][k + 4]);
+                gt[c][k] = V[c][k] - V[c][k + 4];
+            }
+        if (ez < z0) continue;           // first element: its bottom layer is not in this range
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            walsh2(G[c]);
+#pragma unroll
+            for (int k = 1; k < 4; ++k) so[((k - 1) * 3 + c) * Tl::NT + tid] = G[c][k];
+        }
+        __syncthreads();
+        if (nOut) {
+            T y[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                y[c] = G[c][0] + so[(0 * 3 + c) * Tl::NT + tid - 1]          // corner (1,0) of column (ty-1, tx)
+                               + so[(1 * 3 + c) * Tl::NT + tid - TY]         // corner (0,1) of column (ty, tx-1)
+                               + so[(2 * 3 + c) * Tl::NT + tid - TY - 1];    // corner (1,1) of column (ty-1, tx-1)
+            const int idx = eOff + PL * ez;
+            if (MASK) {
+                const uint8_t f = flags[idx];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) y[c] = E0 * in(idx, c);
+            }
+            out(idx, y, dot);
+        }
+    }
+}
+
+// Work = (tile, node layer) pairs, tile-major; CTA b takes the contiguous
+// share [b W / n, (b+1) W / n) and marches each tile's part of it along z,
+// so every CTA gets the same number of layers whatever the grid size.
+// resident CTAs per SM the register budget is fitted to
+template <typename T, int NT> struct WalshOcc {
+    static constexpr int value = sizeof(T) == 4 ? (NT >= 256 ? 3 : 6) : (NT >= 256 ? 1 : 3);
+};
+
+template <typename T, int TY, int TX, class In, class Out>
+__global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
+l0w_kernel(const WalshParam<T> B, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    using Tl = WalshTile<T, TY, TX>;
+    __shared__ T su[3 * Tl::SC];
+    __shared__ T so[9 * Tl::NT];
+    const int tilesY = (g.NY + TY - 2) / (TY - 1);
+    const int64_t total = (int64_t)walsh_tiles(g, TY, TX) * g.NZ;
+    int64_t a = total * blockIdx.x / gridDim.x;
+    const int64_t b = total * (blockIdx.x + 1) / gridDim.x;
+    double dot = 0.0;
+    while (a < b) {
+        const int tile = (int)(a / g.NZ), z0 = (int)(a % g.NZ);
+        const int z1 = (int)(z0 + (b - a) < g.NZ ? z0 + (b - a) : g.NZ);
+        const int y0 = (tile % tilesY) * (TY - 1), x0 = (tile / tilesY) * (TX - 1);
+        if (tileMask[tile])
+            l0w_march<T, TY, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, su, so, dot);
+        else
+            l0w_march<T, TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, su, so, dot);
+        a += z1 - z0;
+    }
+    if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result);
+}
+
+// tileMask[tile] = 1 when a node staged by that tile (any layer) has a fixed component
+template <int TY, int TX>
+__global__ void __launch_bounds__(256)
+walsh_mask_kernel(const uint8_t *__restrict__ flags, Geom g, uint8_t *__restrict__ tileMask)
+{
+    const int tilesY = (g.NY + TY - 2) / (TY - 1);
+    const int y0 = (blockIdx.x % tilesY) * (TY - 1), x0 = (blockIdx.x / tilesY) * (TX - 1);
+    int any = 0;
+    const int ny = TY + 1, nx = TX + 1;
+    for (int k = threadIdx.x; k < ny * nx * g.NZ; k += blockDim.x) {
+        const int Y = y0 - 1 + k % ny, X = x0 - 1 + (k / ny) % nx, Z = k / (ny * nx);
+        if (Y < 0 || Y >= g.NY || X < 0 || X >= g.NX) continue;
+        any |= flags[g.origin + Y + (int64_t)g.PY * X + g.plane * Z] & kFixedMask;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) tileMask[blockIdx.x] = any ? 1 : 0;
+}
+
+}  // namespace topgpu

@@ -262,6 +262,17 @@ class Solver:
         check(lib().top_solver_get_design(self._h, None if xPhys is None else xPhys.data_ptr(),
                                           None if x is None else x.data_ptr()), "top_solver_get_design")
 
+    def set_l0_kernel(self, fp32, kind, ty=16, tx=16, ctas=0):
+        """Level-0 product kernel for one precision: kind 0 dense node-centric, 1 Walsh-basis
+        tiles of ty x tx element columns on ctas CTAs (0: as many as fit at once)."""
+        check(lib().top_solver_set_l0_kernel(self._h, int(bool(fp32)), kind, ty, tx, ctas),
+              "top_solver_set_l0_kernel")
+
+    def l0_kernel(self, fp32):
+        out = (C.c_int * 4)()
+        check(lib().top_solver_get_l0_kernel(self._h, int(bool(fp32)), out), "top_solver_get_l0_kernel")
+        return tuple(out)
+
     @property
     def launches(self):
         """Kernels launched by this solver since creation."""
