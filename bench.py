@@ -175,9 +175,16 @@ def run_ours(args):
     ne, nn = info[0]["numElements"], info[0]["numNodes"]
     stream = torch.cuda.current_stream()
 
+    tuned = {}
+
     def make(mixed):
         s = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=mixed)
         c_solid = s.opt_begin(V0=V0, rMin=RMIN, nLoop=1 << 20, ft=FT)
+        # level-0 kernel autotuner (kind, tile shape, CTA count), once per model
+        if not tuned:
+            tuned.update(s.autotune(nrep=5))
+        for fp32, key in ((False, "fp64"), (True, "fp32")):
+            s.set_l0_kernel(fp32, *tuned[key][1])
         return s, c_solid
 
     def barrier():
@@ -273,6 +280,7 @@ def run_ours(args):
         "density_maxabs_err_mixed_vs_fp64": dens_err,
         "assembly_ms": mixed["asm_ms"], "fp64_assembly_ms": fp64["asm_ms"],
         "kernel_ms": tk,
+        "l0_autotune": {k: {"ms": v[0], "kind_ty_tx_ctas": list(v[1])} for k, v in tuned.items()},
         "matvec_gbs": {"fp64": bytes64 / (tk["l0_f64"] * 1e-3) / 1e9, "fp32": bytes32 / (tk["l0_f32"] * 1e-3) / 1e9},
         "matvec_tflops": {"fp64": flops / (tk["l0_f64"] * 1e-3) / 1e12, "fp32": flops / (tk["l0_f32"] * 1e-3) / 1e12},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -300,9 +308,11 @@ def run_ours(args):
 
 
 def run_kernels_only(args):
-    """Build the workload's mixed solver, assemble, time a few launches of the
-    level-0 stiffness products (FP64 outer, FP32 smoother) and one V-cycle.
-    Few launches: the command the ncu captures of those kernels run."""
+    """Build the workload's mixed solver, assemble, and time --steps launches
+    each of the level-0 stiffness products (FP64 outer, FP32 smoother) and of
+    one V-cycle, L2 not flushed.  Few launches: the command the ncu captures
+    of those kernels run.  --l0 fp64=K,TY,TX,CTAS / fp32=... selects the
+    level-0 kernel configurations (default: the solver's)."""
     import ctypes as C
     import torch
     from top_gpu_on_matlab_b200.fea import Mesh, Solver
@@ -310,6 +320,9 @@ def run_kernels_only(args):
     mesh = Mesh(np.ones(SHAPE, bool), control=CONTROL)
     mesh.apply_optcase(1)
     s = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=True)
+    for spec in args.l0 or []:
+        prec, vals = spec.split("=")
+        s.set_l0_kernel(prec == "fp32", *[int(v) for v in vals.split(",")])
     ne = mesh.info()[0]["numElements"]
     s.set_density(torch.full((ne,), V0, dtype=torch.float64, device="cuda"))
     s.assemble()
@@ -318,7 +331,8 @@ def run_kernels_only(args):
         ms = C.c_double(0)
         check(lib().top_solver_time_kernel(s._h, which, args.steps, 0, C.byref(ms)), "time_kernel")
         out[key] = ms.value
-    print(json.dumps({"kernels_only": out, "workload": WORKLOAD}), flush=True)
+    print(json.dumps({"kernels_only": out, "workload": WORKLOAD,
+                      "l0": {"fp64": s.l0_kernel(False), "fp32": s.l0_kernel(True)}}), flush=True)
 
 
 def main():
@@ -330,6 +344,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--ref-its", type=int, default=20, help="FP64 iteration count used to scale the CPU sample")
     ap.add_argument("--kernels-only", action="store_true", help="time a few launches of the level-0 kernels (profiling)")
+    ap.add_argument("--l0", action="append", help="with --kernels-only: fp64=KIND,TY,TX,CTAS or fp32=...")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

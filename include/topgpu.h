@@ -248,16 +248,24 @@ int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushByte
 
 /* Level-0 stiffness product kernel, per precision (fp32 = 0: the FP64
  * products, 1: the FP32 V-cycle products).  kind 0 = node-centric product
- * with the dense 24x24 Ke; kind 1 = Ke in the Walsh-Hadamard basis of the
- * cube element (eight 3x3 blocks), z-marching tiles of ty x tx element
- * columns, each of ctas CTAs marching an equal share of the (tile, z-layer)
- * work (ctas = 0: as many CTAs as fit on the GPU at once); tile shapes
- * 16x16 and 16x8.  kind 1 needs Ke with the cube's reflection
- * symmetry (always the case for the reference's isotropic voxel) and is the
- * default then.  get returns {kind, ty, tx, ctas}.  No counterpart in the
- * reference. */
+ * with the dense 24x24 Ke.  Kinds 1-3 use Ke in the Walsh-Hadamard basis of
+ * the cube element (eight 3x3 blocks) and march z through tiles of ty x tx
+ * threads, each of ctas CTAs taking an equal share of the (tile, z-layer)
+ * work (ctas = 0: as many CTAs as fit on the GPU at once): kind 1 stages the
+ * node layers in shared memory, kind 2 (FP32 only) gives each thread two
+ * element columns and uses paired FP32 arithmetic, kind 3 loads each
+ * column's corner nodes directly.  Tile shapes 16x16 and 16x8.  Kinds 1-3
+ * need Ke with the cube's reflection symmetry (always the case for the
+ * reference's isotropic voxel); kind 3 is the default then.  get returns
+ * {kind, ty, tx, ctas}.  No counterpart in the reference. */
 int top_solver_set_l0_kernel(top_solver *s, int fp32, int kind, int ty, int tx, int ctas);
 int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);
+/* Autotuner: times each level-0 kernel configuration (kind, tile shape, CTA
+ * count; nrep launches each, L2 flushed by writing flushBytes before every
+ * launch) on this model and keeps the fastest per precision.  msBest2 gets
+ * {FP64, FP32} ms per launch of the winners, configs8 their {kind, ty, tx,
+ * ctas} (either may be NULL).  No counterpart in the reference. */
+int top_solver_autotune(top_solver *s, int nrep, int64_t flushBytes, double *msBest2, int *configs8);
 
 /* Kernels this solver has launched since it was created (every entry point
  * counts the launches it makes on the solver's stream). */

@@ -55,7 +55,22 @@ def model(request):
 
 def test_walsh_is_default(model):
     _, s = model
-    assert s.l0_kernel(False)[0] == 1 and s.l0_kernel(True)[0] == 1
+    assert s.l0_kernel(False)[0] == 3 and s.l0_kernel(True)[0] == 3
+
+
+def test_autotune_picks_a_working_kernel(model):
+    o, s = model
+    keep = s.l0_kernel(False), s.l0_kernel(True)
+    res = s.autotune(nrep=2, flush_bytes=0)
+    assert res["fp64"][0] > 0 and res["fp32"][0] > 0
+    assert s.l0_kernel(False) == res["fp64"][1] and s.l0_kernel(True) == res["fp32"][1]
+    u = np.random.default_rng(5).standard_normal(o.level(0).numDOFs)
+    ref = o.matvec(0, u)
+    ud = torch.from_numpy(u).cuda()
+    assert _rel(s.matvec(0, ud), ref) < 1e-13
+    assert _rel(s.matvec(0, ud, fp32=True), ref) < 2e-6
+    for fp32, k in ((False, keep[0]), (True, keep[1])):
+        s.set_l0_kernel(fp32, *k)
 
 
 @pytest.mark.parametrize("shape", SHAPES)
@@ -68,10 +83,10 @@ def test_walsh_matvec_matches_oracle(model, shape, ctas):
     u = np.random.default_rng(ctas).standard_normal(o.level(0).numDOFs)
     ref = o.matvec(0, u)
     ud = torch.from_numpy(u).cuda()
-    for fp32 in (False, True):
-        s.set_l0_kernel(fp32, 1, shape[0], shape[1], ctas)
+    for fp32, kind in ((False, 1), (True, 1), (True, 2), (False, 3), (True, 3)):
+        s.set_l0_kernel(fp32, kind, shape[0], shape[1], ctas)
         y = s.matvec(0, ud, fp32=fp32)
-        assert _rel(y, ref) < (2e-6 if fp32 else 1e-13), (shape, ctas, fp32)
+        assert _rel(y, ref) < (2e-6 if fp32 else 1e-13), (shape, ctas, fp32, kind)
     for fp32, k in ((False, keep[0]), (True, keep[1])):
         s.set_l0_kernel(fp32, *k)
 
@@ -90,11 +105,14 @@ def test_walsh_and_dense_kernels_agree(model):
 def test_walsh_rejects_bad_shape(model):
     from top_gpu_on_matlab_b200._lib import TopGpuError
     _, s = model
+    keep = s.l0_kernel(False)
     with pytest.raises(TopGpuError):
         s.set_l0_kernel(False, 1, 12, 12, 4)
     with pytest.raises(TopGpuError):
         s.set_l0_kernel(False, 1, 16, 16, -1)
-    assert s.l0_kernel(False)[0] == 1
+    with pytest.raises(TopGpuError):          # paired-element kernel: FP32 only
+        s.set_l0_kernel(False, 2, 16, 8, 0)
+    assert s.l0_kernel(False) == keep        # a rejected configuration changes nothing
 
 
 def test_vcycle_and_pcg_with_walsh_match_oracle():
@@ -103,3 +121,23 @@ def test_vcycle_and_pcg_with_walsh_match_oracle():
     s.assemble()
     r = np.random.default_rng(6).standard_normal(o.level(0).numDOFs)
     assert _rel(s.vcycle(torch.from_numpy(r).cuda()), o.vcycle(r)) < 1e-11
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3])
+def test_mixed_vcycle_kinds_agree(kind):
+    """The FP32 V-cycle with either Walsh kernel stays within FP32 rounding
+    of the FP64 V-cycle."""
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    mask = np.ones((12, 24, 12), bool)
+    m = Mesh(mask, control=20000)
+    m.apply_optcase(1)
+    s64 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6)
+    s32 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6, mixed=True)
+    x = torch.from_numpy(0.3 + 0.6 * np.random.default_rng(1).random(m.info()[0]["numElements"])).cuda()
+    for s in (s64, s32):
+        s.set_density(x)
+        s.assemble()
+    s32.set_l0_kernel(True, kind, 16, 8, 0)
+    r = torch.from_numpy(np.random.default_rng(2).standard_normal(s64.numDOFs)).cuda()
+    z64, z32 = s64.vcycle(r), s32.vcycle(r)
+    assert float((z32 - z64).abs().max() / z64.abs().max()) < 1e-5

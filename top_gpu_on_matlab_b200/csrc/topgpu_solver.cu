@@ -572,7 +572,12 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     for (int t = 0; t < 576; ++t) { s->Ke64.k[t] = M0.Ke[t]; s->Ke32.k[t] = float(M0.Ke[t]); }
     s->walshOK = walsh_blocks(M0.Ke, s->W64) < 1e-12;
     for (int t = 0; t < 8; ++t)
-        for (int k = 0; k < 9; ++k) s->W32.b[t][k] = float(s->W64.b[t][k]);
+        for (int k = 0; k < 9; ++k) {
+            const double b = s->W64.b[t][k];
+            s->W32.b[t][k] = float(b);
+            s->WP64.b[t][k] = make_double2(b, b);
+            s->WP32.b[t][k] = make_float2(float(b), float(b));
+        }
     s->KeDev = s->dalloc<double>(576);
     s->Ec = s->dalloc<double>(M0.Ne);
     s->Eg64 = s->galloc<double>(l0.g.cs, 1);
@@ -689,7 +694,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     // level-0 products in the Walsh basis where Ke allows it
     if (s->walshOK)
         for (int pslot = 0; pslot < 2; ++pslot)
-            if (set_l0_kernel(s, pslot, 1, 16, 8, (pslot ? 12 : 8) * s->numSMs) != TOP_OK) return fail("level-0 kernel setup");
+            if (set_l0_kernel(s, pslot, 3, 16, 8, (pslot ? 16 : 12) * s->numSMs) != TOP_OK) return fail("level-0 kernel setup");
     cudaError_t err = cudaDeviceSynchronize();
     if (err != cudaSuccess) { set_error("top_solver_create: %s", cudaGetErrorString(err)); top_solver_destroy(s); return TOP_ERR_CUDA; }
     *out = s;
@@ -711,6 +716,14 @@ extern "C" int top_solver_set_l0_kernel(top_solver *s, int fp32, int kind, int t
 {
     if (!s) return TOP_ERR_ARGS;
     return set_l0_kernel(s, fp32 ? 1 : 0, kind, ty, tx, ctas);
+}
+
+extern "C" int top_solver_autotune(top_solver *s, int nrep, int64_t flushBytes, double *msBest2, int *configs8)
+{
+    if (!s) return TOP_ERR_ARGS;
+    const int rc = autotune_l0(s, nrep, flushBytes, msBest2, configs8);
+    if (rc != TOP_OK) set_error("top_solver_autotune: failed (%d)", rc);
+    return rc;
 }
 
 extern "C" int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4)

@@ -41,13 +41,16 @@ struct top_solver {
     std::vector<void *> allocs;      // raw allocations (freed on destroy)
     topgpu::KeParam<double> Ke64{}; topgpu::KeParam<float> Ke32{};
     // level-0 product: kind 0 = node-centric dense Ke, 1 = Walsh-basis tiles
-    // of ty x tx element columns on ctas CTAs (0: as many as fit at once);
-    // per precision, set by top_solver_set_l0_kernel or the autotuner
+    // of ty x tx element columns (one per thread), 2 = the same with two
+    // element columns per thread (ty x tx threads), on ctas CTAs (0: as many
+    // as fit at once); per precision, set by top_solver_set_l0_kernel or the
+    // autotuner
     struct L0Kernel { int kind = 0, ty = 16, tx = 16, ctas = 0; uint8_t *mask = nullptr; };
     int numSMs = 148;
     L0Kernel l0k[2];                 // [0] FP64, [1] FP32
     bool walshOK = false;            // Ke has the cube's reflection symmetry
     topgpu::WalshParam<double> W64{}; topgpu::WalshParam<float> W32{};
+    topgpu::WalshPairParam<double> WP64{}; topgpu::WalshPairParam<float> WP32{};
     double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
     double *Ec = nullptr, *Eg64 = nullptr; float *Eg32 = nullptr;
     int32_t *mapUnique = nullptr; double *uFree = nullptr, *uFixed = nullptr; int64_t nU = 0;
@@ -94,6 +97,8 @@ template <typename T, class In, class Out>
 void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done);
 // configure the level-0 kernel of precision slot p (0 FP64, 1 FP32)
 int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas);
+// time every level-0 kernel configuration, keep the fastest per precision
+int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int *configs);
 // PCG (TOP_GPU.m:602-667) on level-0 grid vectors: b and x in the solver's
 // SoA grid layout, x holds the warm start when warm != 0 and the solution.
 int pcg_grid(top_solver *s, const double *bGrid, double *xGrid, int warm, int *itsOut, double *resOut);

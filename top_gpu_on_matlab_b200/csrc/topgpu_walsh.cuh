@@ -291,4 +291,413 @@ walsh_mask_kernel(const uint8_t *__restrict__ flags, Geom g, uint8_t *__restrict
     if (threadIdx.x == 0) tileMask[blockIdx.x] = any ? 1 : 0;
 }
 
+// ---------------------------------------------------------------------------
+// Pair variant: every thread owns two element columns adjacent in y and runs
+// the whole Walsh pipeline on (element A, element B) pairs -- in FP32 with
+// the sm_100 paired instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn), so
+// each add, multiply and multiply-add serves both elements.  A tile of
+// TYP x TX threads covers 2 TYP x TX element columns and produces
+// (2 TYP - 1) x (TX - 1) node columns.
+template <typename T> struct PairOf;
+template <> struct PairOf<float> { using type = float2; };
+template <> struct PairOf<double> { using type = double2; };
+
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ double2 padd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 psub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 pmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 pfma(double2 a, double2 b, double2 c) { return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y)); }
+
+template <typename T> struct WalshPairParam { typename PairOf<T>::type b[8][9]; };   // (B, B) pairs
+
+template <typename T, int TYP, int TX> struct WalshPairTile {
+    static constexpr int NT = TYP * TX;
+    static constexpr int EY = 2 * TYP;                      // element rows of a tile
+    static constexpr int NS = (EY + 1) * (TX + 1);          // staged node columns
+    static constexpr int R = (NS + NT - 1) / NT;            // staged node columns per thread
+    static constexpr int SY = EY + 2;                       // even: rows (2ty, 2ty+1) load as one pair
+    static constexpr int SC = SY * (TX + 1);
+};
+
+__host__ __device__ inline int walsh_pair_tiles(const Geom &g, int TYP, int TX)
+{
+    return ((g.NY + 2 * TYP - 2) / (2 * TYP - 1)) * ((g.NX + TX - 2) / (TX - 1));
+}
+
+template <typename T, int TYP, int TX, bool MASK, class In, class Out>
+__device__ __forceinline__ void l0p_march(const WalshPairParam<T> &B, const In &in, const Out &out,
+                                          const T *__restrict__ E, const uint8_t *__restrict__ flags,
+                                          const Geom &g, int y0, int x0, int z0, int z1, T E0,
+                                          T *su, T *so, double &dot)
+{
+    using P2 = typename PairOf<T>::type;
+    using Tl = WalshPairTile<T, TYP, TX>;
+    const int tid = threadIdx.x, ty = tid % TYP, tx = tid / TYP;
+    const int PY = g.PY, PL = (int)g.plane;
+    // staged node columns (Y, X) = (y0-1+j, x0-1+i), all three components
+    int sOff[Tl::R], sDst[Tl::R];
+#pragma unroll
+    for (int r = 0; r < Tl::R; ++r) {
+        const int q = tid + r * Tl::NT, j = q % (Tl::EY + 1), i = q / (Tl::EY + 1);
+        const int Y = y0 - 1 + j, X = x0 - 1 + i;
+        const bool on = q < Tl::NS && Y <= g.NY && X <= g.NX;
+        sDst[r] = q < Tl::NS ? j + Tl::SY * i : -1;
+        sOff[r] = on ? (int)(g.origin + Y + (int64_t)PY * X) : -1;
+    }
+    T pre[Tl::R][3];
+    auto fetch = [&](int z) {
+#pragma unroll
+        for (int r = 0; r < Tl::R; ++r) {
+            const int m = sOff[r] + PL * z;
+            uint8_t f = 0;
+            if (MASK && sOff[r] >= 0) f = flags[m];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                T v = T(0);
+                if (sOff[r] >= 0) v = in(m, c);
+                if (MASK && (f & (1 << c))) v = T(0);
+                pre[r][c] = v;
+            }
+        }
+    };
+    auto stage = [&]() {
+#pragma unroll
+        for (int r = 0; r < Tl::R; ++r)
+            if (sDst[r] >= 0) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) su[c * Tl::SC + sDst[r]] = pre[r][c];
+            }
+    };
+    // element columns (ey, ey + 1) x ex of this thread
+    const int ey = y0 - 1 + 2 * ty, ex = x0 - 1 + tx;
+    const bool eOnA = ey <= g.NY - 1 && ex <= g.NX - 1, eOnB = ey + 1 <= g.NY - 1 && ex <= g.NX - 1;
+    const int eOff = (int)(g.origin + ey + (int64_t)PY * ex);
+    // nodes (ey, ex) and (ey + 1, ex): corner (0,0) of elements A and B
+    const bool outA = ty >= 1 && tx >= 1 && ey < g.NY && ex < g.NX;
+    const bool outB = tx >= 1 && ey + 1 < g.NY && ex < g.NX;
+    // (y, x) Walsh transform of the current node layer, as (A, B) pairs
+    auto corners = [&](P2 h[3][4]) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+            for (int bx = 0; bx < 2; ++bx) {
+                const T *col = su + c * Tl::SC + Tl::SY * (tx + bx) + 2 * ty;
+                const P2 lo = *reinterpret_cast<const P2 *>(col);     // rows 2ty, 2ty+1
+                const T hi = col[2];                                   // row 2ty+2
+                h[c][2 * bx] = lo;
+                h[c][2 * bx + 1].x = lo.y; h[c][2 * bx + 1].y = hi;
+            }
+            const P2 p0 = padd(h[c][0], h[c][1]), m0 = psub(h[c][0], h[c][1]);
+            const P2 p1 = padd(h[c][2], h[c][3]), m1 = psub(h[c][2], h[c][3]);
+            h[c][0] = padd(p0, p1); h[c][1] = padd(m0, m1); h[c][2] = psub(p0, p1); h[c][3] = psub(m0, m1);
+        }
+    };
+    auto eload = [&](int ez) {
+        P2 e;
+        e.x = eOnA ? E[eOff + PL * ez] : T(0);
+        e.y = eOnB ? E[eOff + 1 + PL * ez] : T(0);
+        return e;
+    };
+
+    P2 hb[3][4], gt[3][4];
+    fetch(z0 - 1);
+    __syncthreads();                     // the previous range's reads of su / so are done
+    stage();
+    fetch(z0);
+    P2 eNext = eload(z0 - 1);
+    __syncthreads();
+    corners(hb);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { gt[c][k].x = T(0); gt[c][k].y = T(0); }
+
+    for (int ez = z0 - 1; ez < z1; ++ez) {
+        __syncthreads();
+        stage();                         // node layer ez + 1
+        if (ez + 2 <= z1) fetch(ez + 2);
+        const P2 Ee = eNext;
+        if (ez + 1 < z1) eNext = eload(ez + 1);
+        __syncthreads();
+        P2 U[3][8];
+        {
+            P2 ht[3][4];
+            corners(ht);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    U[c][k] = pmul(Ee, padd(hb[c][k], ht[c][k]));
+                    U[c][k + 4] = pmul(Ee, psub(hb[c][k], ht[c][k]));
+                    hb[c][k] = ht[c][k];
+                }
+        }
+        // block products, in place: block t reads and writes U[c][t ^ e(c)]
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            P2 v[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                P2 acc; acc.x = T(0); acc.y = T(0);
+                bool first = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if ((walsh_pattern(t) >> (3 * c + d)) & 1u) {
+                        const P2 u = U[d][t ^ walsh_axis_bit(d)];
+                        acc = first ? pmul(B.b[t][3 * c + d], u) : pfma(B.b[t][3 * c + d], u, acc);
+                        first = false;
+                    }
+                v[c] = acc;
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) U[c][t ^ walsh_axis_bit(c)] = v[c];
+        }
+        // back along z with the carry; this element's top layer is the new carry
+        P2 G[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                G[c][k] = padd(gt[c][k], padd(U[c][k], U[c][k + 4]));
+                gt[c][k] = psub(U[c][k], U[c][k + 4]);
+            }
+        if (ez < z0) continue;
+        // back in (y, x): corner k = by + 2 bx of (A, B)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const P2 p0 = padd(G[c][0], G[c][1]), m0 = psub(G[c][0], G[c][1]);
+            const P2 p1 = padd(G[c][2], G[c][3]), m1 = psub(G[c][2], G[c][3]);
+            G[c][0] = padd(p0, p1); G[c][1] = padd(m0, m1); G[c][2] = psub(p0, p1); G[c][3] = psub(m0, m1);
+            // to neighbours: X0 = B(1,0) -> (ty+1, tx); (X1, X2) = (A(0,1), B(0,1) + A(1,1)) -> (ty, tx+1);
+            // X3 = B(1,1) -> (ty+1, tx+1)
+            so[(0 * 3 + c) * Tl::NT + tid] = G[c][1].y;
+            P2 x12; x12.x = G[c][2].x; x12.y = G[c][2].y + G[c][3].x;
+            reinterpret_cast<P2 *>(so + 3 * Tl::NT)[c * Tl::NT + tid] = x12;
+            so[(9 + c) * Tl::NT + tid] = G[c][3].y;
+        }
+        __syncthreads();
+        T yA[3], yB[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            P2 x12; x12.x = T(0); x12.y = T(0);
+            if (tx >= 1) x12 = reinterpret_cast<const P2 *>(so + 3 * Tl::NT)[c * Tl::NT + tid - TYP];
+            const T x0 = ty >= 1 ? so[(0 * 3 + c) * Tl::NT + tid - 1] : T(0);
+            const T x3 = (ty >= 1 && tx >= 1) ? so[(9 + c) * Tl::NT + tid - TYP - 1] : T(0);
+            yA[c] = G[c][0].x + x0 + x12.x + x3;
+            yB[c] = G[c][0].y + G[c][1].x + x12.y;
+        }
+        const int idx = eOff + PL * ez;
+        if (outA) {
+            if (MASK) {
+                const uint8_t f = flags[idx];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) yA[c] = E0 * in(idx, c);
+            }
+            out(idx, yA, dot);
+        }
+        if (outB) {
+            if (MASK) {
+                const uint8_t f = flags[idx + 1];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) yB[c] = E0 * in(idx + 1, c);
+            }
+            out(idx + 1, yB, dot);
+        }
+    }
+}
+
+template <typename T, int NT> struct WalshPairOcc {
+    static constexpr int value = NT >= 256 ? 1 : 3;
+};
+
+template <typename T, int TYP, int TX, class In, class Out>
+__global__ void __launch_bounds__(TYP * TX, WalshPairOcc<T, TYP * TX>::value)
+l0p_kernel(const WalshPairParam<T> B, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    using Tl = WalshPairTile<T, TYP, TX>;
+    __shared__ __align__(16) T su[3 * Tl::SC];
+    __shared__ __align__(16) T so[12 * Tl::NT];
+    const int tilesY = (g.NY + 2 * TYP - 2) / (2 * TYP - 1);
+    const int64_t total = (int64_t)walsh_pair_tiles(g, TYP, TX) * g.NZ;
+    int64_t a = total * blockIdx.x / gridDim.x;
+    const int64_t b = total * (blockIdx.x + 1) / gridDim.x;
+    double dot = 0.0;
+    while (a < b) {
+        const int tile = (int)(a / g.NZ), z0 = (int)(a % g.NZ);
+        const int z1 = (int)(z0 + (b - a) < g.NZ ? z0 + (b - a) : g.NZ);
+        const int y0 = (tile % tilesY) * (2 * TYP - 1), x0 = (tile / tilesY) * (TX - 1);
+        if (tileMask[tile])
+            l0p_march<T, TYP, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, su, so, dot);
+        else
+            l0p_march<T, TYP, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, su, so, dot);
+        a += z1 - z0;
+    }
+    if (red.result) block_sum_to<TYP * TX>(dot, red.partials, red.counter, red.result);
+}
+
+// tileMask[tile] for the pair tiling: any staged node with a fixed component
+template <int TYP, int TX>
+__global__ void __launch_bounds__(256)
+walsh_pair_mask_kernel(const uint8_t *__restrict__ flags, Geom g, uint8_t *__restrict__ tileMask)
+{
+    const int tilesY = (g.NY + 2 * TYP - 2) / (2 * TYP - 1);
+    const int y0 = (blockIdx.x % tilesY) * (2 * TYP - 1), x0 = (blockIdx.x / tilesY) * (TX - 1);
+    int any = 0;
+    const int ny = 2 * TYP + 1, nx = TX + 1;
+    for (int k = threadIdx.x; k < ny * nx * g.NZ; k += blockDim.x) {
+        const int Y = y0 - 1 + k % ny, X = x0 - 1 + (k / ny) % nx, Z = k / (ny * nx);
+        if (Y < 0 || Y >= g.NY || X < 0 || X >= g.NX) continue;
+        any |= flags[g.origin + Y + (int64_t)g.PY * X + g.plane * Z] & kFixedMask;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) tileMask[blockIdx.x] = any ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// Direct-load variant of the single-column kernel: each thread reads the
+// four top corner nodes of its element column straight from global memory
+// (L1-cached: every node is read by the four columns around it, two of them
+// in the same warp), one layer ahead in registers.  Only the node sums go
+// through shared memory, double-buffered, so a layer costs one barrier.
+template <typename T, int TY, int TX, bool MASK, class In, class Out>
+__device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, const Out &out,
+                                          const T *__restrict__ E, const uint8_t *__restrict__ flags,
+                                          const Geom &g, int y0, int x0, int z0, int z1, T E0,
+                                          T *so, double &dot)
+{
+    constexpr int NT = TY * TX;
+    const int tid = threadIdx.x, ty = tid % TY, tx = tid / TY;
+    const int PY = g.PY, PL = (int)g.plane;
+    const int ey = y0 - 1 + ty, ex = x0 - 1 + tx;
+    // the column's corners (ey + by, ex + bx) lie in [-1, NY] x [-1, NX] (guard
+    // slots included) exactly when the column is at most one past the last element
+    const bool cOn = ey <= g.NY - 1 && ex <= g.NX - 1;
+    const int base = cOn ? (int)(g.origin + ey + (int64_t)PY * ex) : 0;
+    const bool nOut = ty >= 1 && tx >= 1 && ey < g.NY && ex < g.NX;
+    auto load = [&](int z, T v[3][4]) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int m = base + (k & 1) + PY * (k >> 1) + PL * z;
+            uint8_t f = 0;
+            if (MASK && cOn) f = flags[m];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                T u = cOn ? in(m, c) : T(0);
+                if (MASK && (f & (1 << c))) u = T(0);
+                v[c][k] = u;
+            }
+        }
+    };
+    auto eload = [&](int z) { return cOn ? E[base + PL * z] : T(0); };
+
+    T hb[3][4], gt[3][4], pre[3][4];
+    __syncthreads();                     // the previous range's reads of so are done
+    load(z0 - 1, hb);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) walsh2(hb[c]);
+    load(z0, pre);
+    T eNext = eload(z0 - 1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gt[c][k] = T(0);
+
+    for (int ez = z0 - 1; ez < z1; ++ez) {
+        T ht[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) ht[c][k] = pre[c][k];
+        if (ez + 2 <= z1) load(ez + 2, pre);
+        const T Ee = eNext;
+        if (ez + 1 < z1) eNext = eload(ez + 1);
+        T U[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            walsh2(ht[c]);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                U[c][k] = Ee * (hb[c][k] + ht[c][k]);
+                U[c][k + 4] = Ee * (hb[c][k] - ht[c][k]);
+                hb[c][k] = ht[c][k];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            T v[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                T acc = T(0);
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if ((walsh_pattern(t) >> (3 * c + d)) & 1u) acc = fma(B.b[t][3 * c + d], U[d][t ^ walsh_axis_bit(d)], acc);
+                v[c] = acc;
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) U[c][t ^ walsh_axis_bit(c)] = v[c];
+        }
+        T G[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                G[c][k] = gt[c][k] + (U[c][k] + U[c][k + 4]);
+                gt[c][k] = U[c][k] - U[c][k + 4];
+            }
+        if (ez < z0) continue;
+        T *buf = so + (ez & 1) * 9 * NT;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            walsh2(G[c]);
+#pragma unroll
+            for (int k = 1; k < 4; ++k) buf[((k - 1) * 3 + c) * NT + tid] = G[c][k];
+        }
+        __syncthreads();
+        if (nOut) {
+            T y[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                y[c] = G[c][0] + buf[(0 * 3 + c) * NT + tid - 1] + buf[(1 * 3 + c) * NT + tid - TY]
+                               + buf[(2 * 3 + c) * NT + tid - TY - 1];
+            const int idx = base + PL * ez;
+            if (MASK) {
+                const uint8_t f = flags[idx];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) y[c] = E0 * in(idx, c);
+            }
+            out(idx, y, dot);
+        }
+    }
+}
+
+template <typename T, int TY, int TX, class In, class Out>
+__global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
+l0d_kernel(const WalshParam<T> B, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    __shared__ T so[2 * 9 * TY * TX];
+    const int tilesY = (g.NY + TY - 2) / (TY - 1);
+    const int64_t total = (int64_t)walsh_tiles(g, TY, TX) * g.NZ;
+    int64_t a = total * blockIdx.x / gridDim.x;
+    const int64_t b = total * (blockIdx.x + 1) / gridDim.x;
+    double dot = 0.0;
+    while (a < b) {
+        const int tile = (int)(a / g.NZ), z0 = (int)(a % g.NZ);
+        const int z1 = (int)(z0 + (b - a) < g.NZ ? z0 + (b - a) : g.NZ);
+        const int y0 = (tile % tilesY) * (TY - 1), x0 = (tile / tilesY) * (TX - 1);
+        if (tileMask[tile])
+            l0d_march<T, TY, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        else
+            l0d_march<T, TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        a += z1 - z0;
+    }
+    if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result);
+}
+
 }  // namespace topgpu

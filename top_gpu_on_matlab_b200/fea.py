@@ -273,6 +273,14 @@ class Solver:
         check(lib().top_solver_get_l0_kernel(self._h, int(bool(fp32)), out), "top_solver_get_l0_kernel")
         return tuple(out)
 
+    def autotune(self, nrep=5, flush_bytes=512 << 20):
+        """Pick the fastest level-0 kernel per precision on this model; returns
+        {"fp64": (ms, (kind, ty, tx, ctas)), "fp32": (...)}."""
+        ms = (C.c_double * 2)()
+        cfg = (C.c_int * 8)()
+        check(lib().top_solver_autotune(self._h, nrep, flush_bytes, ms, cfg), "top_solver_autotune")
+        return {"fp64": (ms[0], tuple(cfg[0:4])), "fp32": (ms[1], tuple(cfg[4:8]))}
+
     @property
     def launches(self):
         """Kernels launched by this solver since creation."""
