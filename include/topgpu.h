@@ -260,6 +260,11 @@ int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushByte
  * {kind, ty, tx, ctas}.  No counterpart in the reference. */
 int top_solver_set_l0_kernel(top_solver *s, int fp32, int kind, int ty, int tx, int ctas);
 int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);
+/* PCG iterations run as CUDA graphs of four iterations each (captured once
+ * per right-hand side / solution pair and operator configuration, launched
+ * on a solver-owned stream ordered after the caller's); on = 0 launches the
+ * kernels one by one instead.  Default on.  No counterpart in the reference. */
+int top_solver_set_graphs(top_solver *s, int on);
 /* Autotuner: times each level-0 kernel configuration (kind, tile shape, CTA
  * count; nrep launches each, L2 flushed by writing flushBytes before every
  * launch) on this model and keeps the fastest per precision.  msBest2 gets

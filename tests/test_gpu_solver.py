@@ -119,6 +119,27 @@ def test_pcg_fp64_matches_oracle(pair):
     assert abs(c - c_o) <= 1e-9 * abs(c_o)
 
 
+def test_pcg_graphs_match_launches(pair):
+    """The CUDA-graph PCG (chunks of four iterations) runs the same kernels in
+    the same order as launch-by-launch PCG: identical iterates."""
+    _smooth_only(pair)
+    _, s, _, _ = pair
+    n0 = s.launches
+    Ug, its_g, res_g = s.pcg(0)
+    n1 = s.launches
+    s.set_graphs(False)
+    try:
+        Ul, its_l, res_l = s.pcg(0)
+    finally:
+        s.set_graphs(True)
+    n2 = s.launches
+    assert its_g == its_l and res_g == res_l
+    assert torch.equal(Ug, Ul)
+    # graph launches count their kernels; whole chunks may run a few extra
+    # (early-exiting) iterations
+    assert n1 - n0 >= n2 - n1 > 0
+
+
 def test_pcg_warm_start_and_unit_compliance(pair):
     _smooth_only(pair)
     o, s, _, _ = pair

@@ -99,7 +99,7 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
 int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 {
     top_solver::L0Kernel &k = s->l0k[p];
-    if (kind == 0) { k.kind = 0; return TOP_OK; }
+    if (kind == 0) { k.kind = 0; ++s->opGen; return TOP_OK; }
     if ((kind != 1 && kind != 3 && !(kind == 2 && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0) return TOP_ERR_ARGS;
     DevLevel &l0 = s->L[0];
     const int tiles = tiles_of(l0.g, kind, ty, tx);
@@ -120,6 +120,7 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
     TOPGPU_COUNT_LAUNCH();
     if (cudaGetLastError() != cudaSuccess) return TOP_ERR_CUDA;
     k.kind = kind; k.ty = ty; k.tx = tx; k.ctas = ctas;
+    ++s->opGen;
     return TOP_OK;
 }
 

@@ -705,6 +705,10 @@ extern "C" int top_solver_destroy(top_solver *s)
 {
     if (!s) return TOP_OK;
     free_opt_state(s);
+    for (auto &G : s->graphs) if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (s->capStream) cudaStreamDestroy(s->capStream);
+    if (s->capIn) cudaEventDestroy(s->capIn);
+    if (s->capOut) cudaEventDestroy(s->capOut);
     for (auto &k : s->l0k) if (k.mask) cudaFree(k.mask);
     for (void *p : s->allocs) cudaFree(p);
     if (s->hstate) cudaFreeHost(s->hstate);
@@ -724,6 +728,13 @@ extern "C" int top_solver_autotune(top_solver *s, int nrep, int64_t flushBytes, 
     const int rc = autotune_l0(s, nrep, flushBytes, msBest2, configs8);
     if (rc != TOP_OK) set_error("top_solver_autotune: failed (%d)", rc);
     return rc;
+}
+
+extern "C" int top_solver_set_graphs(top_solver *s, int on)
+{
+    if (!s) return TOP_ERR_ARGS;
+    s->useGraphs = on != 0;
+    return TOP_OK;
 }
 
 extern "C" int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4)
@@ -935,6 +946,54 @@ __global__ void pcg_init_kernel(PcgState *st)
     if (st->normB == 0.0) st->done = 1;   // zero load: x = 0, no iterations
 }
 
+// The PCG chunk graph for (b, x): captured from `body` (launches on the
+// stream it is given) on first use and again when the operator configuration
+// changed.  Capture runs on the solver's own non-blocking stream (the
+// caller's stream may be the legacy default stream, which cannot be captured).
+template <class Body>
+static cudaError_t pcg_graph_prepare(top_solver *s, const double *b, double *x, int chunk, Body body,
+                                     top_solver::PcgGraph **out)
+{
+    for (auto &G : s->graphs)
+        if (G.exec && G.b == b && G.x == x && G.gen == s->opGen && G.chunk == chunk) { *out = &G; return cudaSuccess; }
+    cudaError_t e;
+    if (!s->capStream) {
+        if ((e = cudaStreamCreateWithFlags(&s->capStream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&s->capIn, cudaEventDisableTiming)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&s->capOut, cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    // drop stale graphs and, beyond eight, the oldest
+    for (size_t i = 0; i < s->graphs.size();) {
+        top_solver::PcgGraph &G = s->graphs[i];
+        if (G.gen != s->opGen || (G.b == b && G.x == x) || s->graphs.size() >= 8) {
+            if (G.exec) cudaGraphExecDestroy(G.exec);
+            s->graphs.erase(s->graphs.begin() + (long)i);
+        } else {
+            ++i;
+        }
+    }
+    top_solver::PcgGraph G;
+    cudaStream_t user = s->st;
+    const int64_t before = s->launches;
+    s->st = s->capStream;                // every launch helper issues on s->st
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamBeginCapture(s->capStream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        body(s->capStream);
+        e = cudaStreamEndCapture(s->capStream, &graph);
+    }
+    s->st = user;
+    G.nodes = s->launches - before;      // captured, not run
+    s->launches = before;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&G.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return e;
+    G.b = b; G.x = x; G.gen = s->opGen; G.chunk = chunk;
+    s->graphs.push_back(G);
+    *out = &s->graphs.back();
+    return cudaSuccess;
+}
+
 int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, int *itsOut, double *resOut)
 {
     if (!s->assembled) { set_error("top_solver_pcg: assemble first"); return TOP_ERR_STATE; }
@@ -965,18 +1024,32 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
     CKL();
     static const bool trace = std::getenv("TOPGPU_PCG_TRACE") != nullptr;
     const int chunk = trace ? 1 : 4;
+    // one PCG iteration (TOP_GPU.m:620-655); every kernel returns at once when done is set
+    auto iteration = [&](cudaStream_t q) {
+        outer_op(s, s->pv, s->v, &s->state->pv, done);                                       // v = A p, p.v
+        pcg_update_kernel<<<VB, 256, 0, q>>>(xg, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
+        TOPGPU_COUNT_LAUNCH();
+        pcg_check_kernel<<<1, 1, 0, q>>>(s->state);
+        TOPGPU_COUNT_LAUNCH();
+        precond(s, s->r, s->z, &s->state->rho, done);                                         // z = M r, z.r
+        pcg_p_kernel<<<VB, 256, 0, q>>>(s->pv, s->z, ng, cs, s->state, 0);                  // p = z + beta p
+        TOPGPU_COUNT_LAUNCH();
+    };
+    top_solver::PcgGraph *G = nullptr;
+    if (s->useGraphs && !trace)
+        CK(pcg_graph_prepare(s, bGrid, xg, chunk, [&](cudaStream_t q) { for (int k = 0; k < chunk; ++k) iteration(q); }, &G));
     for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
-        for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
-            outer_op(s, s->pv, s->v, &s->state->pv, done);                                   // v = A p, p.v
-            pcg_update_kernel<<<VB, 256, 0, st>>>(xg, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
-            TOPGPU_COUNT_LAUNCH();
-            pcg_check_kernel<<<1, 1, 0, st>>>(s->state);
-            TOPGPU_COUNT_LAUNCH();
-            precond(s, s->r, s->z, &s->state->rho, done);                                     // z = M r, z.r
-            pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 0);              // p = z + beta p
+        if (G && it0 + chunk <= s->p.maxIT) {
+            CK(cudaEventRecord(s->capIn, st));
+            CK(cudaStreamWaitEvent(s->capStream, s->capIn, 0));
+            CK(cudaGraphLaunch(G->exec, s->capStream));
+            CK(cudaEventRecord(s->capOut, s->capStream));
+            CK(cudaStreamWaitEvent(st, s->capOut, 0));
+            s->launches += G->nodes;
+        } else {
+            for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) iteration(st);
         }
         CKL();
-        TOPGPU_COUNT_LAUNCH();
         CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (trace && it0 < 12)

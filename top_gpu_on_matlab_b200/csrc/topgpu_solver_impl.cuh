@@ -36,6 +36,16 @@ struct top_solver {
     using Reduce = topgpu::Reduce;
     top_solver_params p{};
     cudaStream_t st = nullptr;
+    // CUDA graph of a chunk of PCG iterations (captured on an internal stream,
+    // re-captured when an operand pointer or the operator configuration changes)
+    struct PcgGraph {
+        cudaGraphExec_t exec = nullptr;
+        const double *b = nullptr; double *x = nullptr; int gen = -1, chunk = 0; int64_t nodes = 0;
+    };
+    std::vector<PcgGraph> graphs;    // one per (right-hand side, solution) pair in use
+    cudaStream_t capStream = nullptr; cudaEvent_t capIn = nullptr, capOut = nullptr;
+    bool useGraphs = true;
+    int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
     std::vector<DevLevel> L;
     std::vector<void *> allocs;      // raw allocations (freed on destroy)

@@ -273,6 +273,10 @@ class Solver:
         check(lib().top_solver_get_l0_kernel(self._h, int(bool(fp32)), out), "top_solver_get_l0_kernel")
         return tuple(out)
 
+    def set_graphs(self, on):
+        """Run PCG iterations as captured CUDA graphs (default) or launch by launch."""
+        check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
+
     def autotune(self, nrep=5, flush_bytes=512 << 20):
         """Pick the fastest level-0 kernel per precision on this model; returns
         {"fp64": (ms, (kind, ty, tx, ctas)), "fp32": (...)}."""
