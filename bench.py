@@ -246,7 +246,8 @@ def run_ours(args):
     peak, peak_kind = _peaks()
     flush = 512 << 20
     tk = {}
-    for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32"), (3, "l1_f32")):
+    for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32"), (3, "l1_f32"), (4, "restrict01_f32"),
+                       (5, "prolong10_f32")):
         ms = C.c_double(0)
         check(lib().top_solver_time_kernel(s._h, which, 20, flush, C.byref(ms)), "time_kernel")
         tk[key] = ms.value

@@ -242,7 +242,8 @@ int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysO
 
 /* Kernel timing with CUDA events on the solver's stream (no host copies):
  * which = 0 level-0 K*u FP64, 1 level-0 K*u FP32, 2 one V-cycle,
- * 3 level-1 K*u FP32; L2 is flushed by writing flushBytes before each launch.
+ * 3 level-1 K*u FP32, 4 level 0 -> 1 restriction FP32, 5 level 1 -> 0
+ * prolongation FP32; L2 is flushed by writing flushBytes before each launch.
  * No counterpart in the reference (its MATLAB driver times with tic/toc). */
 int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushBytes, double *msPerLaunch);
 

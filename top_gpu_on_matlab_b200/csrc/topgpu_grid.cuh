@@ -272,6 +272,66 @@ coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, cons
     if (valid && i == 0) out((int)idx, y, dot);
     if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
 }
+// Tiled variant: a CTA of 32 x 8 threads covers 32 consecutive node slots of
+// one (x, z) row; thread (n, i) multiplies the three rows of incident element
+// i (the node is its corner i) with u_e, so for a fixed i and entry the 32
+// threads of a warp read consecutive element slots (one coalesced run), and
+// the eight partial sums of a node are added in a fixed order.
+constexpr int kCoarseTileX = 32;
+template <typename T, class In, class Out>
+__global__ void __launch_bounds__(kCoarseTileX * 8)
+coarse_tile_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    __shared__ T part[8][3][kCoarseTileX];
+    __shared__ int offs[24 * 24];        // packed-entry offset (entry * CS) of Ks(r, k)
+    const int n = threadIdx.x, i = threadIdx.y;
+    for (int k = n + kCoarseTileX * i; k < 24 * 24; k += kCoarseTileX * 8)
+        offs[k] = sym_pack(k / 24, k % 24) * (int)g.cs;
+    __syncthreads();
+    const int q = blockIdx.x * kCoarseTileX + n;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    const bool valid = Y < g.NY && X < g.NX;
+    const int PY = g.PY, PL = (int)g.plane;
+    const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
+    T y[3] = {T(0), T(0), T(0)};
+    if (valid) {
+        const int slot = idx - cdy(i) - PY * cdx(i) - PL * cdz(i);
+        const T *ke = Ks + slot;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int m = slot + cdy(j) + PY * cdx(j) + PL * cdz(j);
+            const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
+            // row 3i+c, column 3j+d of the packed symmetric Ks (i is warp-uniform:
+            // the offset loads are shared-memory broadcasts)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    y[c] = fma(__ldg(ke + offs[(3 * i + c) * 24 + 3 * j + d]), u[d], y[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) part[i][c][n] = y[c];
+    __syncthreads();
+    double dot = 0.0;
+    if (i == 0 && valid) {
+        T s[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            s[c] = part[0][c][n];
+#pragma unroll
+            for (int k = 1; k < 8; ++k) s[c] += part[k][c][n];
+        }
+        out(idx, s, dot);
+    }
+    if (red.result) block_sum_to<kCoarseTileX * 8>(dot, red.partials, red.counter, red.result);
+}
+inline dim3 coarse_tile_grid(const Geom &g)
+{
+    return dim3((unsigned)(((int64_t)g.PY * g.NX + kCoarseTileX - 1) / kCoarseTileX), (unsigned)g.NZ);
+}
+
 inline unsigned coarse_blocks(const Geom &g)
 {
     const int64_t threads = (int64_t)g.PY * g.NX * g.NZ * kCoarseLanes;
@@ -337,6 +397,85 @@ inline unsigned restrict_blocks(const Geom &gc)
 {
     const int64_t threads = (int64_t)gc.PY * gc.NX * gc.NZ * RestrictLanes<S>::value;
     return (unsigned)((threads + kNodeThreads - 1) / kNodeThreads);
+}
+
+// Separable restriction (trilinear weights factor per axis), one axis per
+// pass: pass A folds the fine y taps, t[c][QY][X][Z] = sum_oy w(oy)
+// r_f[c][S QY + oy][X][Z] (dense NYc x NXf x NZf per component), passes B and
+// C fold x and z.  Same weights and clipping as restrict_kernel; every pass
+// reads runs of consecutive QY.
+template <typename T, int S>
+__global__ void __launch_bounds__(256)
+restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int64_t nt = (int64_t)NYc * gf.NX * gf.NZ;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nt) return;
+    const int QY = (int)(k % NYc), X = (int)((k / NYc) % gf.NX), Z = (int)(k / ((int64_t)NYc * gf.NX));
+    const int64_t base = gf.origin + (int64_t)gf.PY * X + gf.plane * Z;
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int oy = -(S - 1); oy <= S - 1; ++oy) {
+        const int Y = S * QY + oy;
+        if (Y < 0 || Y >= gf.NY) continue;
+        const T w = T(S - (oy < 0 ? -oy : oy)) / T(S);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] = fma(w, rf[c * gf.cs + base + Y], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t[c * nt + k] = acc[c];
+}
+// pass B: fold the x taps, t2[c][QY][QX][Z] = sum_ox w(ox) t[c][QY][S QX + ox][Z]
+template <typename T, int S>
+__global__ void __launch_bounds__(256)
+restrict_x_kernel(const T *__restrict__ t, int NYc, int NXf, int NXc, int NZf, T *__restrict__ t2, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n2) return;
+    const int QY = (int)(k % NYc), QX = (int)((k / NYc) % NXc), Z = (int)(k / ((int64_t)NYc * NXc));
+    T acc[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int ox = -(S - 1); ox <= S - 1; ++ox) {
+        const int X = S * QX + ox;
+        if (X < 0 || X >= NXf) continue;
+        const T w = T(S - (ox < 0 ? -ox : ox)) / T(S);
+        const int64_t o = QY + (int64_t)NYc * (X + (int64_t)NXf * Z);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[c] = fma(w, t[c * nt + o], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) t2[c * n2 + k] = acc[c];
+}
+// pass C: fold the z taps into every active coarse node
+template <typename T, int S>
+__global__ void __launch_bounds__(256)
+restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc,
+                  const uint8_t *__restrict__ flagsC, const int *__restrict__ done)
+{
+    if (done && *done) return;
+    const int NYc = gc.NY, NXc = gc.NX;
+    const int64_t nq = (int64_t)NYc * NXc * gc.NZ, n2 = (int64_t)NYc * NXc * NZf;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nq) return;
+    const int QY = (int)(k % NYc), QX = (int)((k / NYc) % NXc), QZ = (int)(k / ((int64_t)NYc * NXc));
+    const int64_t ic = gc.origin + QY + (int64_t)gc.PY * QX + gc.plane * QZ;
+    T acc[3] = {T(0), T(0), T(0)};
+    if (flagsC[ic] & kActive) {
+#pragma unroll
+        for (int oz = -(S - 1); oz <= S - 1; ++oz) {
+            const int Z = S * QZ + oz;
+            if (Z < 0 || Z >= NZf) continue;
+            const T w = T(S - (oz < 0 ? -oz : oz)) / T(S);
+            const int64_t o = QY + (int64_t)NYc * (QX + (int64_t)NXc * Z);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[c] = fma(w, t2[c * n2 + o], acc[c]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
 }
 
 // x_f = base + P x_c, base = omega*invD.*r when r != nullptr (the pre-smoothed

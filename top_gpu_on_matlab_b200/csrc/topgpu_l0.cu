@@ -196,6 +196,7 @@ template void l0_op<double, VIdd, DotStoreOut<double, double, double>>(top_solve
 template void l0_op<double, VIdd, ResidOut<double, double, double>>(top_solver *, const VIdd &, const ResidOut<double, double, double> &, Reduce, const int *);
 template void l0_op<float, JIfd, ResidOut<float, double, float>>(top_solver *, const JIfd &, const ResidOut<float, double, float> &, Reduce, const int *);
 template void l0_op<float, VIff, PostSmoothOut<float, double, double>>(top_solver *, const VIff &, const PostSmoothOut<float, double, double> &, Reduce, const int *);
+template void l0_op<float, VIff, PostSmoothOut<float, double, float>>(top_solver *, const VIff &, const PostSmoothOut<float, double, float> &, Reduce, const int *);
 template void l0_op<float, VIfd, DotStoreOut<float, double, double>>(top_solver *, const VIfd &, const DotStoreOut<float, double, double> &, Reduce, const int *);
 template void l0_op<float, VIfd, StoreOut<float, double>>(top_solver *, const VIfd &, const StoreOut<float, double> &, Reduce, const int *);
 template void l0_op<float, VIfd, ResidOut<float, double, double>>(top_solver *, const VIfd &, const ResidOut<float, double, double> &, Reduce, const int *);

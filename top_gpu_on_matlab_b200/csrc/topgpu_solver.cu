@@ -255,14 +255,15 @@ __global__ void coarsest_gemv_kernel(const double *__restrict__ Ainv, const doub
 }
 
 // ---- PCG vector kernels (FP64, level-0 grid arrays) ----
+// PCG vector kernels run over whole grid vectors, margins and guard slots
+// included (all zero), as one contiguous range of n = 3 CS values
 __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                                  const double *__restrict__ v, int64_t ng, int64_t cs, PcgState *st, Reduce red)
+                                  const double *__restrict__ v, int64_t n, PcgState *st, Reduce red)
 {
     if (st->done) return;
     const double lambda = st->rho / st->pv;
     double rr = 0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * ng; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = (k / ng) * cs + k % ng;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         x[i] += lambda * p[i];
         const double rv = r[i] - lambda * v[i];
         r[i] = rv;
@@ -281,23 +282,19 @@ __global__ void pcg_check_kernel(PcgState *st)
     if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
     st->rhoOld = st->rho;
 }
-__global__ void pcg_p_kernel(double *__restrict__ p, const double *__restrict__ z, int64_t ng, int64_t cs,
-                             const PcgState *st, int first)
+template <typename TZ>
+__global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, int64_t n, const PcgState *st, int first)
 {
     if (!first && st->done) return;
     const double beta = first ? 0.0 : st->rho / st->rhoOld;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * ng; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = (k / ng) * cs + k % ng;
-        p[i] = z[i] + beta * p[i];
-    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = double(z[i]) + beta * p[i];
 }
-__global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t ng, int64_t cs, Reduce red)
+__global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t n, Reduce red)
 {
     double s = 0;
-    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < 3 * ng; k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = (k / ng) * cs + k % ng;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         s += a[i] * b[i];
-    }
     block_sum_to<256>(s, red.partials, red.counter, red.result);
 }
 // element energies sum_k w_k u_k' Ke u_k (TOP_GPU.m:580-600) on grid vectors
@@ -339,7 +336,7 @@ using namespace topgpu;
 namespace {
 
 inline dim3 node_grid(const Geom &g) { return dim3((unsigned)g.nbx, (unsigned)g.NZ); }
-inline int vec_blocks(int64_t ng) { return (int)std::min<int64_t>((3 * ng + 255) / 256, 4096); }
+inline int vec_blocks(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 4096); }
 
 #define CK(call)                                                                                 \
     do {                                                                                         \
@@ -391,7 +388,32 @@ template <typename T, class In, class Out>
 void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done)
 {
     DevLevel &lv = s->L[l];
-    coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    if (s->coarseLanes)
+        coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    else
+        coarse_tile_kernel<T, In, Out><<<coarse_tile_grid(lv.g), dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    TOPGPU_COUNT_LAUNCH();
+}
+template <typename T> T *rscratch(top_solver *s);
+template <> double *rscratch<double>(top_solver *s) { return s->rscr64; }
+template <> float *rscratch<float>(top_solver *s) { return s->rscr32; }
+// restriction of the level-l residual d onto level l+1 (TOP_GPU.m:817-847)
+template <typename T>
+void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done)
+{
+    DevLevel &lv = s->L[l], &lc = s->L[l + 1];
+    if (lc.span == 4) {
+        const int NYc = lc.g.NY, NXf = lv.g.NX, NXc = lc.g.NX, NZf = lv.g.NZ;
+        const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf, nq = (int64_t)NYc * NXc * lc.g.NZ;
+        T *t1 = rscratch<T>(s), *t2 = t1 + 3 * nt;
+        restrict_y_kernel<T, 4><<<(unsigned)((nt + 255) / 256), 256, 0, s->st>>>(d, lv.g, t1, NYc, done);
+        TOPGPU_COUNT_LAUNCH();
+        restrict_x_kernel<T, 4><<<(unsigned)((n2 + 255) / 256), 256, 0, s->st>>>(t1, NYc, NXf, NXc, NZf, t2, done);
+        TOPGPU_COUNT_LAUNCH();
+        restrict_z_kernel<T, 4><<<(unsigned)((nq + 255) / 256), 256, 0, s->st>>>(t2, NZf, rc, lc.g, lc.flags, done);
+    } else {
+        restrict_kernel<T, 2><<<restrict_blocks<2>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, rc, lc.g, lc.flags, done);
+    }
     TOPGPU_COUNT_LAUNCH();
 }
 // ... of any level (level 0: the configured level-0 kernel, topgpu_l0.cu)
@@ -419,11 +441,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
             l0_op<T>(s, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega}, ResidOut<T, TR, T>{r0, d, lv.g.cs}, none, done);
         else
             coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs}, none, done);
-        if (lc.span == 4)
-            restrict_kernel<T, 4><<<restrict_blocks<4>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
-        else
-            restrict_kernel<T, 2><<<restrict_blocks<2>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, vr<T>(lc), lc.g, lc.flags, done);
-        TOPGPU_COUNT_LAUNCH();
+        restrict_op<T>(s, l, d, vr<T>(lc), done);
     }
     // coarsest direct solve, FP64
     DevLevel &lc = s->L[nL - 1];
@@ -497,7 +515,9 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         d.g = make_geom(d.ny, d.nx, d.nz);
         d.Ne = M.Ne; d.Nn = M.Nn; d.ng = d.g.cs - 2 * kMargin;
         const int64_t cs = d.g.cs;
-        if (cs >= (int64_t(1) << 31) - 1) { set_error("top_solver_create: level %d grid too large for 32-bit in-array indices", l); top_solver_destroy(s); return TOP_ERR_SHAPE; }
+        if (cs >= (int64_t(1) << 31) - 1 || (l > 0 && 300 * cs >= (int64_t(1) << 31))) {
+            set_error("top_solver_create: level %d grid too large for 32-bit in-array indices", l); top_solver_destroy(s); return TOP_ERR_SHAPE;
+        }
         // host-side flags, node and element maps
         std::vector<uint8_t> fl(cs, 0);
         std::vector<int32_t> ng(M.Nn), eg(M.Ne);
@@ -566,6 +586,16 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
             cudaMemcpy(d.tileFixed, tf.data(), tf.size(), cudaMemcpyHostToDevice);
         }
     }
+    // scratch of the separable span-4 restriction (y-folded fine field)
+    {
+        int64_t nt = 1;
+        for (int l = 0; l + 1 < s->nL; ++l)
+            if (s->L[l + 1].span == 4)
+                nt = std::max<int64_t>(nt, (int64_t)s->L[l + 1].g.NY * (s->L[l].g.NX + s->L[l + 1].g.NX) * s->L[l].g.NZ);
+        s->rscr64 = s->dalloc<double>((size_t)3 * nt);
+        s->rscr32 = s->dalloc<float>((size_t)3 * nt);
+        if (!s->rscr64 || !s->rscr32) return fail("out of device memory");
+    }
     // level-0 data
     DevLevel &l0 = s->L[0];
     const MeshLevel &M0 = mesh->L[0];
@@ -625,10 +655,11 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     // PCG vectors
     const int64_t cs0 = l0.g.cs;
     s->x = s->galloc<double>(cs0, 3); s->r = s->galloc<double>(cs0, 3); s->z = s->galloc<double>(cs0, 3);
+    s->z32 = s->galloc<float>(cs0, 3);
     s->pv = s->galloc<double>(cs0, 3); s->v = s->galloc<double>(cs0, 3); s->tmp = s->galloc<double>(cs0, 3);
     s->b = s->galloc<double>(cs0, 3 * std::max(1, s->nLoads));
     s->weights = s->dalloc<double>(std::max(1, s->nLoads));
-    if (!s->x || !s->r || !s->z || !s->pv || !s->v || !s->tmp || !s->b || !s->weights) return fail("out of device memory");
+    if (!s->x || !s->r || !s->z || !s->z32 || !s->pv || !s->v || !s->tmp || !s->b || !s->weights) return fail("out of device memory");
     cudaMemcpy(s->weights, mesh->weights.data(), sizeof(double) * s->nLoads, cudaMemcpyHostToDevice);
     s->nd0 = 3 * M0.Nn;
     {
@@ -888,9 +919,7 @@ extern "C" int top_solver_restrict(top_solver *s, int ii, const double *rF, doub
     CK(cudaMemsetAsync(f.x64 - kMargin, 0, sizeof(double) * 3 * f.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(f.Nn), 256, 0, s->st>>>(rF, f.x64, f.nodeGrid, f.Nn, f.g.cs);
     TOPGPU_COUNT_LAUNCH();
-    if (c.span == 4) restrict_kernel<double, 4><<<restrict_blocks<4>(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
-    else restrict_kernel<double, 2><<<restrict_blocks<2>(c.g), kNodeThreads, 0, s->st>>>(f.x64, f.g, c.t64, c.g, c.flags, nullptr);
-    TOPGPU_COUNT_LAUNCH();
+    restrict_op<double>(s, ii - 1, f.x64, c.t64, nullptr);
     grid_to_compact_kernel<double, double><<<nb256(c.Nn), 256, 0, s->st>>>(c.t64, rC, c.nodeGrid, c.Nn, c.g.cs);
     TOPGPU_COUNT_LAUNCH();
     CKL();
@@ -998,14 +1027,17 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
 {
     if (!s->assembled) { set_error("top_solver_pcg: assemble first"); return TOP_ERR_STATE; }
     DevLevel &l0 = s->L[0];
-    const int64_t cs = l0.g.cs, ng = l0.ng;
+    const int64_t cs = l0.g.cs, nv = 3 * cs;    // whole grid vectors, margins included
     cudaStream_t st = s->st;
-    const int VB = vec_blocks(ng);
+    const int VB = vec_blocks(nv);
+    const int64_t M = kMargin;
+    // mixed precision keeps the FP32 V-cycle's output z in FP32
+    const bool z32 = s->p.precision == TOP_PREC_MIXED;
     PcgState h{};
     h.tol = s->p.tol; h.maxIT = s->p.maxIT;
     CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
     int *done = &s->state->done;
-    dot_kernel<<<VB, 256, 0, st>>>(bGrid, bGrid, ng, cs, s->red(&s->state->normB));
+    dot_kernel<<<VB, 256, 0, st>>>(bGrid - M, bGrid - M, nv, s->red(&s->state->normB));
     TOPGPU_COUNT_LAUNCH();
     pcg_init_kernel<<<1, 1, 0, st>>>(s->state);
     TOPGPU_COUNT_LAUNCH();
@@ -1018,22 +1050,28 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
         l0_op<double>(s, VecIn<double, double>{xg, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
                          Reduce{nullptr, nullptr, nullptr}, done);
     // z = M r ; rho = z . r ; p = z
-    precond(s, s->r, s->z, &s->state->rho, done);
-    pcg_p_kernel<<<VB, 256, 0, st>>>(s->pv, s->z, ng, cs, s->state, 1);
-    TOPGPU_COUNT_LAUNCH();
+    auto precond_p = [&](cudaStream_t q, int first) {                                         // z = M r, z.r; p = z + beta p
+        if (z32) {
+            vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done);
+            pcg_p_kernel<float><<<VB, 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first);
+        } else {
+            vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done);
+            pcg_p_kernel<double><<<VB, 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first);
+        }
+        TOPGPU_COUNT_LAUNCH();
+    };
+    precond_p(st, 1);
     CKL();
     static const bool trace = std::getenv("TOPGPU_PCG_TRACE") != nullptr;
     const int chunk = trace ? 1 : 4;
     // one PCG iteration (TOP_GPU.m:620-655); every kernel returns at once when done is set
     auto iteration = [&](cudaStream_t q) {
         outer_op(s, s->pv, s->v, &s->state->pv, done);                                       // v = A p, p.v
-        pcg_update_kernel<<<VB, 256, 0, q>>>(xg, s->r, s->pv, s->v, ng, cs, s->state, s->red(&s->state->rr));
+        pcg_update_kernel<<<VB, 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, s->red(&s->state->rr));
         TOPGPU_COUNT_LAUNCH();
         pcg_check_kernel<<<1, 1, 0, q>>>(s->state);
         TOPGPU_COUNT_LAUNCH();
-        precond(s, s->r, s->z, &s->state->rho, done);                                         // z = M r, z.r
-        pcg_p_kernel<<<VB, 256, 0, q>>>(s->pv, s->z, ng, cs, s->state, 0);                  // p = z + beta p
-        TOPGPU_COUNT_LAUNCH();
+        precond_p(q, 0);
     };
     top_solver::PcgGraph *G = nullptr;
     if (s->useGraphs && !trace)
@@ -1144,6 +1182,15 @@ extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_
         case 0: l0_op<double>(s, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr); break;
         case 1: l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr); break;
         case 2: precond(s, s->r, s->z, nullptr, s->zeroDone); break;
+        case 4: if (s->nL > 2) {   // level-0 -> level-1 restriction, FP32
+            restrict_op<float>(s, 0, s->L[0].t32, s->L[1].r32, nullptr);
+        } break;
+        case 5: if (s->nL > 2) {   // level-1 -> level-0 prolongation with the Jacobi base, FP32
+            DevLevel &f = s->L[0], &c = s->L[1];
+            if (c.span == 4) prolong_kernel<float, 4, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
+            else prolong_kernel<float, 2, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
+            TOPGPU_COUNT_LAUNCH();
+        } break;
         case 3: if (s->nL > 2) coarse_op<float>(s, 1, VecIn<float, float>{s->L[1].x32, s->L[1].g.cs}, StoreOut<float, float>{s->L[1].t32, s->L[1].g.cs}, none, nullptr); break;
         default: set_error("top_solver_time_kernel: unknown kernel %d", which); return TOP_ERR_ARGS;
         }

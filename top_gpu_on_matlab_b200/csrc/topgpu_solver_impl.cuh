@@ -3,6 +3,7 @@
 // (filters, sensitivities, OC loop).
 #pragma once
 #include <cuda_runtime.h>
+#include <cstdlib>
 #include <vector>
 #include "topgpu_grid.cuh"
 #include "topgpu_walsh.cuh"
@@ -45,6 +46,7 @@ struct top_solver {
     std::vector<PcgGraph> graphs;    // one per (right-hand side, solution) pair in use
     cudaStream_t capStream = nullptr; cudaEvent_t capIn = nullptr, capOut = nullptr;
     bool useGraphs = true;
+    bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
     int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
     std::vector<DevLevel> L;
@@ -67,6 +69,8 @@ struct top_solver {
     double *Qs = nullptr; int32_t *eye = nullptr;
     int32_t *bndList = nullptr; int64_t nBnd = 0;   // level-1 cells with fixed-DOF children
     double *x = nullptr, *r = nullptr, *z = nullptr, *pv = nullptr, *v = nullptr, *tmp = nullptr;
+    float *z32 = nullptr;            // FP32 preconditioned residual of the mixed path
+    double *rscr64 = nullptr; float *rscr32 = nullptr;   // separable restriction scratch
     double *b = nullptr;             // [nLoads][3 x cs]
     double *weights = nullptr;
     PcgState *state = nullptr, *hstate = nullptr;
