@@ -240,6 +240,30 @@ int top_solver_set_design(top_solver *s, const double *xPhys, const double *x);
 int top_solver_optimize(top_solver *s, const top_opt_params *prm, double *xPhysOut,
                         top_opt_record *hist, int *nIter, double *cSolid);
 
+/* Adjoint sensitivities at the design xPhys (device, [Ne]; x = the design
+ * variables for ft = 1, NULL: xPhys).  objective 0: the weighted compliance
+ * J = sum_k w_k F_k' U_k, self-adjoint, dJ/dxPhys_e = -p xPhys^(p-1)
+ * (E0-Emin) sum_k w_k U_ke' Ke U_ke (the reference's dc times cSolid,
+ * TOP_GPU.m:191-198, 580-600); objective 1: the displacement J = U_k[dof]
+ * (DOF in the reference's node-interleaved numbering, 0-based), with the
+ * adjoint solve K L = e_dof and dJ/dxPhys_e = -p xPhys^(p-1) (E0-Emin)
+ * L_e' Ke U_e.  The state (and adjoint) solves start cold and stop at
+ * relative residual tol (0: the solver's).  ft chains the result to the
+ * design variables: 0 none, 1 the reference's sensitivity filter
+ * H(x.*g)/max(1e-3,x), 2 the PDE density filter's transpose (the filter is
+ * symmetric); ft != 0 needs top_solver_filter_setup.  Writes dJdx [Ne]
+ * (device), J and the summed PCG iterations (either may be NULL).  The
+ * reference has the compliance sensitivity only. */
+typedef struct {
+    int     objective;   /* 0 compliance, 1 displacement                          */
+    int     loadCase;    /* objective 1: load case k                              */
+    int64_t dof;         /* objective 1: DOF index                                */
+    int     ft;          /* 0, 1, 2                                               */
+    double  tol;         /* PCG relative residual of the solves (0: solver's)     */
+} top_sens_params;
+int top_solver_sensitivity(top_solver *s, const top_sens_params *prm, const double *xPhys, const double *x,
+                           double *dJdx, double *J, int *pcgIts);
+
 /* Kernel timing with CUDA events on the solver's stream (no host copies):
  * which = 0 level-0 K*u FP64, 1 level-0 K*u FP32, 2 one V-cycle,
  * 3 level-1 K*u FP32, 4 level 0 -> 1 restriction FP32, 5 level 1 -> 0

@@ -52,6 +52,10 @@ class SolverParams(C.Structure):
     ]
 
 
+class SensParams(C.Structure):
+    _fields_ = [("objective", C.c_int), ("loadCase", C.c_int), ("dof", C.c_int64), ("ft", C.c_int), ("tol", C.c_double)]
+
+
 class OptParams(C.Structure):
     _fields_ = [("V0", C.c_double), ("rMin", C.c_double), ("nLoop", C.c_int), ("ft", C.c_int)]
 
@@ -109,6 +113,7 @@ SIGNATURES = {
     "top_solver_get_l0_kernel": (_int, [_vp, _int, _vp]),
     "top_solver_autotune": (_int, [_vp, _int, _i64, _vp, _vp]),
     "top_solver_set_graphs": (_int, [_vp, _int]),
+    "top_solver_sensitivity": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "top_solver_optimize": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
 }
 

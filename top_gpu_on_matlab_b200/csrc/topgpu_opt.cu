@@ -37,6 +37,14 @@ struct FilterState {
     PcgState *st = nullptr;
 };
 
+struct AdjState {
+    double *U = nullptr;     // [nLoads][3 x cs] state fields
+    double *L = nullptr;     // [3 x cs] adjoint field
+    double *e = nullptr;     // [3 x cs] unit load
+    double *g = nullptr, *t = nullptr;   // element vectors [Ne]
+    double *J = nullptr;     // device scalar
+};
+
 struct OptState {
     bool begun = false;
     top_opt_params prm{};
@@ -377,7 +385,8 @@ void topgpu::free_opt_state(top_solver *s)
 {
     delete reinterpret_cast<FilterState *>(s->filterState);
     delete reinterpret_cast<OptState *>(s->optState);
-    s->filterState = s->optState = nullptr;
+    delete reinterpret_cast<AdjState *>(s->adjState);
+    s->filterState = s->optState = s->adjState = nullptr;
 }
 
 extern "C" int top_solver_filter_setup(top_solver *s, double rMin)
@@ -697,5 +706,155 @@ extern "C" int top_solver_optimize(top_solver *s, const top_opt_params *prm, dou
     }
     if (nIter) *nIter = o.loop;
     if (xPhysOut) return top_solver_get_design(s, xPhysOut, nullptr);
+    return TOP_OK;
+}
+
+// ============================================================================
+// Adjoint sensitivities.  For K(E(xPhys)) U = F and an objective J(U):
+//   compliance J = sum_k w_k F_k' U_k is self-adjoint: dJ/dE_e = -sum_k w_k U_ke' Ke U_ke
+//   (the reference's element energies, TOP_GPU.m:580-600, 191-198);
+//   a displacement J = U_k[dof] needs the adjoint solve K L = e_dof:
+//   dJ/dE_e = -L_e' Ke U_ke.
+// Elements with fixed DOFs use E Kfree + Kfixed (TOP_GPU.m:1729-1741); U and L
+// vanish on the fixed DOFs, so Ke gives the same products.  dE/dxPhys =
+// p xPhys^(p-1) (E0 - Emin) (SIMP, TOP_GPU.m:169).  The chain to the design
+// variables follows the filter: ft = 1 the reference's sensitivity filter
+// dc = H(x .* dc) / max(1e-3, x) (TOP_GPU.m:213-219), ft = 2 the PDE density
+// filter's transpose (the Helmholtz filter is symmetric: H' = H).
+
+namespace {
+AdjState &adj(top_solver *s) { return *reinterpret_cast<AdjState *>(s->adjState); }
+
+// dJ[e] = -p x^(p-1) (E0-Emin) sum_k w_k A_ke' Ke B_ke ; J += sum_e E_e sum_k w_k A_ke' Ke B_ke
+__global__ void mutual_energy_kernel(const KeParam<double> K, const double *__restrict__ A, int64_t aStride,
+                                     const double *__restrict__ B, int64_t bStride, int nPairs,
+                                     const double *__restrict__ w, const int32_t *__restrict__ eleGrid, int64_t Ne,
+                                     Geom g, const double *__restrict__ xPhys, const double *__restrict__ Ec,
+                                     double E0, double Emin, double penal, double *__restrict__ dJ, Reduce redJ)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double jpart = 0;
+    if (e < Ne) {
+        const int slot = eleGrid[e];
+        double acc = 0;
+        for (int k = 0; k < nPairs; ++k) {
+            const double *a = A + k * aStride, *b = B + k * bStride;
+            double ae[24], be[24];
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int64_t o = c * g.cs + slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j);
+                    ae[3 * j + c] = a[o];
+                    be[3 * j + c] = b[o];
+                }
+            double m = 0;
+#pragma unroll
+            for (int r = 0; r < 24; ++r) {
+                double t = 0;
+#pragma unroll
+                for (int q = 0; q < 24; ++q) t = fma(K.k[r + 24 * q], be[q], t);
+                m = fma(ae[r], t, m);
+            }
+            acc += (w ? w[k] : 1.0) * m;
+        }
+        const double x = xPhys[e];
+        dJ[e] = -(penal * (E0 - Emin) * pow(x, penal - 1.0)) * acc;
+        jpart = Ec[e] * acc;
+    }
+    if (redJ.result) block_sum_to<256>(jpart, redJ.partials, redJ.counter, redJ.result);
+}
+__global__ void unit_load_kernel(double *__restrict__ v, const int32_t *__restrict__ nodeGrid, int64_t node, int comp, int64_t cs)
+{
+    v[comp * cs + nodeGrid[node]] = 1.0;
+}
+__global__ void pick_dof_kernel(const double *__restrict__ U, const int32_t *__restrict__ nodeGrid, int64_t node, int comp,
+                                int64_t cs, double *__restrict__ out)
+{
+    *out = U[comp * cs + nodeGrid[node]];
+}
+}  // namespace
+
+extern "C" int top_solver_sensitivity(top_solver *s, const top_sens_params *prm, const double *xPhys, const double *x,
+                                      double *dJdx, double *Jout, int *itsOut)
+{
+    if (!s || !prm || !xPhys || !dJdx) return TOP_ERR_ARGS;
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs, Ne = l0.Ne;
+    if (prm->objective != 0 && prm->objective != 1) { set_error("top_solver_sensitivity: unknown objective %d", prm->objective); return TOP_ERR_ARGS; }
+    if (prm->objective == 1 && (prm->loadCase < 0 || prm->loadCase >= s->nLoads || prm->dof < 0 || prm->dof >= s->nd0)) {
+        set_error("top_solver_sensitivity: load case or DOF out of range"); return TOP_ERR_ARGS;
+    }
+    if (prm->ft < 0 || prm->ft > 2) { set_error("top_solver_sensitivity: ft must be 0, 1 or 2"); return TOP_ERR_ARGS; }
+    if (prm->ft != 0 && (!s->filterState || !filt(s).ready)) { set_error("top_solver_sensitivity: call top_solver_filter_setup first"); return TOP_ERR_STATE; }
+    if (!s->adjState) s->adjState = new AdjState();
+    AdjState &a = adj(s);
+    if (!a.U) {
+        a.U = s->galloc<double>(cs, 3 * s->nLoads); a.L = s->galloc<double>(cs, 3); a.e = s->galloc<double>(cs, 3);
+        a.g = s->dalloc<double>(Ne); a.t = s->dalloc<double>(Ne); a.J = s->dalloc<double>(1);
+        if (!a.U || !a.L || !a.e || !a.g || !a.t || !a.J) { set_error("top_solver_sensitivity: out of device memory"); return TOP_ERR_NOMEM; }
+    }
+    cudaStream_t st = s->st;
+    int rc = set_modulus_dev(s, xPhys, 1, 1);
+    if (rc) return rc;
+    rc = top_solver_assemble(s);
+    if (rc) return rc;
+    const double tolKeep = s->p.tol;
+    if (prm->tol > 0) s->p.tol = prm->tol;
+    int its = 0, tot = 0;
+    // state solves (cold start)
+    const int k0 = prm->objective == 0 ? 0 : prm->loadCase, k1 = prm->objective == 0 ? s->nLoads : prm->loadCase + 1;
+    for (int k = k0; k < k1 && rc == TOP_OK; ++k) {
+        rc = pcg_grid(s, s->b + (size_t)k * 3 * cs, a.U + (size_t)k * 3 * cs, 0, &its, nullptr);
+        tot += its;
+    }
+    double J = 0;
+    if (rc == TOP_OK && prm->objective == 0) {
+        mutual_energy_kernel<<<nb256(Ne), 256, 0, st>>>(s->Ke64, a.U, 3 * cs, a.U, 3 * cs, s->nLoads, s->weights, l0.eleGrid, Ne,
+                                                        l0.g, xPhys, s->Ec, s->p.E0, s->p.Emin, s->p.penal, a.g, s->red(a.J));
+        TOPGPU_COUNT_LAUNCH();
+        CK(cudaMemcpyAsync(&J, a.J, sizeof(double), cudaMemcpyDeviceToHost, st));
+    } else if (rc == TOP_OK) {
+        // adjoint: K L = e_dof (the reference's DOF numbering: node-interleaved, compact nodes)
+        const int64_t node = prm->dof / 3; const int comp = (int)(prm->dof % 3);
+        const double *Uk = a.U + (size_t)prm->loadCase * 3 * cs;
+        CK(cudaMemsetAsync(a.e - kMargin, 0, sizeof(double) * 3 * cs, st));
+        unit_load_kernel<<<1, 1, 0, st>>>(a.e, l0.nodeGrid, node, comp, cs);
+        TOPGPU_COUNT_LAUNCH();
+        pick_dof_kernel<<<1, 1, 0, st>>>(Uk, l0.nodeGrid, node, comp, cs, a.J);
+        TOPGPU_COUNT_LAUNCH();
+        CK(cudaMemcpyAsync(&J, a.J, sizeof(double), cudaMemcpyDeviceToHost, st));
+        rc = pcg_grid(s, a.e, a.L, 0, &its, nullptr);
+        tot += its;
+        if (rc == TOP_OK) {
+            mutual_energy_kernel<<<nb256(Ne), 256, 0, st>>>(s->Ke64, a.L, 0, Uk, 0, 1, nullptr, l0.eleGrid, Ne, l0.g, xPhys,
+                                                            s->Ec, s->p.E0, s->p.Emin, s->p.penal, a.g, Reduce{nullptr, nullptr, nullptr});
+            TOPGPU_COUNT_LAUNCH();
+        }
+    }
+    s->p.tol = tolKeep;
+    if (rc != TOP_OK) return rc;
+    // chain to the design variables
+    const int VB = vb(Ne);
+    int fits = 0;
+    if (prm->ft == 0) {
+        copy_kernel<<<VB, 256, 0, st>>>(a.g, dJdx, Ne);
+        TOPGPU_COUNT_LAUNCH();
+    } else if (prm->ft == 1) {
+        const double *xd = x ? x : xPhys;
+        mul_kernel<<<VB, 256, 0, st>>>(xd, a.g, a.t, Ne);
+        TOPGPU_COUNT_LAUNCH();
+        rc = filter_apply(s, a.t, a.g, &fits);
+        if (rc) return rc;
+        div_floor_kernel<<<VB, 256, 0, st>>>(a.g, xd, dJdx, Ne);
+        TOPGPU_COUNT_LAUNCH();
+    } else {
+        rc = filter_apply(s, a.g, dJdx, &fits);
+        if (rc) return rc;
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    if (Jout) *Jout = J;
+    if (itsOut) *itsOut = tot;
     return TOP_OK;
 }

@@ -81,7 +81,7 @@ struct top_solver {
     int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
     bool assembled = false;
     int64_t launches = 0;            // kernels launched by this solver (all entry points)
-    void *filterState = nullptr, *optState = nullptr;   // topgpu_opt.cu
+    void *filterState = nullptr, *optState = nullptr, *adjState = nullptr;   // topgpu_opt.cu
     std::vector<double> Fhost; int64_t nd0 = 0;
 
     template <typename T> T *dalloc(size_t n)

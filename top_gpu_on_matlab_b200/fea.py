@@ -273,6 +273,24 @@ class Solver:
         check(lib().top_solver_get_l0_kernel(self._h, int(bool(fp32)), out), "top_solver_get_l0_kernel")
         return tuple(out)
 
+    def sensitivity(self, xPhys, objective="compliance", dof=None, load_case=0, ft=0, x=None, tol=0.0):
+        """Adjoint sensitivity dJ/dx at design xPhys (CUDA float64 [Ne]).  objective
+        "compliance" (self-adjoint) or "displacement" (J = U[dof], adjoint solve);
+        ft 0/1/2 chains through no filter / the sensitivity filter / the PDE
+        density filter (filter_setup first).  Returns (dJdx, J, pcg_its)."""
+        from ._lib import SensParams
+        obj = {"compliance": 0, "displacement": 1}[objective]
+        prm = SensParams(objective=obj, loadCase=load_case, dof=-1 if dof is None else int(dof), ft=ft, tol=tol)
+        ne = self.levels[0]["numElements"]
+        if xPhys.dtype != torch.float64 or xPhys.numel() != ne or not xPhys.is_cuda:
+            raise ValueError("sensitivity: CUDA float64 xPhys of numElements expected")
+        out = torch.empty(ne, dtype=torch.float64, device=xPhys.device)
+        J, its = C.c_double(0), C.c_int(0)
+        check(lib().top_solver_sensitivity(self._h, C.byref(prm), xPhys.data_ptr(),
+                                           None if x is None else x.data_ptr(), out.data_ptr(),
+                                           C.byref(J), C.byref(its)), "top_solver_sensitivity")
+        return out, J.value, its.value
+
     def set_graphs(self, on):
         """Run PCG iterations as captured CUDA graphs (default) or launch by launch."""
         check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
