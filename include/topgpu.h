@@ -173,7 +173,8 @@ int top_solver_create(const top_mesh *mesh, const top_solver_params *p, top_solv
 int top_solver_destroy(top_solver *s);
 int top_solver_set_stream(top_solver *s, void *stream);
 
-/* Element moduli.  where: 0 = host pointer, 1 = device pointer.
+/* Element moduli ([64 x Ne] sub-voxel values for super-element models).
+ * where: 0 = host pointer, 1 = device pointer.
  * set_density applies SIMP: E = Emin + x^p (E0 - Emin) (TOP_GPU.m:169). */
 int top_solver_set_modulus(top_solver *s, const double *E, int where);
 int top_solver_set_density(top_solver *s, const double *xPhys, int where);
@@ -224,6 +225,13 @@ typedef struct {     /* one optimisation iteration (TOP_GPU.m:279-291)         *
  * tol/10; its may be NULL. */
 int top_solver_filter_setup(top_solver *s, double rMin);
 int top_solver_filter(top_solver *s, const double *src, double *tar, int *its);
+/* Super-element density filter (TOP_GPU.m:113-121, 221-227, 262-265) on
+ * [64 x Ne] sub-voxel vectors (device): h = max(0, 4 rMin - dist),
+ * Hs = imfilter(ones, h); mode 0: tar = imfilter(src ./ Hs, h) (the
+ * sensitivities), mode 1: tar = imfilter(src, h) ./ Hs (the densities).
+ * Super-element models on a full box only. */
+int top_solver_super_filter_setup(top_solver *s, double rMin);
+int top_solver_super_filter(top_solver *s, const double *src, double *tar, int mode);
 /* The optimisation loop of TOP_GPU.m:141-292 on the device: opt_begin runs
  * the fully solid solve (cSolid) and sets x = xPhys = V0; each opt_step is
  * one iteration (SIMP, assembly, warm-started PCG per load case,

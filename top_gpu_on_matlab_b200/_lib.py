@@ -103,6 +103,8 @@ SIGNATURES = {
     "top_solver_time_kernel": (_int, [_vp, _int, _int, _i64, _vp]),
     "top_solver_filter_setup": (_int, [_vp, _dbl]),
     "top_solver_filter": (_int, [_vp, _vp, _vp, _vp]),
+    "top_solver_super_filter_setup": (_int, [_vp, _dbl]),
+    "top_solver_super_filter": (_int, [_vp, _vp, _vp, _int]),
     "top_solver_opt_begin": (_int, [_vp, _vp, _vp]),
     "top_solver_opt_step": (_int, [_vp, _vp]),
     "top_solver_opt_state": (_int, [_vp, _vp, _vp, _vp]),

@@ -52,13 +52,15 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
 {
     __shared__ double red[NT / 32];
     __shared__ bool last;
+    // linear thread index: blocks may be 1-, 2- or 3-D (NT threads in all)
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = tid & 31, w = tid >> 5;
     if (lane == 0) red[w] = v;
     __syncthreads();
     const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
     const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         double s = 0;
         for (int i = 0; i < NT / 32; ++i) s += red[i];
         partials[bid] = s;
@@ -69,11 +71,11 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
     if (!last) return;
     __threadfence();
     double s = 0;
-    for (unsigned i = threadIdx.x; i < nb; i += NT) s += ((volatile double *)partials)[i];
+    for (unsigned i = tid; i < nb; i += NT) s += ((volatile double *)partials)[i];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) red[w] = s;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         double t = 0;
         for (int i = 0; i < NT / 32; ++i) t += red[i];
         *result = t;

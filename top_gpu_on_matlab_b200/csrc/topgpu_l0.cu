@@ -66,7 +66,11 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
 {
     DevLevel &lv = s->L[0];
     const top_solver::L0Kernel &k = s->l0k[prec_slot<T>()];
-    if (k.kind == 1) {
+    if (s->super) {                   // per-element matrices (K_mat), packed on the grid
+        const T *Kp;
+        if constexpr (sizeof(T) == 8) Kp = lv.KsP64; else Kp = lv.KsP32;
+        coarse_tile_kernel<T, In, Out><<<coarse_tile_grid(lv.g), dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, Kp, lv.g, red, done);
+    } else if (k.kind == 1) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                     \
         if (k.ty == A && k.tx == B)                                                                   \
             l0w_kernel<T, A, B, In, Out><<<l0w_ctas<T, A, B, In, Out, 1>(s, k), A * B, 0, s->st>>>(   \

@@ -45,6 +45,17 @@ struct AdjState {
     double *J = nullptr;     // device scalar
 };
 
+// Super-element density filter on the 4x refined sub-voxel grid
+// (TOP_GPU.m:113-121, 221-227, 262-265): h = max(0, 4 rMin - dist) over a
+// (2R+1)^3 box, R = ceil(4 rMin) - 1, imfilter with zero padding;
+// Hs = imfilter(ones, h).
+struct SFilterState {
+    bool ready = false;
+    double rMin = 0;
+    int R = 0, fy = 0, fx = 0, fz = 0;
+    double *h = nullptr, *Hs = nullptr, *g = nullptr, *t = nullptr;
+};
+
 struct OptState {
     bool begun = false;
     top_opt_params prm{};
@@ -55,6 +66,8 @@ struct OptState {
     double *U = nullptr;     // [nLoads][3 x cs] grid displacement fields (warm starts)
     OptScalars *sc = nullptr, *hsc = nullptr;
     double *ocPartials = nullptr; int ocBlocks = 0;
+    int64_t nv = 0;          // design variables (64 per super-element)
+    SFilterState sf;         // super-element density filter
 };
 
 }  // namespace topgpu
@@ -236,6 +249,61 @@ __global__ void fpcg_start_kernel(PcgState *st, double tol, int maxIT)
     st->done = st->normB == 0.0 ? 1 : 0;
 }
 
+// ---- super-element density filter ---------------------------------------------
+// sub-voxel (q, e) of the element-major [64 x Ne] layout <-> fine-grid voxel
+// (y fastest); q = ly + 4 (lx + 4 lz) (gen_index_mapping, TOP_GPU.m:2673-2697)
+__device__ __forceinline__ int64_t sub_to_fine(int64_t i, int ny, int nx, int fy, int fx)
+{
+    const int64_t e = i / 64; const int q = (int)(i % 64);
+    const int ey = (int)(e % ny), ex = (int)((e / ny) % nx), ez = (int)(e / ((int64_t)ny * nx));
+    const int y = 4 * ey + (q & 3), x = 4 * ex + ((q >> 2) & 3), z = 4 * ez + (q >> 4);
+    return y + (int64_t)fy * (x + (int64_t)fx * z);
+}
+// mode 0: g = in ./ Hs (sensitivities), mode 1: g = in (densities)
+__global__ void sfilt_gather_kernel(const double *__restrict__ in, const double *__restrict__ Hs, int mode, int ny, int nx,
+                                    int fy, int fx, int64_t n, double *__restrict__ g)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t f = sub_to_fine(i, ny, nx, fy, fx);
+    g[f] = mode == 0 ? in[i] / Hs[f] : in[i];
+}
+__global__ void sfilt_scatter_kernel(const double *__restrict__ t, const double *__restrict__ Hs, int mode, int ny, int nx,
+                                     int fy, int fx, int64_t n, double *__restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t f = sub_to_fine(i, ny, nx, fy, fx);
+    out[i] = mode == 1 ? t[f] / Hs[f] : t[f];
+}
+// t = imfilter(g, h): correlation, zero outside (the kernel is symmetric)
+__global__ void sfilt_conv_kernel(const double *__restrict__ g, const double *__restrict__ h, int R, int fy, int fx, int fz,
+                                  double *__restrict__ t)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)fy * fx * fz;
+    if (i >= n) return;
+    const int y = (int)(i % fy), x = (int)((i / fy) % fx), z = (int)(i / ((int64_t)fy * fx));
+    const int w = 2 * R + 1;
+    double s = 0;
+    for (int dz = -R; dz <= R; ++dz) {
+        const int zz = z + dz;
+        if (zz < 0 || zz >= fz) continue;
+        for (int dx = -R; dx <= R; ++dx) {
+            const int xx = x + dx;
+            if (xx < 0 || xx >= fx) continue;
+            const double *gr = g + (int64_t)fy * (xx + (int64_t)fx * zz);
+            const double *hr = h + w * ((dx + R) + w * (dz + R)) + R;
+            for (int dy = -R; dy <= R; ++dy) {
+                const int yy = y + dy;
+                if (yy < 0 || yy >= fy) continue;
+                s = fma(gr[yy], hr[dy], s);
+            }
+        }
+    }
+    t[i] = s;
+}
+
 // ---- sensitivities ----------------------------------------------------------
 // ce_e = sum_k w_k u_ke' Ke u_ke; dc = -p (E0-Emin) x^(p-1) ce / cSolid; dv = 1;
 // sums: cObj = sum E_e ce_e / cSolid, sumX = sum xPhys (TOP_GPU.m:191-199)
@@ -278,6 +346,70 @@ __global__ void sensitivity_kernel(const KeParam<double> K, const double *__rest
         cpart = Ec[e] * cn;
     }
     if (redC.result) block_sum_to<256>(cpart, redC.partials, redC.counter, redC.result);
+}
+// super-element mode: ce_e = sum_k w_k u_ke' K_mat_e u_ke (TOP_GPU.m:2622-2645),
+// dc(q, e) = -p x^(p-1) (E0-Emin) sum_k w_k u_ke' I_q u_ke / cSolid
+// (pre_compute_der, 2646-2671); one 64-thread CTA per element, thread = q
+__global__ void __launch_bounds__(64)
+sensitivity_super_kernel(const double *__restrict__ Imat, const double *__restrict__ Kc, const double *__restrict__ U,
+                         int64_t ustride, int nLoads, const double *__restrict__ w, const int32_t *__restrict__ eleGrid,
+                         Geom g, const double *__restrict__ xPhys, double E0, double Emin, double penal, double cSolid,
+                         double *__restrict__ ce, double *__restrict__ dc, double *__restrict__ dv, Reduce redC)
+{
+    __shared__ double ue[24];
+    __shared__ double part[24];
+    const int64_t e = blockIdx.x;
+    const int q = threadIdx.x;
+    const int slot = eleGrid[e];
+    double dq = 0, cp = 0;
+    for (int k = 0; k < nLoads; ++k) {
+        const double *u = U + k * ustride;
+        if (q < 24) {
+            const int j = q / 3, c = q % 3;
+            ue[q] = u[c * g.cs + slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j)];
+        }
+        __syncthreads();
+        const double *I = Imat + (size_t)q * 576;
+        double a = 0;
+        for (int col = 0; col < 24; ++col) {
+            double r = 0;
+#pragma unroll
+            for (int row = 0; row < 24; ++row) r = fma(I[row + 24 * col], ue[row], r);
+            a = fma(r, ue[col], a);
+        }
+        dq += w[k] * a;
+        if (q < 24) {
+            const double *K = Kc + e * 576;
+            double r = 0;
+#pragma unroll
+            for (int col = 0; col < 24; ++col) r = fma(K[q + 24 * col], ue[col], r);
+            cp += w[k] * r * ue[q];
+        }
+        __syncthreads();
+    }
+    if (q < 24) part[q] = cp;
+    __syncthreads();
+    double cpart = 0;
+    if (q == 0) {
+        double sc = 0;
+        for (int i = 0; i < 24; ++i) sc += part[i];
+        if (ce) ce[e] = sc;
+        cpart = cSolid > 0 ? sc / cSolid : sc;
+    }
+    if (dc) {
+        const double x = xPhys[e * 64 + q];
+        const double dn = cSolid > 0 ? dq / cSolid : dq;
+        dc[e * 64 + q] = -(penal * (E0 - Emin) * pow(x, penal - 1.0)) * dn;
+        dv[e * 64 + q] = 1.0;
+    }
+    if (redC.result) block_sum_to<64>(cpart, redC.partials, redC.counter, redC.result);
+}
+
+__global__ void sum_scaled_kernel(const double *__restrict__ a, int64_t n, double scale, Reduce red)
+{
+    double s = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += a[i] * scale;
+    block_sum_to<256>(s, red.partials, red.counter, red.result);
 }
 __global__ void sum_kernel(const double *__restrict__ a, int64_t n, int mode, Reduce red)
 {   // mode 0: sum a ; mode 1: sum a(1-a)
@@ -384,6 +516,7 @@ int ensure_state(top_solver *s)
 void topgpu::free_opt_state(top_solver *s)
 {
     delete reinterpret_cast<FilterState *>(s->filterState);
+    if (s->optState && opt(s).sf.h) cudaFree(opt(s).sf.h);
     delete reinterpret_cast<OptState *>(s->optState);
     delete reinterpret_cast<AdjState *>(s->adjState);
     s->filterState = s->optState = s->adjState = nullptr;
@@ -477,6 +610,76 @@ extern "C" int top_solver_filter(top_solver *s, const double *src, double *tar, 
     return TOP_OK;
 }
 
+// ---- super-element density filter (host side) --------------------------------
+static int sfilter_setup(top_solver *s, double rMin)
+{
+    OptState &o = opt(s);
+    SFilterState &f = o.sf;
+    DevLevel &l0 = s->L[0];
+    if ((int64_t)s->nely * s->nelx * s->nelz != l0.Ne) {
+        set_error("super-element filter: needs a full box of super-elements"); return TOP_ERR_SHAPE;
+    }
+    const double r = 4.0 * rMin;
+    f.R = (int)std::ceil(r) - 1;
+    const int w = 2 * f.R + 1;
+    f.fy = 4 * s->nely; f.fx = 4 * s->nelx; f.fz = 4 * s->nelz;
+    const int64_t N = (int64_t)f.fy * f.fx * f.fz;
+    if (!f.Hs) {
+        f.Hs = s->dalloc<double>(N); f.g = s->dalloc<double>(N); f.t = s->dalloc<double>(N);
+        if (!f.Hs || !f.g || !f.t) { set_error("super-element filter: out of device memory"); return TOP_ERR_NOMEM; }
+    }
+    std::vector<double> h((size_t)w * w * w);
+    for (int dz = -f.R; dz <= f.R; ++dz)
+        for (int dx = -f.R; dx <= f.R; ++dx)
+            for (int dy = -f.R; dy <= f.R; ++dy) {
+                const double v = r - std::sqrt(double(dx * dx + dy * dy + dz * dz));
+                h[(dy + f.R) + w * ((dx + f.R) + w * (dz + f.R))] = v > 0 ? v : 0.0;
+            }
+    if (f.h) cudaFree(f.h);
+    if (cudaMalloc(&f.h, sizeof(double) * h.size()) != cudaSuccess) { f.h = nullptr; return TOP_ERR_NOMEM; }
+    CK(cudaMemcpyAsync(f.h, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice, s->st));
+    fill_kernel<<<vb(N), 256, 0, s->st>>>(f.g, 1.0, N);
+    TOPGPU_COUNT_LAUNCH();
+    sfilt_conv_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s->st>>>(f.g, f.h, f.R, f.fy, f.fx, f.fz, f.Hs);
+    TOPGPU_COUNT_LAUNCH();
+    CK(cudaStreamSynchronize(s->st));      // h (host vector) is consumed
+    f.rMin = rMin;
+    f.ready = true;
+    return TOP_OK;
+}
+// mode 0: out = imfilter(in ./ Hs, h) ; mode 1: out = imfilter(in, h) ./ Hs
+static int sfilter_apply(top_solver *s, const double *in, double *out, int mode)
+{
+    SFilterState &f = opt(s).sf;
+    const int64_t n = 64 * s->L[0].Ne, N = (int64_t)f.fy * f.fx * f.fz;
+    sfilt_gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(in, f.Hs, mode, s->nely, s->nelx, f.fy, f.fx, n, f.g);
+    TOPGPU_COUNT_LAUNCH();
+    sfilt_conv_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s->st>>>(f.g, f.h, f.R, f.fy, f.fx, f.fz, f.t);
+    TOPGPU_COUNT_LAUNCH();
+    sfilt_scatter_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->st>>>(f.t, f.Hs, mode, s->nely, s->nelx, f.fy, f.fx, n, out);
+    TOPGPU_COUNT_LAUNCH();
+    CK(cudaGetLastError());
+    return TOP_OK;
+}
+
+extern "C" int top_solver_super_filter_setup(top_solver *s, double rMin)
+{
+    if (!s || !(rMin > 0)) return TOP_ERR_ARGS;
+    if (!s->super) { set_error("top_solver_super_filter_setup: super-element models only"); return TOP_ERR_ARGS; }
+    ensure_state(s);
+    return sfilter_setup(s, rMin);
+}
+
+extern "C" int top_solver_super_filter(top_solver *s, const double *src, double *tar, int mode)
+{
+    if (!s || !src || !tar || (mode != 0 && mode != 1)) return TOP_ERR_ARGS;
+    if (!s->optState || !opt(s).sf.ready) { set_error("top_solver_super_filter: call top_solver_super_filter_setup first"); return TOP_ERR_STATE; }
+    const int rc = sfilter_apply(s, src, tar, mode);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return TOP_OK;
+}
+
 // ---- the optimisation loop ---------------------------------------------------
 static int solve_all(top_solver *s, int warm, int *itsTotal)
 {
@@ -499,6 +702,18 @@ static int sensitivities(top_solver *s, int withGrad)
 {
     OptState &o = opt(s);
     DevLevel &l0 = s->L[0];
+    if (s->super) {      // one CTA per element: the objective is summed from ce afterwards
+        sensitivity_super_kernel<<<(unsigned)l0.Ne, 64, 0, s->st>>>(
+            s->Imat, l0.KsC, o.U, 3 * l0.g.cs, s->nLoads, s->weights, l0.eleGrid, l0.g, o.xPhys,
+            s->p.E0, s->p.Emin, s->p.penal, withGrad ? o.cSolid : 0.0, o.ce, withGrad ? o.dc : nullptr, o.dv,
+            Reduce{nullptr, nullptr, nullptr});
+        TOPGPU_COUNT_LAUNCH();
+        sum_scaled_kernel<<<vb(l0.Ne), 256, 0, s->st>>>(o.ce, l0.Ne, withGrad && o.cSolid > 0 ? 1.0 / o.cSolid : 1.0,
+                                                        s->red(&o.sc->cObj));
+        TOPGPU_COUNT_LAUNCH();
+        CK(cudaGetLastError());
+        return TOP_OK;
+    }
     sensitivity_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(
         s->Ke64, o.U, 3 * l0.g.cs, s->nLoads, s->weights, l0.eleGrid, l0.Ne, l0.g, o.xPhys, s->Ec,
         s->p.E0, s->p.Emin, s->p.penal, withGrad ? o.cSolid : 0.0, o.ce, withGrad ? o.dc : nullptr, o.dv,
@@ -513,13 +728,18 @@ extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, do
     if (!s || !prm || prm->nLoop < 0 || !(prm->V0 > 0) || (prm->ft != 0 && prm->ft != 1 && prm->ft != 2)) {
         set_error("top_solver_opt_begin: bad arguments"); return TOP_ERR_ARGS;
     }
+    if (s->super && prm->ft != 2) {      // TOP_GPU.m:113-121: super-element models filter densities
+        set_error("top_solver_opt_begin: super-element models use ft = 2"); return TOP_ERR_ARGS;
+    }
     ensure_state(s);
     OptState &o = opt(s);
     DevLevel &l0 = s->L[0];
     const int64_t Ne = l0.Ne, cs = l0.g.cs;
+    const int64_t nv = Ne * (s->super ? 64 : 1);
+    o.nv = nv;
     if (!o.xd) {
-        o.xd = s->dalloc<double>(Ne); o.xPhys = s->dalloc<double>(Ne); o.xnew = s->dalloc<double>(Ne);
-        o.dc = s->dalloc<double>(Ne); o.dv = s->dalloc<double>(Ne); o.ce = s->dalloc<double>(Ne); o.tmp = s->dalloc<double>(Ne);
+        o.xd = s->dalloc<double>(nv); o.xPhys = s->dalloc<double>(nv); o.xnew = s->dalloc<double>(nv);
+        o.dc = s->dalloc<double>(nv); o.dv = s->dalloc<double>(nv); o.ce = s->dalloc<double>(Ne); o.tmp = s->dalloc<double>(nv);
         o.U = s->galloc<double>(cs, 3 * s->nLoads);
         o.sc = s->dalloc<OptScalars>(1);
         if (cudaMallocHost(&o.hsc, sizeof(OptScalars)) != cudaSuccess) o.hsc = nullptr;
@@ -527,16 +747,17 @@ extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, do
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, oc_kernel, 256, 0);
-        o.ocBlocks = std::max(1, std::min<int>(nsm * std::max(1, perSM), (int)((Ne + 255) / 256)));
+        o.ocBlocks = std::max(1, std::min<int>(nsm * std::max(1, perSM), (int)((nv + 255) / 256)));
         o.ocPartials = s->dalloc<double>(o.ocBlocks);
         if (!o.xd || !o.xPhys || !o.xnew || !o.dc || !o.dv || !o.ce || !o.tmp || !o.U || !o.sc || !o.hsc || !o.ocPartials) {
             set_error("top_solver_opt_begin: out of memory"); return TOP_ERR_NOMEM;
         }
     }
     o.prm = *prm;
-    if (prm->ft != 0) { const int rc = top_solver_filter_setup(s, prm->rMin); if (rc) return rc; }
+    if (s->super) { const int rc = sfilter_setup(s, prm->rMin); if (rc) return rc; }
+    else if (prm->ft != 0) { const int rc = top_solver_filter_setup(s, prm->rMin); if (rc) return rc; }
     // fully solid solve and its compliance (TOP_GPU.m:142-165)
-    fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.tmp, s->p.E0, Ne);
+    fill_kernel<<<vb(nv), 256, 0, s->st>>>(o.tmp, s->p.E0, nv);
     TOPGPU_COUNT_LAUNCH();
     int rc = set_modulus_dev(s, o.tmp, 1, 0);
     if (rc) return rc;
@@ -550,10 +771,10 @@ extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, do
     if (rc) return rc;
     CK(cudaMemcpyAsync(o.hsc, o.sc, sizeof(OptScalars), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
-    o.cSolid = o.hsc->cObj;       // cSolid = E0 * sum(ceList) with E = E0
-    fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.xd, prm->V0, Ne);
+    o.cSolid = o.hsc->cObj;       // cSolid = E0 * sum(ceList) with E = E0 (super: sum(ceList))
+    fill_kernel<<<vb(nv), 256, 0, s->st>>>(o.xd, prm->V0, nv);
     TOPGPU_COUNT_LAUNCH();
-    fill_kernel<<<vb(Ne), 256, 0, s->st>>>(o.xPhys, prm->V0, Ne);
+    fill_kernel<<<vb(nv), 256, 0, s->st>>>(o.xPhys, prm->V0, nv);
     TOPGPU_COUNT_LAUNCH();
     CK(cudaGetLastError());
     o.loop = 0; o.change = 1.0; o.sharp = 1.0;
@@ -566,8 +787,7 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
 {
     if (!s || !s->optState || !opt(s).begun) { set_error("top_solver_opt_step: call top_solver_opt_begin first"); return TOP_ERR_STATE; }
     OptState &o = opt(s);
-    DevLevel &l0 = s->L[0];
-    const int64_t Ne = l0.Ne;
+    const int64_t Ne = o.nv;           // design variables (64 per super-element)
     cudaStream_t st = s->st;
     const int VB = vb(Ne);
     cudaEvent_t ev[7];
@@ -598,6 +818,12 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
         if (rc) return rc;
         div_floor_kernel<<<VB, 256, 0, st>>>(o.dc, o.xd, o.dc, Ne);
         TOPGPU_COUNT_LAUNCH();
+    } else if (o.prm.ft == 2 && s->super) {   // dc = imfilter(dc./Hs, h), dv likewise (TOP_GPU.m:221-227)
+        rc = sfilter_apply(s, o.dc, o.tmp, 0);
+        if (!rc) { copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dc, Ne); TOPGPU_COUNT_LAUNCH(); rc = sfilter_apply(s, o.dv, o.tmp, 0); }
+        if (rc) return rc;
+        copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dv, Ne);
+        TOPGPU_COUNT_LAUNCH();
     } else if (o.prm.ft == 2) {
         rc = filter_apply(s, o.dc, o.tmp, &fits);
         if (!rc) { copy_kernel<<<VB, 256, 0, st>>>(o.tmp, o.dc, Ne); TOPGPU_COUNT_LAUNCH(); rc = filter_apply(s, o.dv, o.tmp, &fits); }
@@ -624,7 +850,8 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
     }
     CK(cudaEventRecord(ev[5], st));
     // xPhys (TOP_GPU.m:256-267): the new design, or its PDE-filtered version
-    if (o.prm.ft == 2) { rc = filter_apply(s, o.xd, o.xPhys, &fits); if (rc) return rc; }
+    if (o.prm.ft == 2 && s->super) { rc = sfilter_apply(s, o.xd, o.xPhys, 1); if (rc) return rc; }   // 262-265
+    else if (o.prm.ft == 2) { rc = filter_apply(s, o.xd, o.xPhys, &fits); if (rc) return rc; }
     else { copy_kernel<<<VB, 256, 0, st>>>(o.xd, o.xPhys, Ne); TOPGPU_COUNT_LAUNCH(); }
     sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 1, s->red(&o.sc->sharp));
     TOPGPU_COUNT_LAUNCH();
@@ -669,7 +896,7 @@ extern "C" int top_solver_get_design(top_solver *s, double *xPhys, double *x)
 {
     if (!s || !s->optState || !opt(s).begun) return TOP_ERR_STATE;
     OptState &o = opt(s);
-    const int64_t Ne = s->L[0].Ne;
+    const int64_t Ne = o.nv;
     if (xPhys) CK(cudaMemcpyAsync(xPhys, o.xPhys, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
     if (x) CK(cudaMemcpyAsync(x, o.xd, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -680,7 +907,7 @@ extern "C" int top_solver_set_design(top_solver *s, const double *xPhys, const d
 {
     if (!s || !s->optState || !opt(s).begun) return TOP_ERR_STATE;
     OptState &o = opt(s);
-    const int64_t Ne = s->L[0].Ne;
+    const int64_t Ne = o.nv;
     if (xPhys) CK(cudaMemcpyAsync(o.xPhys, xPhys, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
     if (x) CK(cudaMemcpyAsync(o.xd, x, sizeof(double) * Ne, cudaMemcpyDefault, s->st));
     return TOP_OK;
@@ -786,6 +1013,7 @@ extern "C" int top_solver_sensitivity(top_solver *s, const top_sens_params *prm,
         set_error("top_solver_sensitivity: load case or DOF out of range"); return TOP_ERR_ARGS;
     }
     if (prm->ft < 0 || prm->ft > 2) { set_error("top_solver_sensitivity: ft must be 0, 1 or 2"); return TOP_ERR_ARGS; }
+    if (s->super) { set_error("top_solver_sensitivity: voxel (non-super-element) models only"); return TOP_ERR_ARGS; }
     if (prm->ft != 0 && (!s->filterState || !filt(s).ready)) { set_error("top_solver_sensitivity: call top_solver_filter_setup first"); return TOP_ERR_STATE; }
     if (!s->adjState) s->adjState = new AdjState();
     AdjState &a = adj(s);

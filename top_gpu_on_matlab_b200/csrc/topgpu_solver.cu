@@ -60,6 +60,33 @@ __global__ void modulus_kernel(const double *__restrict__ src, int simp, double 
     Eg[eleGrid[e]] = v;
     Eg32[eleGrid[e]] = float(v);
 }
+// super-element mode: sub-voxel moduli (SIMP when simp != 0), [64 x Ne]
+__global__ void modulus_super_kernel(const double *__restrict__ src, int simp, double E0, double Emin, double p,
+                                     double *__restrict__ Esub, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) Esub[i] = simp ? Emin + pow(src[i], p) * (E0 - Emin) : src[i];
+}
+// K_mat(:, e) = I_mat * E_sub(:, e) (TOP_GPU.m:1101-1104); elements with fixed
+// DOFs: sum_q Kfree(:, q, uid) E_sub(q, e) + Kfixed(:, uid) (TOP_GPU.m:723-734).
+// One CTA per element, one thread per matrix entry.
+__global__ void __launch_bounds__(576)
+super_kmat_kernel(const double *__restrict__ Imat, const double *__restrict__ Esub, const int32_t *__restrict__ mapUnique,
+                  const double *__restrict__ uFree, const double *__restrict__ uFixed, double *__restrict__ Kc)
+{
+    __shared__ double Ee[64];
+    const int64_t e = blockIdx.x;
+    const int t = threadIdx.x;
+    if (t < 64) Ee[t] = Esub[e * 64 + t];
+    __syncthreads();
+    const int32_t u = mapUnique[e];
+    const double *I = u > 0 ? uFree + (size_t)(u - 1) * 576 * 64 : Imat;
+    double acc = 0;
+#pragma unroll 8
+    for (int q = 0; q < 64; ++q) acc = fma(I[(size_t)q * 576 + t], Ee[q], acc);
+    if (u > 0) acc += uFixed[(size_t)(u - 1) * 576 + t];
+    Kc[e * 576 + t] = acc;
+}
 // Level-0 Jacobi diagonal: sum_e E_e diag(Ke) on free components, E0 on
 // fixed ones (the element matrices of TOP_GPU.m:1184-1188 summed per node).
 __global__ void diag_l0_kernel(const KeParam<double> K, const double *__restrict__ E,
@@ -325,8 +352,34 @@ __global__ void compliance_kernel(const KeParam<double> K, const double *__restr
     }
     ce[e] = acc;
 }
-
-
+// super-element mode: ce_e = sum_k w_k u_ke' K_mat_e u_ke (TOP_GPU.m:2622-2645)
+__global__ void compliance_kmat_kernel(const double *__restrict__ Kc, const double *__restrict__ U, int64_t ustride,
+                                       int nLoads, const double *__restrict__ w, const int32_t *__restrict__ eleGrid,
+                                       int64_t Ne, Geom g, double *__restrict__ ce)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Ne) return;
+    const int64_t slot = eleGrid[e];
+    const double *K = Kc + e * 576;
+    double acc = 0;
+    for (int k = 0; k < nLoads; ++k) {
+        const double *u = U + k * ustride;
+        double ue[24];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ue[3 * j + c] = u[c * g.cs + slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j)];
+        double s = 0;
+        for (int a = 0; a < 24; ++a) {
+            double t = 0;
+#pragma unroll
+            for (int b = 0; b < 24; ++b) t = fma(K[a + 24 * b], ue[b], t);
+            s = fma(t, ue[a], s);
+        }
+        acc += s * w[k];
+    }
+    ce[e] = acc;
+}
 
 }  // namespace topgpu
 
@@ -499,7 +552,6 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
 {
     if (!mesh || !p || !out) { set_error("top_solver_create: bad arguments"); return TOP_ERR_ARGS; }
     if (!mesh->hasBC) { set_error("top_solver_create: apply boundary conditions first"); return TOP_ERR_STATE; }
-    if (mesh->superElement) { set_error("top_solver_create: super-element models use top_super_* entry points"); return TOP_ERR_ARGS; }
     if (p->precision != TOP_PREC_FP64 && p->precision != TOP_PREC_MIXED) { set_error("top_solver_create: bad precision"); return TOP_ERR_ARGS; }
     top_solver *s = new (std::nothrow) top_solver();
     if (!s) return TOP_ERR_NOMEM;
@@ -613,8 +665,21 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     s->Eg64 = s->galloc<double>(l0.g.cs, 1);
     s->Eg32 = s->galloc<float>(l0.g.cs, 1);
     s->nU = (int64_t)mesh->eleWithFixedDOFs.size();
+    s->super = mesh->superElement != 0;
+    s->nely = mesh->nely; s->nelx = mesh->nelx; s->nelz = mesh->nelz;
+    const int slices = s->super ? 64 : 1;
     s->mapUnique = s->dalloc<int32_t>(M0.Ne);
-    s->uFree = s->dalloc<double>((size_t)576 * s->nU);
+    s->uFree = s->dalloc<double>((size_t)576 * slices * s->nU);
+    if (s->super) {
+        s->Esub = s->dalloc<double>((size_t)64 * M0.Ne);
+        s->stage = s->dalloc<double>((size_t)64 * M0.Ne);
+        s->Imat = s->dalloc<double>((size_t)576 * 64);
+        l0.KsC = s->dalloc<double>((size_t)M0.Ne * 576);
+        l0.KsP64 = s->galloc<double>(l0.g.cs, 300);
+        l0.KsP32 = s->galloc<float>(l0.g.cs, 300);
+        if (!s->Esub || !s->stage || !s->Imat || !l0.KsC || !l0.KsP64 || !l0.KsP32) return fail("out of device memory");
+        cudaMemcpy(s->Imat, mesh->I_mat.data(), sizeof(double) * 576 * 64, cudaMemcpyHostToDevice);
+    }
     s->uFixed = s->dalloc<double>((size_t)576 * s->nU);
     s->P4 = s->dalloc<double>((size_t)576 * 64);
     s->P2 = s->dalloc<double>((size_t)576 * 8);
@@ -639,7 +704,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         }
     }
     cudaMemcpy(s->mapUnique, mesh->mapUniqueKes.data(), sizeof(int32_t) * M0.Ne, cudaMemcpyHostToDevice);
-    cudaMemcpy(s->uFree, mesh->uniqueKesFree.data(), sizeof(double) * 576 * s->nU, cudaMemcpyHostToDevice);
+    cudaMemcpy(s->uFree, mesh->uniqueKesFree.data(), sizeof(double) * 576 * slices * s->nU, cudaMemcpyHostToDevice);
     {
         std::vector<double> fx(mesh->uniqueKesFixed);
         for (auto &v : fx) v *= p->E0;     // uniqueKesFixed_ * modulus_ (TOP_GPU.m:1614)
@@ -673,8 +738,14 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         }
     }
     // reduction scratch
+    // one partial per CTA of every reducing launch: node grids, coarse tiles,
+    // per-element kernels (256 elements per CTA)
     int64_t maxBlocks = 4096;
-    for (auto &d : s->L) maxBlocks = std::max<int64_t>(maxBlocks, (int64_t)d.g.nbx * d.g.NZ);
+    for (auto &d : s->L) {
+        maxBlocks = std::max<int64_t>(maxBlocks, (int64_t)d.g.nbx * d.g.NZ);
+        maxBlocks = std::max<int64_t>(maxBlocks, (int64_t)coarse_tile_grid(d.g).x * coarse_tile_grid(d.g).y);
+        maxBlocks = std::max<int64_t>(maxBlocks, (d.Ne + 255) / 256 + 1);
+    }
     s->nPartials = maxBlocks;
     s->partials = s->dalloc<double>(maxBlocks);
     s->counter = s->dalloc<unsigned>(4);
@@ -722,7 +793,8 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
             s->numSMs = nsm;
     }
-    // level-0 products in the Walsh basis where Ke allows it
+    // level-0 products in the Walsh basis where Ke allows it (voxel mode)
+    if (s->super) s->walshOK = false;
     if (s->walshOK)
         for (int pslot = 0; pslot < 2; ++pslot)
             if (set_l0_kernel(s, pslot, 3, 16, 8, (pslot ? 16 : 12) * s->numSMs) != TOP_OK) return fail("level-0 kernel setup");
@@ -795,6 +867,17 @@ int topgpu::set_modulus_dev(top_solver *s, const double *src, int where, int sim
     if (!s || !src) return TOP_ERR_ARGS;
     const int64_t Ne = s->L[0].Ne;
     const double *d = src;
+    if (s->super) {      // [64 x Ne] sub-voxel values
+        if (where == 0) {
+            CK(cudaMemcpyAsync(s->stage, src, sizeof(double) * 64 * Ne, cudaMemcpyHostToDevice, s->st));
+            d = s->stage;
+        }
+        modulus_super_kernel<<<nb256(64 * Ne), 256, 0, s->st>>>(d, simp, s->p.E0, s->p.Emin, s->p.penal, s->Esub, 64 * Ne);
+        TOPGPU_COUNT_LAUNCH();
+        CKL();
+        s->assembled = false;
+        return TOP_OK;
+    }
     if (where == 0) {
         CK(cudaMemcpyAsync(s->tmp, src, sizeof(double) * Ne, cudaMemcpyHostToDevice, s->st));
         d = s->tmp;
@@ -812,11 +895,23 @@ extern "C" int top_solver_assemble(top_solver *s)
 {
     if (!s) return TOP_ERR_ARGS;
     cudaStream_t st = s->st;
+    DevLevel &l0 = s->L[0];
+    if (s->super) {      // level-0 element matrices, packed copies, diagonal
+        super_kmat_kernel<<<(unsigned)l0.Ne, 576, 0, st>>>(s->Imat, s->Esub, s->mapUnique, s->uFree, s->uFixed, l0.KsC);
+        TOPGPU_COUNT_LAUNCH();
+        pack_ks_kernel<<<(unsigned)((l0.Ne + kPackE - 1) / kPackE), 256, 0, st>>>(l0.KsC, l0.eleGrid, l0.Ne, l0.KsP64, l0.KsP32, l0.g.cs);
+        TOPGPU_COUNT_LAUNCH();
+        diag_coarse_kernel<<<node_grid(l0.g), kNodeThreads, 0, st>>>(l0.KsP64, l0.g, l0.flags, l0.diag, l0.invD64, l0.invD32);
+        TOPGPU_COUNT_LAUNCH();
+    }
     // Galerkin Ks (TOP_GPU.m:1054-1147)
     for (int l = 1; l < s->nL; ++l) {
         DevLevel &d = s->L[l];
         int rc;
-        if (l == 1)
+        if (s->super)    // P_s' K_mat(child) P_s, K_mat with the boundary override (superEle_inplace.cu:70-173)
+            rc = assemble_higher_f64(d.KsC, d.upMap, s->L[l - 1].KsC, d.span == 4 ? s->P4 : s->P2, d.Ne,
+                                     d.span * d.span * d.span, st);
+        else if (l == 1)
             rc = assemble_level2_f64(d.KsC, d.upMap, s->Ec, s->KeDev, s->P4, s->mapUnique, s->uFree, s->uFixed,
                                      d.Ne, 64, s->nU, s->Qs, s->eye, st, s->bndList, s->nBnd);
         else
@@ -829,9 +924,10 @@ extern "C" int top_solver_assemble(top_solver *s)
             TOPGPU_COUNT_LAUNCH();
         }
     }
-    DevLevel &l0 = s->L[0];
-    diag_l0_kernel<<<node_grid(l0.g), kNodeThreads, 0, st>>>(s->Ke64, s->Eg64, l0.flags, l0.g, s->p.E0, l0.diag, l0.invD64, l0.invD32);
-    TOPGPU_COUNT_LAUNCH();
+    if (!s->super) {
+        diag_l0_kernel<<<node_grid(l0.g), kNodeThreads, 0, st>>>(s->Ke64, s->Eg64, l0.flags, l0.g, s->p.E0, l0.diag, l0.invD64, l0.invD32);
+        TOPGPU_COUNT_LAUNCH();
+    }
     CKL();
     // coarsest matrix, Cholesky, inverse (TOP_GPU.m:1240-1255)
     DevLevel &lc = s->L[s->nL - 1];
@@ -960,7 +1056,7 @@ extern "C" int top_solver_get_diag(top_solver *s, int level, double *diag)
 
 extern "C" int top_solver_get_ks(top_solver *s, int level, double *Ks)
 {
-    if (!s || !Ks || level < 1 || level >= s->nL) return TOP_ERR_ARGS;
+    if (!s || !Ks || level < (s->super ? 0 : 1) || level >= s->nL) return TOP_ERR_ARGS;   // super: level 0 = K_mat
     if (!s->assembled) { set_error("top_solver_get_ks: assemble first"); return TOP_ERR_STATE; }
     DevLevel &d = s->L[level];
     CK(cudaMemcpyAsync(Ks, d.KsC, sizeof(double) * 576 * d.Ne, cudaMemcpyDeviceToDevice, s->st));
@@ -1152,7 +1248,10 @@ extern "C" int top_solver_unit_compliance(top_solver *s, const double *U, double
     CK(cudaMemsetAsync(Ug - kMargin, 0, sizeof(double) * 3 * cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U, Ug, l0.nodeGrid, l0.Nn, cs);
     TOPGPU_COUNT_LAUNCH();
-    compliance_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(s->Ke64, Ug, 3 * cs, 1, s->weights, l0.eleGrid, l0.Ne, l0.g, ce);
+    if (s->super)
+        compliance_kmat_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(l0.KsC, Ug, 3 * cs, 1, s->weights, l0.eleGrid, l0.Ne, l0.g, ce);
+    else
+        compliance_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(s->Ke64, Ug, 3 * cs, 1, s->weights, l0.eleGrid, l0.Ne, l0.g, ce);
     TOPGPU_COUNT_LAUNCH();
     CKL();
     CK(cudaStreamSynchronize(s->st));

@@ -80,6 +80,13 @@ struct top_solver {
     int64_t nC = 0; double *Ac = nullptr, *Ainv = nullptr, *Wc = nullptr, *cr = nullptr;
     int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
     bool assembled = false;
+    // super-element mode (TOP_GPU.m:1101-1104, 721-741): level-0 elements are
+    // 4x4x4 sub-voxel blocks with per-element K_mat = I_mat * E_sub
+    bool super = false;
+    double *Esub = nullptr;          // [64 x Ne] sub-voxel moduli
+    double *Imat = nullptr;          // [576 x 64]
+    double *stage = nullptr;         // host-upload staging for [64 x Ne] vectors
+    int nely = 0, nelx = 0, nelz = 0;   // the model's voxel (super-element) counts
     int64_t launches = 0;            // kernels launched by this solver (all entry points)
     void *filterState = nullptr, *optState = nullptr, *adjState = nullptr;   // topgpu_opt.cu
     std::vector<double> Fhost; int64_t nd0 = 0;

@@ -136,12 +136,17 @@ class Solver:
             raise ValueError("expected %d entries, got %d" % (n, t.numel()))
         return t
 
+    @property
+    def num_design(self):
+        """Design variables: one per element, 64 per super-element (sub-voxels)."""
+        return self.levels[0]["numElements"] * (64 if self.mesh.super_element else 1)
+
     def set_modulus(self, E):
-        E = self._dev(E, self.levels[0]["numElements"])
+        E = self._dev(E, self.num_design)
         check(lib().top_solver_set_modulus(self._h, E.data_ptr(), 1), "top_solver_set_modulus")
 
     def set_density(self, x):
-        x = self._dev(x, self.levels[0]["numElements"])
+        x = self._dev(x, self.num_design)
         check(lib().top_solver_set_density(self._h, x.data_ptr(), 1), "top_solver_set_density")
 
     def assemble(self):
@@ -238,7 +243,7 @@ class Solver:
         return loop.value, ch.value, sh.value
 
     def design(self):
-        ne = self.levels[0]["numElements"]
+        ne = self.num_design
         xp = torch.zeros(ne, dtype=torch.float64, device="cuda")
         x = torch.zeros(ne, dtype=torch.float64, device="cuda")
         check(lib().top_solver_get_design(self._h, xp.data_ptr(), x.data_ptr()), "top_solver_get_design")
@@ -246,7 +251,7 @@ class Solver:
 
     def set_design(self, xPhys=None, x=None):
         """Replace the design the next opt_step starts from (device or pinned/pageable host tensors)."""
-        ne = self.levels[0]["numElements"]
+        ne = self.num_design
         ptrs = []
         for v in (xPhys, x):
             if v is None:
@@ -291,6 +296,17 @@ class Solver:
                                            C.byref(J), C.byref(its)), "top_solver_sensitivity")
         return out, J.value, its.value
 
+    def super_filter_setup(self, rMin):
+        check(lib().top_solver_super_filter_setup(self._h, rMin), "top_solver_super_filter_setup")
+
+    def super_filter(self, src, mode):
+        """Super-element density filter on [64 x Ne] vectors: mode 0 = imfilter(src./Hs, h),
+        1 = imfilter(src, h)./Hs."""
+        src = self._dev(src, self.num_design)
+        out = torch.empty_like(src)
+        check(lib().top_solver_super_filter(self._h, src.data_ptr(), out.data_ptr(), mode), "top_solver_super_filter")
+        return out
+
     def set_graphs(self, on):
         """Run PCG iterations as captured CUDA graphs (default) or launch by launch."""
         check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
@@ -315,7 +331,7 @@ class Solver:
         prm = OptParams(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
         hist = (OptRecord * max(1, nLoop))()
         n, cs = C.c_int(0), C.c_double(0)
-        xp = torch.zeros(self.levels[0]["numElements"], dtype=torch.float64, device="cuda")
+        xp = torch.zeros(self.num_design, dtype=torch.float64, device="cuda")
         check(lib().top_solver_optimize(self._h, C.byref(prm), xp.data_ptr(), hist, C.byref(n), C.byref(cs)),
               "top_solver_optimize")
         rows = [{k: getattr(hist[i], k) for k, _ in OptRecord._fields_} for i in range(n.value)]
