@@ -200,6 +200,13 @@ int top_solver_get_ks(top_solver *s, int level, double *Ks);
  * interleaved) is the warm start when warm = 1 and receives the solution.
  * its / relres may be NULL.  Returns TOP_ERR_NOT_CONVERGED at maxIT. */
 int top_solver_pcg(top_solver *s, int loadCase, double *U, int warm, int *its, double *relres);
+/* All load cases at once (the state solves of TOP_GPU.m:181-187): one PCG
+ * over the nLoads right-hand sides, every operator launched once per
+ * iteration for all of them, each with its own recurrence and stopping test
+ * (the iterates equal those of top_solver_pcg per load case).  U device
+ * [3Nn x nLoads] (warm start when warm != 0); its / relres arrays of nLoads
+ * (may be NULL).  No single counterpart in the reference (it loops). */
+int top_solver_pcg_all(top_solver *s, double *U, int warm, int *its, double *relres);
 /* Same on an explicit right-hand side b (device, compact interleaved). */
 int top_solver_pcg_rhs(top_solver *s, const double *b, double *U, int warm, int *its, double *relres);
 

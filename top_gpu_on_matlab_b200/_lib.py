@@ -98,6 +98,7 @@ SIGNATURES = {
     "top_solver_get_ks": (_int, [_vp, _int, _vp]),
     "top_solver_pcg": (_int, [_vp, _int, _vp, _int, _vp, _vp]),
     "top_solver_pcg_rhs": (_int, [_vp, _vp, _vp, _int, _vp, _vp]),
+    "top_solver_pcg_all": (_int, [_vp, _vp, _int, _vp, _vp]),
     "top_solver_unit_compliance": (_int, [_vp, _vp, _vp]),
     "top_solver_sizes": (_int, [_vp, _vp]),
     "top_solver_time_kernel": (_int, [_vp, _int, _int, _i64, _vp]),

@@ -48,7 +48,18 @@ template <typename T> struct KeParam { T k[576]; };
 // Deterministic grid-wide sum: per-block partials, the last block to finish
 // adds them in index order and writes *result.
 template <int NT>
+__device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result,
+                                             unsigned nb, unsigned bid);
+template <int NT>
 __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result)
+{
+    block_sum_to<NT>(v, partials, counter, result, gridDim.x * gridDim.y * gridDim.z,
+                     blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+}
+// nb CTAs (numbered bid) contribute to this sum -- one vector of a batched launch
+template <int NT>
+__device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result,
+                                             unsigned nb, unsigned bid)
 {
     __shared__ double red[NT / 32];
     __shared__ bool last;
@@ -58,8 +69,6 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
     const int lane = tid & 31, w = tid >> 5;
     if (lane == 0) red[w] = v;
     __syncthreads();
-    const unsigned nb = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if (tid == 0) {
         double s = 0;
         for (int i = 0; i < NT / 32; ++i) s += red[i];
@@ -83,63 +92,98 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
     }
 }
 
+// PCG scalars of one right-hand side; batched solves keep one per vector
+struct PcgState {
+    double normB, rho, rhoOld, pv, rr, resnorm, tol;
+    int its, maxIT, done, status;
+};
+constexpr int kStateInts = int(sizeof(PcgState) / sizeof(int));
+constexpr int kStateDoubles = int(sizeof(PcgState) / sizeof(double));
+static_assert(sizeof(PcgState) % sizeof(double) == 0, "PcgState packs into doubles");
+
 struct Reduce {             // where a fused dot product goes
     double *partials; unsigned *counter; double *result;
+    int64_t pStride = 0;    // batched launches: partials per vector
+    int64_t rStride = 0;    //                   result stride (doubles) per vector
+    __host__ __device__ Reduce at(int k) const
+    {
+        if (k == 0) return *this;
+        return Reduce{partials + k * pStride, counter + k, result ? result + k * rStride : nullptr, pStride, rStride};
+    }
 };
+// per-vector done flag of a batched launch (flags in consecutive PcgState's)
+__device__ __forceinline__ const int *done_of(const int *done, int k) { return done ? done + k * kStateInts : nullptr; }
 
 // ---------------------------------------------------------------------------
 // Inputs of the node kernels: the value of the operand vector at a node.
 // Functors carry one base pointer per component (set on the host), so device
 // code indexes each component with 32-bit in-array offsets.
+// Batched launches (several right-hand sides) keep the vectors of a level at
+// a fixed stride vs (3 CS); shift(k) moves a functor to vector k.
 template <typename P> struct Comp3 {
     P p0, p1, p2;
     Comp3() = default;
     Comp3(P base, int64_t cs) : p0(base), p1(base + cs), p2(base + 2 * cs) {}
     __device__ __forceinline__ P operator[](int c) const { return c == 0 ? p0 : (c == 1 ? p1 : p2); }
+    __device__ __forceinline__ Comp3 shifted(int64_t o) const { Comp3 r = *this; r.p0 += o; r.p1 += o; r.p2 += o; return r; }
 };
 
 template <typename T, typename TV>
 struct VecIn {
-    Comp3<const TV *> u;
-    VecIn(const TV *base, int64_t cs) : u(base, cs) {}
+    Comp3<const TV *> u; int64_t vs;
+    VecIn(const TV *base, int64_t cs, int64_t vstride = 0) : u(base, cs), vs(vstride) {}
+    __device__ __forceinline__ VecIn shift(int k) const { VecIn r = *this; if (k) r.u = u.shifted(k * vs); return r; }
     __device__ __forceinline__ T operator()(int m, int c) const { return T(u[c][m]); }
 };
 // x = omega * invD .* r  (the Jacobi pre-smoothing step, evaluated on the fly)
 template <typename T, typename TR>
 struct JacobiIn {
-    Comp3<const TR *> r; Comp3<const T *> invD; T omega;
-    JacobiIn(const TR *rb, const T *ib, int64_t cs, T om) : r(rb, cs), invD(ib, cs), omega(om) {}
+    Comp3<const TR *> r; Comp3<const T *> invD; T omega; int64_t vs;
+    JacobiIn(const TR *rb, const T *ib, int64_t cs, T om, int64_t vstride = 0) : r(rb, cs), invD(ib, cs), omega(om), vs(vstride) {}
+    __device__ __forceinline__ JacobiIn shift(int k) const { JacobiIn o = *this; if (k) o.r = r.shifted(k * vs); return o; }
     __device__ __forceinline__ T operator()(int m, int c) const { return omega * invD[c][m] * T(r[c][m]); }
 };
 
 // Epilogues: what a node kernel does with y = (K u)(node).
 template <typename T, typename TY>
 struct StoreOut {   // y
-    Comp3<TY *> y;
-    StoreOut(TY *yb, int64_t cs) : y(yb, cs) {}
+    Comp3<TY *> y; int64_t vs;
+    StoreOut(TY *yb, int64_t cs, int64_t vstride = 0) : y(yb, cs), vs(vstride) {}
+    __device__ __forceinline__ StoreOut shift(int k) const { StoreOut o = *this; if (k) o.y = y.shifted(k * vs); return o; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     { for (int c = 0; c < 3; ++c) y[c][i] = TY(yv[c]); (void)dot; }
 };
 template <typename T, typename TU, typename TY>
 struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
-    Comp3<TY *> y; Comp3<const TU *> u;
-    DotStoreOut(TY *yb, const TU *ub, int64_t cs) : y(yb, cs), u(ub, cs) {}
+    Comp3<TY *> y; Comp3<const TU *> u; int64_t vs;
+    DotStoreOut(TY *yb, const TU *ub, int64_t cs, int64_t vstride = 0) : y(yb, cs), u(ub, cs), vs(vstride) {}
+    __device__ __forceinline__ DotStoreOut shift(int k) const
+    { DotStoreOut o = *this; if (k) { o.y = y.shifted(k * vs); o.u = u.shifted(k * vs); } return o; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     { for (int c = 0; c < 3; ++c) { y[c][i] = TY(yv[c]); dot += double(u[c][i]) * double(yv[c]); } }
 };
 template <typename T, typename TR, typename TD>
 struct ResidOut {   // d = r - y
-    Comp3<const TR *> r; Comp3<TD *> d;
-    ResidOut(const TR *rb, TD *db, int64_t cs) : r(rb, cs), d(db, cs) {}
+    Comp3<const TR *> r; Comp3<TD *> d; int64_t vsR, vsD;
+    ResidOut(const TR *rb, TD *db, int64_t cs, int64_t vsr = 0, int64_t vsd = -1)
+        : r(rb, cs), d(db, cs), vsR(vsr), vsD(vsd < 0 ? vsr : vsd) {}
+    __device__ __forceinline__ ResidOut shift(int k) const
+    { ResidOut o = *this; if (k) { o.r = r.shifted(k * vsR); o.d = d.shifted(k * vsD); } return o; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     { for (int c = 0; c < 3; ++c) d[c][i] = TD(T(r[c][i]) - yv[c]); (void)dot; }
 };
 // z = x + omega*invD.*(r - y), optionally dot += z . r  (post-smoothing)
 template <typename T, typename TR, typename TZ>
 struct PostSmoothOut {
-    Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega;
-    PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om)
-        : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om) {}
+    Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega; int64_t vs;
+    PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om, int64_t vstride = 0)
+        : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om), vs(vstride) {}
+    __device__ __forceinline__ PostSmoothOut shift(int k) const
+    {
+        PostSmoothOut o = *this;
+        if (k) { o.x = x.shifted(k * vs); o.r = r.shifted(k * vs); o.z = z.shifted(k * vs); }
+        return o;
+    }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     {
         for (int c = 0; c < 3; ++c) {
@@ -213,10 +257,13 @@ __device__ __forceinline__ void l0_node(const KeParam<T> &K, const In &in, const
 
 template <typename T, class In, class Out>
 __global__ void __launch_bounds__(kNodeThreads)
-l0_kernel(const KeParam<T> K, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
-          const uint8_t *__restrict__ tileFixed, Geom g, T E0, Reduce red, const int *__restrict__ done)
+l0_kernel(const KeParam<T> K, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+          const uint8_t *__restrict__ tileFixed, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    const int vk = blockIdx.z;          // right-hand side of a batched launch
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
     const int q = blockIdx.x * kNodeThreads + threadIdx.x;
     const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
     const bool valid = Y < g.NY && X < g.NX;
@@ -226,7 +273,8 @@ l0_kernel(const KeParam<T> K, In in, Out out, const T *__restrict__ E, const uin
         l0_node<T, true>(K, in, out, E, flags, g, idx, valid, E0, dot);
     else
         l0_node<T, false>(K, in, out, E, flags, g, idx, valid, E0, dot);
-    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
+    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result, gridDim.x * gridDim.y,
+                                               blockIdx.x + gridDim.x * blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -238,9 +286,12 @@ constexpr int kCoarseLanes = 8;
 
 template <typename T, class In, class Out>
 __global__ void __launch_bounds__(kNodeThreads)
-coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, const int *__restrict__ done)
+coarse_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, const int *__restrict__ done0)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
     const int64_t gt = (int64_t)blockIdx.x * kNodeThreads + threadIdx.x;
     const int64_t node = gt / kCoarseLanes;
     const int i = int(gt % kCoarseLanes);
@@ -272,7 +323,7 @@ coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, cons
         for (int c = 0; c < 3; ++c) y[c] += __shfl_down_sync(0xffffffffu, y[c], o, kCoarseLanes);
     double dot = 0.0;
     if (valid && i == 0) out((int)idx, y, dot);
-    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result);
+    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 // Tiled variant: a CTA of 32 x 8 threads covers 32 consecutive node slots of
 // one (x, z) row; thread (n, i) multiplies the three rows of incident element
@@ -282,9 +333,12 @@ coarse_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, cons
 constexpr int kCoarseTileX = 32;
 template <typename T, class In, class Out>
 __global__ void __launch_bounds__(kCoarseTileX * 8)
-coarse_tile_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red, const int *__restrict__ done)
+coarse_tile_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, const int *__restrict__ done0)
 {
+    const int vk = blockIdx.z;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
     __shared__ T part[8][3][kCoarseTileX];
     __shared__ int offs[24 * 24];        // packed-entry offset (entry * CS) of Ks(r, k)
     const int n = threadIdx.x, i = threadIdx.y;
@@ -327,7 +381,8 @@ coarse_tile_kernel(In in, Out out, const T *__restrict__ Ks, Geom g, Reduce red,
         }
         out(idx, s, dot);
     }
-    if (red.result) block_sum_to<kCoarseTileX * 8>(dot, red.partials, red.counter, red.result);
+    if (red.result) block_sum_to<kCoarseTileX * 8>(dot, red.partials, red.counter, red.result, gridDim.x * gridDim.y,
+                                                   blockIdx.x + gridDim.x * blockIdx.y);
 }
 inline dim3 coarse_tile_grid(const Geom &g)
 {
@@ -354,9 +409,12 @@ template <int S> struct RestrictLanes { static constexpr int value = (S >= 4) ? 
 template <typename T, int S>
 __global__ void __launch_bounds__(kNodeThreads)
 restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
-                const uint8_t *__restrict__ flagsC, const int *__restrict__ done)
+                const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsF = 0, int64_t vsC = 0)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    rf += vk * vsF; rc += vk * vsC;
     constexpr int LPN = RestrictLanes<S>::value, W = 2 * S - 1;
     const int64_t gt = (int64_t)blockIdx.x * kNodeThreads + threadIdx.x;
     const int64_t node = gt / LPN;
@@ -408,9 +466,13 @@ inline unsigned restrict_blocks(const Geom &gc)
 // reads runs of consecutive QY.
 template <typename T, int S>
 __global__ void __launch_bounds__(256)
-restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc, const int *__restrict__ done)
+restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc, const int *__restrict__ done0,
+                  int64_t vsF = 0, int64_t vsT = 0)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    rf += vk * vsF; t += vk * vsT;
     const int64_t nt = (int64_t)NYc * gf.NX * gf.NZ;
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nt) return;
@@ -431,9 +493,13 @@ restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc,
 // pass B: fold the x taps, t2[c][QY][QX][Z] = sum_ox w(ox) t[c][QY][S QX + ox][Z]
 template <typename T, int S>
 __global__ void __launch_bounds__(256)
-restrict_x_kernel(const T *__restrict__ t, int NYc, int NXf, int NXc, int NZf, T *__restrict__ t2, const int *__restrict__ done)
+restrict_x_kernel(const T *__restrict__ t, int NYc, int NXf, int NXc, int NZf, T *__restrict__ t2, const int *__restrict__ done0,
+                  int64_t vsT = 0, int64_t vsT2 = 0)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    t += vk * vsT; t2 += vk * vsT2;
     const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf;
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n2) return;
@@ -455,9 +521,12 @@ restrict_x_kernel(const T *__restrict__ t, int NYc, int NXf, int NXc, int NZf, T
 template <typename T, int S>
 __global__ void __launch_bounds__(256)
 restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc,
-                  const uint8_t *__restrict__ flagsC, const int *__restrict__ done)
+                  const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsT2 = 0, int64_t vsC = 0)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    t2 += vk * vsT2; rc += vk * vsC;
     const int NYc = gc.NY, NXc = gc.NX;
     const int64_t nq = (int64_t)NYc * NXc * gc.NZ, n2 = (int64_t)NYc * NXc * NZf;
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -486,9 +555,14 @@ template <typename T, int S, typename TR>
 __global__ void __launch_bounds__(kNodeThreads)
 prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
                const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
-               const T *__restrict__ invD, T omega, const int *__restrict__ done)
+               const T *__restrict__ invD, T omega, const int *__restrict__ done0,
+               int64_t vsC = 0, int64_t vsF = 0, int64_t vsR = 0)
 {
+    const int vk = blockIdx.z;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    xc += vk * vsC; xf += vk * vsF;
+    if (r) r += vk * vsR;
     const int q = blockIdx.x * kNodeThreads + threadIdx.x;
     const int Y = q % gf.PY, X = q / gf.PY, Z = blockIdx.y;
     if (Y >= gf.NY || X >= gf.NX) return;

@@ -62,39 +62,41 @@ unsigned l0w_ctas(const top_solver *s, const top_solver::L0Kernel &k)
 }  // namespace
 
 template <typename T, class In, class Out>
-void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done)
+void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done, int nv)
 {
     DevLevel &lv = s->L[0];
     const top_solver::L0Kernel &k = s->l0k[prec_slot<T>()];
+    const unsigned K = (unsigned)nv;  // right-hand sides (grid y or z)
     if (s->super) {                   // per-element matrices (K_mat), packed on the grid
         const T *Kp;
         if constexpr (sizeof(T) == 8) Kp = lv.KsP64; else Kp = lv.KsP32;
-        coarse_tile_kernel<T, In, Out><<<coarse_tile_grid(lv.g), dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, Kp, lv.g, red, done);
+        dim3 gr = coarse_tile_grid(lv.g); gr.z = K;
+        coarse_tile_kernel<T, In, Out><<<gr, dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, Kp, lv.g, red, done);
     } else if (k.kind == 1) {
-#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                     \
-        if (k.ty == A && k.tx == B)                                                                   \
-            l0w_kernel<T, A, B, In, Out><<<l0w_ctas<T, A, B, In, Out, 1>(s, k), A * B, 0, s->st>>>(   \
+#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
+        if (k.ty == A && k.tx == B)                                                                           \
+            l0w_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 1>(s, k), K), A * B, 0, s->st>>>(  \
                 walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
         TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
     } else if (k.kind == 3) {
-#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                     \
-        if (k.ty == A && k.tx == B)                                                                   \
-            l0d_kernel<T, A, B, In, Out><<<l0w_ctas<T, A, B, In, Out, 3>(s, k), A * B, 0, s->st>>>(   \
+#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
+        if (k.ty == A && k.tx == B)                                                                           \
+            l0d_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 3>(s, k), K), A * B, 0, s->st>>>(  \
                 walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
         TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
     } else if (k.kind == 2) {        // FP32 only: the FP64 pair state does not fit in registers
         if constexpr (sizeof(T) == 4) {
-#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                     \
-            if (k.ty == A && k.tx == B)                                                               \
-                l0p_kernel<T, A, B, In, Out><<<l0w_ctas<T, A, B, In, Out, 2>(s, k), A * B, 0, s->st>>>( \
+#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
+            if (k.ty == A && k.tx == B)                                                                       \
+                l0p_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 2>(s, k), K), A * B, 0, s->st>>>( \
                     walshpair<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
             TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
         }
     } else {
-        l0_kernel<T, In, Out><<<dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ), kNodeThreads, 0, s->st>>>(
+        l0_kernel<T, In, Out><<<dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ, K), kNodeThreads, 0, s->st>>>(
             keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
     }
     TOPGPU_COUNT_LAUNCH();
@@ -107,8 +109,8 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
     if ((kind != 1 && kind != 3 && !(kind == 2 && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0) return TOP_ERR_ARGS;
     DevLevel &l0 = s->L[0];
     const int tiles = tiles_of(l0.g, kind, ty, tx);
-    if (ctas > s->nPartials) {                         // one reduction partial per CTA
-        double *pp = s->dalloc<double>((size_t)ctas);
+    if (ctas > s->nPartials) {                         // one reduction partial per CTA and right-hand side
+        double *pp = s->dalloc<double>((size_t)ctas * s->kMax);
         if (!pp) return TOP_ERR_NOMEM;
         s->partials = pp; s->nPartials = ctas;
     }
@@ -141,8 +143,8 @@ double time_l0(top_solver *s, int p, int nrep, void *flush, size_t flushBytes, c
     for (int k = 0; k < nrep + 1; ++k) {
         if (flush) cudaMemsetAsync(flush, k & 0xff, flushBytes, s->st);
         cudaEventRecord(a, s->st);
-        if (p == 0) l0_op<double>(s, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr);
-        else l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr);
+        if (p == 0) l0_op<double>(s, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr, 1);
+        else l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr, 1);
         cudaEventRecord(b, s->st);
         if (cudaEventSynchronize(b) != cudaSuccess) return -1.0;
         float ms = 0.f;
@@ -193,16 +195,16 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
 // the operand / epilogue pairs of the solver's level-0 products
 using VIdd = VecIn<double, double>;  using VIff = VecIn<float, float>;  using VIfd = VecIn<float, double>;
 using JIdd = JacobiIn<double, double>; using JIfd = JacobiIn<float, double>;
-template void l0_op<double, VIdd, StoreOut<double, double>>(top_solver *, const VIdd &, const StoreOut<double, double> &, Reduce, const int *);
-template void l0_op<double, JIdd, ResidOut<double, double, double>>(top_solver *, const JIdd &, const ResidOut<double, double, double> &, Reduce, const int *);
-template void l0_op<double, VIdd, PostSmoothOut<double, double, double>>(top_solver *, const VIdd &, const PostSmoothOut<double, double, double> &, Reduce, const int *);
-template void l0_op<double, VIdd, DotStoreOut<double, double, double>>(top_solver *, const VIdd &, const DotStoreOut<double, double, double> &, Reduce, const int *);
-template void l0_op<double, VIdd, ResidOut<double, double, double>>(top_solver *, const VIdd &, const ResidOut<double, double, double> &, Reduce, const int *);
-template void l0_op<float, JIfd, ResidOut<float, double, float>>(top_solver *, const JIfd &, const ResidOut<float, double, float> &, Reduce, const int *);
-template void l0_op<float, VIff, PostSmoothOut<float, double, double>>(top_solver *, const VIff &, const PostSmoothOut<float, double, double> &, Reduce, const int *);
-template void l0_op<float, VIff, PostSmoothOut<float, double, float>>(top_solver *, const VIff &, const PostSmoothOut<float, double, float> &, Reduce, const int *);
-template void l0_op<float, VIfd, DotStoreOut<float, double, double>>(top_solver *, const VIfd &, const DotStoreOut<float, double, double> &, Reduce, const int *);
-template void l0_op<float, VIfd, StoreOut<float, double>>(top_solver *, const VIfd &, const StoreOut<float, double> &, Reduce, const int *);
-template void l0_op<float, VIfd, ResidOut<float, double, double>>(top_solver *, const VIfd &, const ResidOut<float, double, double> &, Reduce, const int *);
-template void l0_op<float, VIff, StoreOut<float, float>>(top_solver *, const VIff &, const StoreOut<float, float> &, Reduce, const int *);
+template void l0_op<double, VIdd, StoreOut<double, double>>(top_solver *, const VIdd &, const StoreOut<double, double> &, Reduce, const int *, int);
+template void l0_op<double, JIdd, ResidOut<double, double, double>>(top_solver *, const JIdd &, const ResidOut<double, double, double> &, Reduce, const int *, int);
+template void l0_op<double, VIdd, PostSmoothOut<double, double, double>>(top_solver *, const VIdd &, const PostSmoothOut<double, double, double> &, Reduce, const int *, int);
+template void l0_op<double, VIdd, DotStoreOut<double, double, double>>(top_solver *, const VIdd &, const DotStoreOut<double, double, double> &, Reduce, const int *, int);
+template void l0_op<double, VIdd, ResidOut<double, double, double>>(top_solver *, const VIdd &, const ResidOut<double, double, double> &, Reduce, const int *, int);
+template void l0_op<float, JIfd, ResidOut<float, double, float>>(top_solver *, const JIfd &, const ResidOut<float, double, float> &, Reduce, const int *, int);
+template void l0_op<float, VIff, PostSmoothOut<float, double, double>>(top_solver *, const VIff &, const PostSmoothOut<float, double, double> &, Reduce, const int *, int);
+template void l0_op<float, VIff, PostSmoothOut<float, double, float>>(top_solver *, const VIff &, const PostSmoothOut<float, double, float> &, Reduce, const int *, int);
+template void l0_op<float, VIfd, DotStoreOut<float, double, double>>(top_solver *, const VIfd &, const DotStoreOut<float, double, double> &, Reduce, const int *, int);
+template void l0_op<float, VIfd, StoreOut<float, double>>(top_solver *, const VIfd &, const StoreOut<float, double> &, Reduce, const int *, int);
+template void l0_op<float, VIfd, ResidOut<float, double, double>>(top_solver *, const VIfd &, const ResidOut<float, double, double> &, Reduce, const int *, int);
+template void l0_op<float, VIff, StoreOut<float, float>>(top_solver *, const VIff &, const StoreOut<float, float> &, Reduce, const int *, int);
 }  // namespace topgpu

@@ -681,19 +681,16 @@ extern "C" int top_solver_super_filter(top_solver *s, const double *src, double 
 }
 
 // ---- the optimisation loop ---------------------------------------------------
+// state solves of all load cases (TOP_GPU.m:181-187) as one batched PCG
 static int solve_all(top_solver *s, int warm, int *itsTotal)
 {
     OptState &o = opt(s);
-    DevLevel &l0 = s->L[0];
-    const int64_t cs = l0.g.cs;
+    std::vector<int> its((size_t)std::max(1, s->nLoads), 0);
+    const int rc = pcg_block(s, s->b, o.U, s->nLoads, warm, its.data(), nullptr);
+    if (rc != TOP_OK && rc != TOP_ERR_NOT_CONVERGED) return rc;
+    if (rc == TOP_ERR_NOT_CONVERGED) std::fprintf(stderr, "Warning: Exceed the maximum iterate numbers\n");
     int tot = 0;
-    for (int k = 0; k < s->nLoads; ++k) {
-        int its = 0;
-        const int rc = pcg_grid(s, s->b + (size_t)k * 3 * cs, o.U + (size_t)k * 3 * cs, warm, &its, nullptr);
-        tot += its;
-        if (rc != TOP_OK && rc != TOP_ERR_NOT_CONVERGED) return rc;
-        if (rc == TOP_ERR_NOT_CONVERGED) std::fprintf(stderr, "Warning: Exceed the maximum iterate numbers\n");
-    }
+    for (int k = 0; k < s->nLoads; ++k) tot += its[k];
     if (itsTotal) *itsTotal = tot;
     return TOP_OK;
 }

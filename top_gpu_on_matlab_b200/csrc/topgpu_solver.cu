@@ -259,9 +259,12 @@ __global__ void inv_gram_kernel(const double *__restrict__ W, double *__restrict
 // coarsest solve: x_grid = Ainv * r (r gathered from the grid in compact order)
 template <typename T>
 __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const int32_t *__restrict__ nodeGrid,
-                                       int64_t Nn, double *__restrict__ cr, const int *__restrict__ done)
+                                       int64_t Nn, double *__restrict__ cr, const int *__restrict__ done0, int64_t vs)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    r += vk * vs; cr += vk * 3 * Nn;
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 3 * Nn) return;
     cr[t] = double(r[(t % 3) * g.cs + nodeGrid[t / 3]]);
@@ -269,9 +272,12 @@ __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const in
 template <typename T>
 __global__ void coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__ cr, int64_t n,
                                      T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
-                                     const int *__restrict__ done)
+                                     const int *__restrict__ done0, int64_t vs)
 {
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    cr += vk * n; x += vk * vs;
     const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
@@ -285,9 +291,13 @@ __global__ void coarsest_gemv_kernel(const double *__restrict__ Ainv, const doub
 // PCG vector kernels run over whole grid vectors, margins and guard slots
 // included (all zero), as one contiguous range of n = 3 CS values
 __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                                  const double *__restrict__ v, int64_t n, PcgState *st, Reduce red)
+                                  const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0)
 {
+    const int vk = blockIdx.y;           // right-hand side; vectors at stride n
+    st += vk;
     if (st->done) return;
+    x += vk * n; r += vk * n; p += vk * n; v += vk * n;
+    const Reduce red = red0.at(vk);
     const double lambda = st->rho / st->pv;
     double rr = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -296,10 +306,12 @@ __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r
         r[i] = rv;
         rr += rv * rv;
     }
-    block_sum_to<256>(rr, red.partials, red.counter, red.result);
+    block_sum_to<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
-__global__ void pcg_check_kernel(PcgState *st)
-{   // TOP_GPU.m:630-649
+__global__ void pcg_check_kernel(PcgState *st, int nv)
+{   // TOP_GPU.m:630-649, one thread per right-hand side
+    if ((int)threadIdx.x >= nv) return;
+    st += threadIdx.x;
     if (st->done) return;
     st->its += 1;
     const double res = sqrt(st->rr) / st->normB;
@@ -312,17 +324,23 @@ __global__ void pcg_check_kernel(PcgState *st)
 template <typename TZ>
 __global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, int64_t n, const PcgState *st, int first)
 {
+    const int vk = blockIdx.y;
+    st += vk;
     if (!first && st->done) return;
+    p += vk * n; z += vk * n;
     const double beta = first ? 0.0 : st->rho / st->rhoOld;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = double(z[i]) + beta * p[i];
 }
-__global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t n, Reduce red)
+__global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t n, Reduce red0)
 {
+    const int vk = blockIdx.y;
+    a += vk * n; b += vk * n;
+    const Reduce red = red0.at(vk);
     double s = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         s += a[i] * b[i];
-    block_sum_to<256>(s, red.partials, red.counter, red.result);
+    block_sum_to<256>(s, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 // element energies sum_k w_k u_k' Ke u_k (TOP_GPU.m:580-600) on grid vectors
 __global__ void compliance_kernel(const KeParam<double> K, const double *__restrict__ U, int64_t ustride,
@@ -436,36 +454,45 @@ template <typename T> const T *egrid(const top_solver *s);
 template <> const double *egrid<double>(const top_solver *s) { return s->Eg64; }
 template <> const float *egrid<float>(const top_solver *s) { return s->Eg32; }
 
-// y-epilogue applied to (K_level in)(node) for every node of a coarse level
+// y-epilogue applied to (K_level in)(node) for every node of a coarse level;
+// nv right-hand sides in one launch (vectors at the functors' strides)
 template <typename T, class In, class Out>
-void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done)
+void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done, int nv = 1)
 {
     DevLevel &lv = s->L[l];
-    if (s->coarseLanes)
-        coarse_kernel<T, In, Out><<<coarse_blocks(lv.g), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
-    else
-        coarse_tile_kernel<T, In, Out><<<coarse_tile_grid(lv.g), dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    if (s->coarseLanes) {
+        coarse_kernel<T, In, Out><<<dim3(coarse_blocks(lv.g), (unsigned)nv), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    } else {
+        dim3 gr = coarse_tile_grid(lv.g); gr.z = (unsigned)nv;
+        coarse_tile_kernel<T, In, Out><<<gr, dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+    }
     TOPGPU_COUNT_LAUNCH();
 }
 template <typename T> T *rscratch(top_solver *s);
 template <> double *rscratch<double>(top_solver *s) { return s->rscr64; }
 template <> float *rscratch<float>(top_solver *s) { return s->rscr32; }
-// restriction of the level-l residual d onto level l+1 (TOP_GPU.m:817-847)
+// level vectors (r, x, t of each level) hold kMax right-hand sides at stride 3 CS
+inline int64_t lvs(const DevLevel &l) { return 3 * l.g.cs; }
+// restriction of the level-l residual d onto level l+1 (TOP_GPU.m:817-847);
+// d and rc at the level vector strides
 template <typename T>
-void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done)
+void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int nv = 1)
 {
     DevLevel &lv = s->L[l], &lc = s->L[l + 1];
+    const unsigned K = (unsigned)nv;
     if (lc.span == 4) {
         const int NYc = lc.g.NY, NXf = lv.g.NX, NXc = lc.g.NX, NZf = lv.g.NZ;
         const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf, nq = (int64_t)NYc * NXc * lc.g.NZ;
+        const int64_t vsS = 3 * (nt + n2);          // scratch per right-hand side
         T *t1 = rscratch<T>(s), *t2 = t1 + 3 * nt;
-        restrict_y_kernel<T, 4><<<(unsigned)((nt + 255) / 256), 256, 0, s->st>>>(d, lv.g, t1, NYc, done);
+        restrict_y_kernel<T, 4><<<dim3((unsigned)((nt + 255) / 256), K), 256, 0, s->st>>>(d, lv.g, t1, NYc, done, lvs(lv), vsS);
         TOPGPU_COUNT_LAUNCH();
-        restrict_x_kernel<T, 4><<<(unsigned)((n2 + 255) / 256), 256, 0, s->st>>>(t1, NYc, NXf, NXc, NZf, t2, done);
+        restrict_x_kernel<T, 4><<<dim3((unsigned)((n2 + 255) / 256), K), 256, 0, s->st>>>(t1, NYc, NXf, NXc, NZf, t2, done, vsS, vsS);
         TOPGPU_COUNT_LAUNCH();
-        restrict_z_kernel<T, 4><<<(unsigned)((nq + 255) / 256), 256, 0, s->st>>>(t2, NZf, rc, lc.g, lc.flags, done);
+        restrict_z_kernel<T, 4><<<dim3((unsigned)((nq + 255) / 256), K), 256, 0, s->st>>>(t2, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc));
     } else {
-        restrict_kernel<T, 2><<<restrict_blocks<2>(lc.g), kNodeThreads, 0, s->st>>>(d, lv.g, rc, lc.g, lc.flags, done);
+        restrict_kernel<T, 2><<<dim3(restrict_blocks<2>(lc.g), K), kNodeThreads, 0, s->st>>>(d, lv.g, rc, lc.g, lc.flags, done,
+                                                                                           lvs(lv), lvs(lc));
     }
     TOPGPU_COUNT_LAUNCH();
 }
@@ -478,51 +505,60 @@ void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, co
 }
 
 // V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
-// residual r0 (type TR, grid layout); writes z0 (type TZ) and, when zr is
-// set, z0 . r0 into *zr.
+// residuals r0 (type TR, grid layout, nv right-hand sides at stride vs0);
+// writes z0 (type TZ, same stride) and, when zr is set, z0 . r0 into zr
+// (per right-hand side: consecutive PcgState's when nv > 1).
 template <typename T, typename TR, typename TZ>
-void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done)
+void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, int nv = 1, int64_t vs0 = 0)
 {
     const int nL = s->nL;
     const T omega = T(s->p.omega);
     const Reduce none{nullptr, nullptr, nullptr};
+    const unsigned K = (unsigned)nv;
     // restriction leg
     for (int l = 0; l < nL - 1; ++l) {
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
+        const int64_t vs = lvs(lv);
         if (l == 0)
-            l0_op<T>(s, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega}, ResidOut<T, TR, T>{r0, d, lv.g.cs}, none, done);
+            l0_op<T>(s, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega, vs0}, ResidOut<T, TR, T>{r0, d, lv.g.cs, vs0, vs},
+                     none, done, nv);
         else
-            coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs}, none, done);
-        restrict_op<T>(s, l, d, vr<T>(lc), done);
+            coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega, vs}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs, vs},
+                         none, done, nv);
+        restrict_op<T>(s, l, d, vr<T>(lc), done, nv);
     }
     // coarsest direct solve, FP64
     DevLevel &lc = s->L[nL - 1];
     const int64_t n = 3 * lc.Nn;
-    coarsest_gather_kernel<T><<<nb256(n), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done);
+    coarsest_gather_kernel<T><<<dim3(nb256(n), K), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
     TOPGPU_COUNT_LAUNCH();
-    coarsest_gemv_kernel<T><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g, lc.nodeGrid, done);
+    coarsest_gemv_kernel<T><<<dim3((unsigned)((n * 32 + 255) / 256), K), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
+                                                                                            lc.nodeGrid, done, lvs(lc));
     TOPGPU_COUNT_LAUNCH();
     // interpolation leg
     for (int l = nL - 2; l >= 0; --l) {
         DevLevel &lv = s->L[l], &lcn = s->L[l + 1];
         const T *xc = vt<T>(lcn);
         T *x = vx<T>(lv);
+        const int64_t vs = lvs(lv), vsc = lvs(lcn);
+        dim3 gr = node_grid(lv.g); gr.z = K;
         if (l == 0) {
             if (lcn.span == 4)
-                prolong_kernel<T, 4, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
+                prolong_kernel<T, 4, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
             else
-                prolong_kernel<T, 2, TR><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done);
+                prolong_kernel<T, 2, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
             TOPGPU_COUNT_LAUNCH();
-            l0_op<T>(s, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega},
-                        zr ? s->red(zr) : none, done);
+            const Reduce rz = zr ? (nv > 1 ? s->redk(zr) : s->red(zr)) : none;
+            l0_op<T>(s, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega, vs0}, rz, done, nv);
         } else {
             if (lcn.span == 4)
-                prolong_kernel<T, 4, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
+                prolong_kernel<T, 4, T><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             else
-                prolong_kernel<T, 2, T><<<node_grid(lv.g), kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done);
+                prolong_kernel<T, 2, T><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             TOPGPU_COUNT_LAUNCH();
-            coarse_op<T>(s, l, VecIn<T, T>{x, lv.g.cs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega}, none, done);
+            coarse_op<T>(s, l, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega, vs},
+                         none, done, nv);
         }
     }
 }
@@ -533,16 +569,17 @@ void precond(top_solver *s, const double *r0, double *z0, double *zr, const int 
     else vcycle<double, double, double>(s, r0, z0, zr, done);
 }
 
-// outer operator v = K0 u on FP64 grid vectors, u.v into *uy.  FP64 unless
-// outerFP32 (the reference's mixed mode runs it in single, TOP_GPU.m:683-684).
-void outer_op(top_solver *s, const double *u, double *y, double *uy, const int *done)
+// outer operator v = K0 u on FP64 grid vectors (nv right-hand sides at
+// stride vs), u.v into uy.  FP64 unless outerFP32 (the reference's mixed mode
+// runs it in single, TOP_GPU.m:683-684).
+void outer_op(top_solver *s, const double *u, double *y, double *uy, const int *done, int nv = 1, int64_t vs = 0)
 {
     DevLevel &l0 = s->L[0];
-    const Reduce red = uy ? s->red(uy) : Reduce{nullptr, nullptr, nullptr};
+    const Reduce red = uy ? (nv > 1 ? s->redk(uy) : s->red(uy)) : Reduce{nullptr, nullptr, nullptr};
     if (s->p.outerFP32)
-        l0_op<float>(s, VecIn<float, double>{u, l0.g.cs}, DotStoreOut<float, double, double>{y, u, l0.g.cs}, red, done);
+        l0_op<float>(s, VecIn<float, double>{u, l0.g.cs, vs}, DotStoreOut<float, double, double>{y, u, l0.g.cs, vs}, red, done, nv);
     else
-        l0_op<double>(s, VecIn<double, double>{u, l0.g.cs}, DotStoreOut<double, double, double>{y, u, l0.g.cs}, red, done);
+        l0_op<double>(s, VecIn<double, double>{u, l0.g.cs, vs}, DotStoreOut<double, double, double>{y, u, l0.g.cs, vs}, red, done, nv);
 }
 
 }  // namespace
@@ -558,6 +595,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     s->p = *p;
     s->nL = (int)mesh->L.size();
     s->nLoads = mesh->nLoads;
+    s->kMax = std::max(1, s->nLoads);   // load cases solve as one batched PCG
     s->L.resize(s->nL);
     auto fail = [&](const char *what) { set_error("top_solver_create: %s", what); top_solver_destroy(s); return TOP_ERR_NOMEM; };
     for (int l = 0; l < s->nL; ++l) {
@@ -600,10 +638,11 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         d.diag = s->galloc<double>(cs, 3);
         d.invD64 = s->galloc<double>(cs, 3);
         d.invD32 = s->galloc<float>(cs, 3);
-        d.x64 = s->galloc<double>(cs, 3); d.t64 = s->galloc<double>(cs, 3);
-        d.x32 = s->galloc<float>(cs, 3); d.t32 = s->galloc<float>(cs, 3);
+        const int KM = s->kMax;       // V-cycle vectors of every right-hand side
+        d.x64 = s->galloc<double>(cs, 3 * KM); d.t64 = s->galloc<double>(cs, 3 * KM);
+        d.x32 = s->galloc<float>(cs, 3 * KM); d.t32 = s->galloc<float>(cs, 3 * KM);
         if (l > 0) {
-            d.r64 = s->galloc<double>(cs, 3); d.r32 = s->galloc<float>(cs, 3);
+            d.r64 = s->galloc<double>(cs, 3 * KM); d.r32 = s->galloc<float>(cs, 3 * KM);
             const int nch = M.span * M.span * M.span;
             d.upMap = s->dalloc<int32_t>((size_t)M.Ne * nch);
             d.KsC = s->dalloc<double>((size_t)M.Ne * 576);
@@ -644,8 +683,8 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         for (int l = 0; l + 1 < s->nL; ++l)
             if (s->L[l + 1].span == 4)
                 nt = std::max<int64_t>(nt, (int64_t)s->L[l + 1].g.NY * (s->L[l].g.NX + s->L[l + 1].g.NX) * s->L[l].g.NZ);
-        s->rscr64 = s->dalloc<double>((size_t)3 * nt);
-        s->rscr32 = s->dalloc<float>((size_t)3 * nt);
+        s->rscr64 = s->dalloc<double>((size_t)3 * nt * s->kMax);
+        s->rscr32 = s->dalloc<float>((size_t)3 * nt * s->kMax);
         if (!s->rscr64 || !s->rscr32) return fail("out of device memory");
     }
     // level-0 data
@@ -719,9 +758,10 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     }
     // PCG vectors
     const int64_t cs0 = l0.g.cs;
-    s->x = s->galloc<double>(cs0, 3); s->r = s->galloc<double>(cs0, 3); s->z = s->galloc<double>(cs0, 3);
-    s->z32 = s->galloc<float>(cs0, 3);
-    s->pv = s->galloc<double>(cs0, 3); s->v = s->galloc<double>(cs0, 3); s->tmp = s->galloc<double>(cs0, 3);
+    const int KM = s->kMax;           // PCG vectors of every right-hand side
+    s->x = s->galloc<double>(cs0, 3 * KM); s->r = s->galloc<double>(cs0, 3 * KM); s->z = s->galloc<double>(cs0, 3 * KM);
+    s->z32 = s->galloc<float>(cs0, 3 * KM);
+    s->pv = s->galloc<double>(cs0, 3 * KM); s->v = s->galloc<double>(cs0, 3 * KM); s->tmp = s->galloc<double>(cs0, 3 * KM);
     s->b = s->galloc<double>(cs0, 3 * std::max(1, s->nLoads));
     s->weights = s->dalloc<double>(std::max(1, s->nLoads));
     if (!s->x || !s->r || !s->z || !s->z32 || !s->pv || !s->v || !s->tmp || !s->b || !s->weights) return fail("out of device memory");
@@ -747,12 +787,12 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         maxBlocks = std::max<int64_t>(maxBlocks, (d.Ne + 255) / 256 + 1);
     }
     s->nPartials = maxBlocks;
-    s->partials = s->dalloc<double>(maxBlocks);
-    s->counter = s->dalloc<unsigned>(4);
+    s->partials = s->dalloc<double>(maxBlocks * s->kMax);
+    s->counter = s->dalloc<unsigned>(4 + s->kMax);
     s->scal = s->dalloc<double>(16);
     s->zeroDone = s->dalloc<int>(4);
-    s->state = s->dalloc<PcgState>(1);
-    if (cudaMallocHost(&s->hstate, sizeof(PcgState)) != cudaSuccess) s->hstate = nullptr;
+    s->state = s->dalloc<PcgState>(s->kMax);
+    if (cudaMallocHost(&s->hstate, sizeof(PcgState) * s->kMax) != cudaSuccess) s->hstate = nullptr;
     if (!s->partials || !s->counter || !s->scal || !s->zeroDone || !s->state || !s->hstate) return fail("out of memory");
     // coarsest level maps
     {
@@ -782,7 +822,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         s->Ac = s->dalloc<double>((size_t)s->nC * s->nC);
         s->Ainv = s->dalloc<double>((size_t)s->nC * s->nC);
         s->Wc = s->dalloc<double>((size_t)s->nC * s->nC);
-        s->cr = s->dalloc<double>((size_t)s->nC);
+        s->cr = s->dalloc<double>((size_t)s->nC * s->kMax);
         if (!s->eleCompactC || !s->nodeCompactC || !s->Ac || !s->Ainv || !s->Wc || !s->cr) return fail("out of device memory");
         cudaMemcpy(s->eleCompactC, ec.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
         cudaMemcpy(s->nodeCompactC, nc.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
@@ -1065,8 +1105,10 @@ extern "C" int top_solver_get_ks(top_solver *s, int level, double *Ks)
 }
 
 // ---- PCG (Solving_PCG, TOP_GPU.m:602-667) ---------------------------------
-__global__ void pcg_init_kernel(PcgState *st)
+__global__ void pcg_init_kernel(PcgState *st, int nv)
 {   // ||b|| from the squared norm written by dot_kernel into st->normB
+    if ((int)threadIdx.x >= nv) return;
+    st += threadIdx.x;
     st->normB = sqrt(st->normB);
     if (st->normB == 0.0) st->done = 1;   // zero load: x = 0, no iterations
 }
@@ -1076,11 +1118,11 @@ __global__ void pcg_init_kernel(PcgState *st)
 // changed.  Capture runs on the solver's own non-blocking stream (the
 // caller's stream may be the legacy default stream, which cannot be captured).
 template <class Body>
-static cudaError_t pcg_graph_prepare(top_solver *s, const double *b, double *x, int chunk, Body body,
+static cudaError_t pcg_graph_prepare(top_solver *s, const double *b, double *x, int chunk, int nrhs, Body body,
                                      top_solver::PcgGraph **out)
 {
     for (auto &G : s->graphs)
-        if (G.exec && G.b == b && G.x == x && G.gen == s->opGen && G.chunk == chunk) { *out = &G; return cudaSuccess; }
+        if (G.exec && G.b == b && G.x == x && G.gen == s->opGen && G.chunk == chunk && G.nrhs == nrhs) { *out = &G; return cudaSuccess; }
     cudaError_t e;
     if (!s->capStream) {
         if ((e = cudaStreamCreateWithFlags(&s->capStream, cudaStreamNonBlocking)) != cudaSuccess) return e;
@@ -1090,7 +1132,7 @@ static cudaError_t pcg_graph_prepare(top_solver *s, const double *b, double *x, 
     // drop stale graphs and, beyond eight, the oldest
     for (size_t i = 0; i < s->graphs.size();) {
         top_solver::PcgGraph &G = s->graphs[i];
-        if (G.gen != s->opGen || (G.b == b && G.x == x) || s->graphs.size() >= 8) {
+        if (G.gen != s->opGen || (G.b == b && G.x == x && G.nrhs == nrhs) || s->graphs.size() >= 8) {
             if (G.exec) cudaGraphExecDestroy(G.exec);
             s->graphs.erase(s->graphs.begin() + (long)i);
         } else {
@@ -1113,46 +1155,54 @@ static cudaError_t pcg_graph_prepare(top_solver *s, const double *b, double *x, 
     if (e == cudaSuccess) e = cudaGraphInstantiate(&G.exec, graph, 0);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) return e;
-    G.b = b; G.x = x; G.gen = s->opGen; G.chunk = chunk;
+    G.b = b; G.x = x; G.gen = s->opGen; G.chunk = chunk; G.nrhs = nrhs;
     s->graphs.push_back(G);
     *out = &s->graphs.back();
     return cudaSuccess;
 }
 
-int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, int *itsOut, double *resOut)
+// PCG (TOP_GPU.m:602-667) on nrhs right-hand sides at once: b and x hold
+// nrhs level-0 grid vectors at stride 3 CS; every operator runs once per
+// iteration for all of them (one launch, the right-hand side in the grid's
+// y or z index); each right-hand side keeps its own scalars and stops on its
+// own residual.  itsOut / resOut: arrays of nrhs (may be NULL).
+int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, int warm, int *itsOut, double *resOut)
 {
     if (!s->assembled) { set_error("top_solver_pcg: assemble first"); return TOP_ERR_STATE; }
+    if (nrhs < 1 || nrhs > s->kMax) { set_error("top_solver_pcg: %d right-hand sides (at most %d)", nrhs, s->kMax); return TOP_ERR_ARGS; }
     DevLevel &l0 = s->L[0];
     const int64_t cs = l0.g.cs, nv = 3 * cs;    // whole grid vectors, margins included
     cudaStream_t st = s->st;
     const int VB = vec_blocks(nv);
     const int64_t M = kMargin;
+    const unsigned K = (unsigned)nrhs;
     // mixed precision keeps the FP32 V-cycle's output z in FP32
     const bool z32 = s->p.precision == TOP_PREC_MIXED;
-    PcgState h{};
-    h.tol = s->p.tol; h.maxIT = s->p.maxIT;
-    CK(cudaMemcpyAsync(s->state, &h, sizeof(PcgState), cudaMemcpyHostToDevice, st));
+    std::vector<PcgState> h0((size_t)nrhs);
+    for (auto &h : h0) { h = PcgState{}; h.tol = s->p.tol; h.maxIT = s->p.maxIT; }
+    CK(cudaMemcpyAsync(s->state, h0.data(), sizeof(PcgState) * nrhs, cudaMemcpyHostToDevice, st));
     int *done = &s->state->done;
-    dot_kernel<<<VB, 256, 0, st>>>(bGrid - M, bGrid - M, nv, s->red(&s->state->normB));
+    auto red = [&](double *r) { return nrhs > 1 ? s->redk(r) : s->red(r); };
+    dot_kernel<<<dim3(VB, K), 256, 0, st>>>(bGrid - M, bGrid - M, nv, red(&s->state->normB));
     TOPGPU_COUNT_LAUNCH();
-    pcg_init_kernel<<<1, 1, 0, st>>>(s->state);
+    pcg_init_kernel<<<1, 32, 0, st>>>(s->state, nrhs);
     TOPGPU_COUNT_LAUNCH();
-    if (!warm) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * 3 * cs, st));
+    if (!warm) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * nv * nrhs, st));
     // r = b - A x
     if (s->p.outerFP32)
-        l0_op<float>(s, VecIn<float, double>{xg, cs}, ResidOut<float, double, double>{bGrid, s->r, cs},
-                        Reduce{nullptr, nullptr, nullptr}, done);
+        l0_op<float>(s, VecIn<float, double>{xg, cs, nv}, ResidOut<float, double, double>{bGrid, s->r, cs, nv},
+                     Reduce{nullptr, nullptr, nullptr}, done, nrhs);
     else
-        l0_op<double>(s, VecIn<double, double>{xg, cs}, ResidOut<double, double, double>{bGrid, s->r, cs},
-                         Reduce{nullptr, nullptr, nullptr}, done);
+        l0_op<double>(s, VecIn<double, double>{xg, cs, nv}, ResidOut<double, double, double>{bGrid, s->r, cs, nv},
+                      Reduce{nullptr, nullptr, nullptr}, done, nrhs);
     // z = M r ; rho = z . r ; p = z
     auto precond_p = [&](cudaStream_t q, int first) {                                         // z = M r, z.r; p = z + beta p
         if (z32) {
-            vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done);
-            pcg_p_kernel<float><<<VB, 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first);
+            vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv);
+            pcg_p_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first);
         } else {
-            vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done);
-            pcg_p_kernel<double><<<VB, 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first);
+            vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv);
+            pcg_p_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first);
         }
         TOPGPU_COUNT_LAUNCH();
     };
@@ -1160,18 +1210,18 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
     CKL();
     static const bool trace = std::getenv("TOPGPU_PCG_TRACE") != nullptr;
     const int chunk = trace ? 1 : 4;
-    // one PCG iteration (TOP_GPU.m:620-655); every kernel returns at once when done is set
+    // one PCG iteration (TOP_GPU.m:620-655); every kernel returns at once for a converged right-hand side
     auto iteration = [&](cudaStream_t q) {
-        outer_op(s, s->pv, s->v, &s->state->pv, done);                                       // v = A p, p.v
-        pcg_update_kernel<<<VB, 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, s->red(&s->state->rr));
+        outer_op(s, s->pv, s->v, &s->state->pv, done, nrhs, nv);                             // v = A p, p.v
+        pcg_update_kernel<<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr));
         TOPGPU_COUNT_LAUNCH();
-        pcg_check_kernel<<<1, 1, 0, q>>>(s->state);
+        pcg_check_kernel<<<1, 32, 0, q>>>(s->state, nrhs);
         TOPGPU_COUNT_LAUNCH();
         precond_p(q, 0);
     };
     top_solver::PcgGraph *G = nullptr;
     if (s->useGraphs && !trace)
-        CK(pcg_graph_prepare(s, bGrid, xg, chunk, [&](cudaStream_t q) { for (int k = 0; k < chunk; ++k) iteration(q); }, &G));
+        CK(pcg_graph_prepare(s, bGrid, xg, chunk, nrhs, [&](cudaStream_t q) { for (int k = 0; k < chunk; ++k) iteration(q); }, &G));
     for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
         if (G && it0 + chunk <= s->p.maxIT) {
             CK(cudaEventRecord(s->capIn, st));
@@ -1184,20 +1234,32 @@ int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, i
             for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) iteration(st);
         }
         CKL();
-        CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(s->hstate, s->state, sizeof(PcgState) * nrhs, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (trace && it0 < 12)
             std::fprintf(stderr, "pcg it %d rho %.6e rhoOld %.6e pv %.6e rr %.6e res %.6e done %d\n", s->hstate->its,
                          s->hstate->rho, s->hstate->rhoOld, s->hstate->pv, s->hstate->rr, s->hstate->resnorm, s->hstate->done);
-        if (s->hstate->done) break;
+        bool all = true;
+        for (int k = 0; k < nrhs; ++k) all = all && s->hstate[k].done;
+        if (all) break;
     }
-    const PcgState &f = *s->hstate;
-    if (f.normB == 0.0) CK(cudaMemsetAsync(xg - kMargin, 0, sizeof(double) * 3 * cs, st));
-    if (itsOut) *itsOut = f.its;
-    if (resOut) *resOut = f.resnorm;
-    if (f.status == TOP_ERR_NAN) { set_error("top_solver_pcg: non-finite PCG scalar at iteration %d", f.its); return TOP_ERR_NAN; }
-    if (f.status == TOP_ERR_NOT_CONVERGED) { set_error("Exceed the maximum iterate numbers (residual %.4e)", f.resnorm); return TOP_ERR_NOT_CONVERGED; }
-    return TOP_OK;
+    int rc = TOP_OK;
+    for (int k = 0; k < nrhs; ++k) {
+        const PcgState &f = s->hstate[k];
+        if (f.normB == 0.0) CK(cudaMemsetAsync(xg + k * nv - kMargin, 0, sizeof(double) * nv, st));
+        if (itsOut) itsOut[k] = f.its;
+        if (resOut) resOut[k] = f.resnorm;
+        if (f.status == TOP_ERR_NAN) { set_error("top_solver_pcg: non-finite PCG scalar at iteration %d", f.its); rc = TOP_ERR_NAN; }
+        else if (f.status == TOP_ERR_NOT_CONVERGED && rc == TOP_OK) {
+            set_error("Exceed the maximum iterate numbers (residual %.4e)", f.resnorm); rc = TOP_ERR_NOT_CONVERGED;
+        }
+    }
+    return rc;
+}
+
+int topgpu::pcg_grid(top_solver *s, const double *bGrid, double *xg, int warm, int *itsOut, double *resOut)
+{
+    return pcg_block(s, bGrid, xg, 1, warm, itsOut, resOut);
 }
 
 // compact warm start / solution around pcg_grid
@@ -1223,6 +1285,29 @@ extern "C" int top_solver_pcg(top_solver *s, int loadCase, double *U, int warm, 
 {
     if (!s || !U || loadCase < 0 || loadCase >= s->nLoads) { set_error("top_solver_pcg: bad arguments"); return TOP_ERR_ARGS; }
     return pcg_run(s, s->b + (size_t)loadCase * 3 * s->L[0].g.cs, U, warm, its, relres);
+}
+
+extern "C" int top_solver_pcg_all(top_solver *s, double *U, int warm, int *its, double *relres)
+{
+    if (!s || !U) { set_error("top_solver_pcg_all: bad arguments"); return TOP_ERR_ARGS; }
+    DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs, nd = 3 * l0.Nn;
+    const int K = s->nLoads;
+    CK(cudaMemsetAsync(s->x - kMargin, 0, sizeof(double) * 3 * cs * K, s->st));
+    if (warm)
+        for (int k = 0; k < K; ++k) {
+            compact_to_grid_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(U + k * nd, s->x + k * 3 * cs, l0.nodeGrid, l0.Nn, cs);
+            TOPGPU_COUNT_LAUNCH();
+        }
+    const int rc = pcg_block(s, s->b, s->x, K, 1, its, relres);
+    if (rc != TOP_OK && rc != TOP_ERR_NOT_CONVERGED) return rc;
+    for (int k = 0; k < K; ++k) {
+        grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(s->x + k * 3 * cs, U + k * nd, l0.nodeGrid, l0.Nn, cs);
+        TOPGPU_COUNT_LAUNCH();
+    }
+    CKL();
+    CK(cudaStreamSynchronize(s->st));
+    return rc;
 }
 
 extern "C" int top_solver_pcg_rhs(top_solver *s, const double *b, double *U, int warm, int *its, double *relres)

@@ -10,11 +10,6 @@
 
 namespace topgpu {
 
-struct PcgState {
-    double normB, rho, rhoOld, pv, rr, resnorm, tol;
-    int its, maxIT, done, status;
-};
-
 // ---------------------------------------------------------------------------
 struct DevLevel {
     int ny = 0, nx = 0, nz = 0, span = 0;
@@ -41,7 +36,7 @@ struct top_solver {
     // re-captured when an operand pointer or the operator configuration changes)
     struct PcgGraph {
         cudaGraphExec_t exec = nullptr;
-        const double *b = nullptr; double *x = nullptr; int gen = -1, chunk = 0; int64_t nodes = 0;
+        const double *b = nullptr; double *x = nullptr; int gen = -1, chunk = 0, nrhs = 1; int64_t nodes = 0;
     };
     std::vector<PcgGraph> graphs;    // one per (right-hand side, solution) pair in use
     cudaStream_t capStream = nullptr; cudaEvent_t capIn = nullptr, capOut = nullptr;
@@ -106,6 +101,9 @@ struct top_solver {
         return b ? b + topgpu::kMargin : nullptr;
     }
     Reduce red(double *result) const { return Reduce{partials, counter, result}; }
+    // per-right-hand-side sums into consecutive PcgState's (batched launches)
+    Reduce redk(double *result) const { return Reduce{partials, counter, result, nPartials, topgpu::kStateDoubles}; }
+    int kMax = 1;                    // right-hand sides the buffers hold (load cases)
 };
 
 // every kernel launch of the solver is counted on the solver it serves
@@ -115,7 +113,7 @@ namespace topgpu {
 // y-epilogue applied to (K_0 in)(node) for every level-0 node, with the
 // level-0 kernel configured for precision T (topgpu_l0.cu)
 template <typename T, class In, class Out>
-void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done);
+void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *done, int nv = 1);
 // configure the level-0 kernel of precision slot p (0 FP64, 1 FP32)
 int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas);
 // time every level-0 kernel configuration, keep the fastest per precision
@@ -123,6 +121,8 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
 // PCG (TOP_GPU.m:602-667) on level-0 grid vectors: b and x in the solver's
 // SoA grid layout, x holds the warm start when warm != 0 and the solution.
 int pcg_grid(top_solver *s, const double *bGrid, double *xGrid, int warm, int *itsOut, double *resOut);
+// the same on nrhs right-hand sides at once (vectors at stride 3 CS)
+int pcg_block(top_solver *s, const double *bGrid, double *xGrid, int nrhs, int warm, int *itsOut, double *resOut);
 void free_opt_state(top_solver *s);
 // element moduli from a compact element vector (SIMP when simp != 0)
 int set_modulus_dev(top_solver *s, const double *src, int where, int simp);

@@ -248,10 +248,13 @@ template <typename T, int NT> struct WalshOcc {
 
 template <typename T, int TY, int TX, class In, class Out>
 __global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
-l0w_kernel(const WalshParam<T> B, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
-           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red, const int *__restrict__ done)
+l0w_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    const int vk = blockIdx.y;          // right-hand side of a batched launch
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
     using Tl = WalshTile<T, TY, TX>;
     __shared__ T su[3 * Tl::SC];
     __shared__ T so[9 * Tl::NT];
@@ -270,7 +273,7 @@ l0w_kernel(const WalshParam<T> B, In in, Out out, const T *__restrict__ E, const
             l0w_march<T, TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, su, so, dot);
         a += z1 - z0;
     }
-    if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result);
+    if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 
 // tileMask[tile] = 1 when a node staged by that tile (any layer) has a fixed component
@@ -515,10 +518,13 @@ template <typename T, int NT> struct WalshPairOcc {
 
 template <typename T, int TYP, int TX, class In, class Out>
 __global__ void __launch_bounds__(TYP * TX, WalshPairOcc<T, TYP * TX>::value)
-l0p_kernel(const WalshPairParam<T> B, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
-           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red, const int *__restrict__ done)
+l0p_kernel(const WalshPairParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    const int vk = blockIdx.y;          // right-hand side of a batched launch
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
     using Tl = WalshPairTile<T, TYP, TX>;
     __shared__ __align__(16) T su[3 * Tl::SC];
     __shared__ __align__(16) T so[12 * Tl::NT];
@@ -537,7 +543,7 @@ l0p_kernel(const WalshPairParam<T> B, In in, Out out, const T *__restrict__ E, c
             l0p_march<T, TYP, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, su, so, dot);
         a += z1 - z0;
     }
-    if (red.result) block_sum_to<TYP * TX>(dot, red.partials, red.counter, red.result);
+    if (red.result) block_sum_to<TYP * TX>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 
 // tileMask[tile] for the pair tiling: any staged node with a fixed component
@@ -677,10 +683,13 @@ __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, 
 
 template <typename T, int TY, int TX, class In, class Out>
 __global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
-l0d_kernel(const WalshParam<T> B, In in, Out out, const T *__restrict__ E, const uint8_t *__restrict__ flags,
-           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red, const int *__restrict__ done)
+l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    const int vk = blockIdx.y;          // right-hand side of a batched launch
+    const int *done = done_of(done0, vk);
     if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
     __shared__ T so[2 * 9 * TY * TX];
     const int tilesY = (g.NY + TY - 2) / (TY - 1);
     const int64_t total = (int64_t)walsh_tiles(g, TY, TX) * g.NZ;
@@ -697,7 +706,7 @@ l0d_kernel(const WalshParam<T> B, In in, Out out, const T *__restrict__ E, const
             l0d_march<T, TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
         a += z1 - z0;
     }
-    if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result);
+    if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 
 }  // namespace topgpu

@@ -188,6 +188,22 @@ class Solver:
         check(lib().top_solver_get_ks(self._h, level, out.data_ptr()), "top_solver_get_ks")
         return out
 
+    def pcg_all(self, U=None):
+        """All load cases as one batched PCG; returns (U [3Nn x nLoads] as a
+        column-major flat tensor, its list, relres list)."""
+        nd = 3 * self.levels[0]["numNodes"]
+        out = torch.zeros(nd * self.nLoads, dtype=torch.float64, device="cuda")
+        warm = 0
+        if U is not None:
+            out.copy_(self._dev(U, nd * self.nLoads))
+            warm = 1
+        its = (C.c_int * self.nLoads)()
+        res = (C.c_double * self.nLoads)()
+        st = lib().top_solver_pcg_all(self._h, out.data_ptr(), warm, its, res)
+        if st not in (TOP_OK, TOP_ERR_NOT_CONVERGED):
+            check(st, "top_solver_pcg_all")
+        return out, list(its), list(res)
+
     def pcg(self, load_case=0, U=None, b=None, raise_on_maxit=False):
         """Solving_PCG on load case k (or an explicit rhs b); U is the warm start.
 
