@@ -1,0 +1,94 @@
+"""The batching configuration at full size: a synthetic irregular domain in a
+192x384x192 grid (the union of three seeded ellipsoids, semi-axes 40-90
+voxels, and a cylinder of radius 30 along x; 4.8 M active voxels), all DOFs
+fixed on the active nodes of the x = 0 face, four load cases (unit loads in
+-y, +z, -z, +y spread over seeded 200-node patches of the x = max face),
+solved as one batched PCG per iteration.  Mixed precision against the FP64
+path over two optimisation iterations (ft = 2, V0 = 0.3): compliance within
+1e-6, densities within 1e-4; plus the batched solves against per-load solves."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (192, 384, 192)
+CONTROL = 1000          # coarsest level 1302 DOF
+
+
+def domain_mask(seed=34, shape=SHAPE):
+    ny, nx, nz = shape
+    rng = np.random.default_rng(seed)
+    y, x, z = np.meshgrid(np.arange(ny) + 0.5, np.arange(nx) + 0.5, np.arange(nz) + 0.5, indexing="ij")
+    m = np.zeros(shape, bool)
+    for _ in range(3):
+        c = np.array([rng.uniform(0.3, 0.7) * ny, rng.uniform(0.25, 0.75) * nx, rng.uniform(0.3, 0.7) * nz])
+        a = rng.uniform(40, 90, 3)
+        m |= ((y - c[0]) / a[0]) ** 2 + ((x - c[1]) / a[1]) ** 2 + ((z - c[2]) / a[2]) ** 2 <= 1
+    m |= (y - ny / 2) ** 2 + (z - nz / 2) ** 2 <= 30 ** 2
+    return m
+
+
+def boundary_conditions(mesh, seed=1, patch=200):
+    lv = mesh.info()[0]
+    NY, NX = lv["resY"] + 1, lv["resX"] + 1
+    fwd = mesh.get(0, "nodMapForward")                      # grid node -> compact (1-based), 0 = void
+    act = np.flatnonzero(fwd)
+    Y, X, Z = act % NY, (act // NY) % NX, act // (NY * NX)
+    fixed = fwd[act[X == 0]]
+    fix = np.column_stack([fixed, np.ones((len(fixed), 3))]).astype(float)
+    face = act[X == X.max()]
+    fy, fz = face % NY, face // (NY * NX)
+    rng = np.random.default_rng(seed)
+    loads = []
+    for d in ((0, -1, 0), (0, 0, 1), (0, 0, -1), (0, 1, 0)):
+        c = rng.integers(len(face))
+        near = np.argsort((fy - fy[c]) ** 2 + (fz - fz[c]) ** 2, kind="stable")[:patch]
+        rows = np.column_stack([fwd[face[near]], np.tile(np.array(d, float) / patch, (patch, 1))])
+        loads.append(rows.astype(float))
+    return fix, loads
+
+
+@pytest.fixture(scope="module")
+def model():
+    from top_gpu_on_matlab_b200.fea import Mesh
+    m = Mesh(domain_mask(), control=CONTROL)
+    fix, loads = boundary_conditions(m)
+    m.apply_bc(fix, loads)
+    return m
+
+
+def test_domain_and_hierarchy(model):
+    info = model.info()
+    assert info[0]["numElements"] == 4804189
+    assert 3 * info[-1]["numNodes"] <= 5000
+
+
+def test_batched_solves_equal_per_load_solves(model):
+    from top_gpu_on_matlab_b200.fea import Solver
+    s = Solver(model, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6, mixed=True)
+    ne = model.info()[0]["numElements"]
+    s.set_density(torch.full((ne,), 0.3, dtype=torch.float64, device="cuda"))
+    s.assemble()
+    nd = s.numDOFs
+    Ub, its_b, _ = s.pcg_all()
+    for k in (0, 3):
+        Uk, its_k, _ = s.pcg(k)
+        assert its_b[k] == its_k
+        assert torch.equal(Ub[k * nd:(k + 1) * nd], Uk)
+
+
+def test_mixed_tracks_fp64_over_two_iterations(model):
+    from top_gpu_on_matlab_b200.fea import Solver
+    out = {}
+    for name, mixed in (("fp64", False), ("mixed", True)):
+        s = Solver(model, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6, mixed=mixed)
+        s.autotune(nrep=2, flush_bytes=0)
+        s.opt_begin(V0=0.3, rMin=np.sqrt(3), nLoop=30, ft=2)
+        recs = [s.opt_step() for _ in range(2)]
+        xp, _ = s.design()
+        out[name] = (recs, xp)
+        del s
+    for a, b in zip(out["mixed"][0], out["fp64"][0]):
+        assert abs(a["c"] - b["c"]) <= 1e-6 * abs(b["c"])
+    assert float((out["mixed"][1] - out["fp64"][1]).abs().max()) <= 1e-4
