@@ -288,13 +288,14 @@ int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushByte
 
 /* Level-0 stiffness product kernel, per precision (fp32 = 0: the FP64
  * products, 1: the FP32 V-cycle products).  kind 0 = node-centric product
- * with the dense 24x24 Ke.  Kinds 1-3 use Ke in the Walsh-Hadamard basis of
+ * with the dense 24x24 Ke.  Kinds 1-4 use Ke in the Walsh-Hadamard basis of
  * the cube element (eight 3x3 blocks) and march z through tiles of ty x tx
  * threads, each of ctas CTAs taking an equal share of the (tile, z-layer)
  * work (ctas = 0: as many CTAs as fit on the GPU at once): kind 1 stages the
  * node layers in shared memory, kind 2 (FP32 only) gives each thread two
  * element columns and uses paired FP32 arithmetic, kind 3 loads each
- * column's corner nodes directly.  Tile shapes 16x16 and 16x8.  Kinds 1-3
+ * column's corner nodes directly, kind 4 (FP32 only) combines the two.
+ * Tile shapes 16x16 and 16x8.  Kinds 1-4
  * need Ke with the cube's reflection symmetry (always the case for the
  * reference's isotropic voxel); kind 3 is the default then.  get returns
  * {kind, ty, tx, ctas}.  No counterpart in the reference. */
@@ -305,6 +306,11 @@ int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);
  * on a solver-owned stream ordered after the caller's); on = 0 launches the
  * kernels one by one instead.  Default on.  No counterpart in the reference. */
 int top_solver_set_graphs(top_solver *s, int on);
+/* The V-cycle below level 0 (coarse products, span-2 transfers, coarsest
+ * solve) as one persistent cooperative launch with grid-wide barriers
+ * (on = 1, default) or one launch per step (0); identical results.  No
+ * counterpart in the reference. */
+int top_solver_set_coarse_persistent(top_solver *s, int on);
 /* Autotuner: times each level-0 kernel configuration (kind, tile shape, CTA
  * count; nrep launches each, L2 flushed by writing flushBytes before every
  * launch) on this model and keeps the fastest per precision.  msBest2 gets

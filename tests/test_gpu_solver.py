@@ -140,6 +140,23 @@ def test_pcg_graphs_match_launches(pair):
     assert n1 - n0 >= n2 - n1 > 0
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_persistent_coarse_vcycle_matches_per_level_launches(pair, mixed):
+    """levels below 0 in one cooperative launch give the per-level launches'
+    results bit for bit (same device code, same summation order)"""
+    o, s, m, _ = pair
+    from top_gpu_on_matlab_b200.fea import Solver
+    s2 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6, mixed=mixed)
+    x = torch.from_numpy(0.2 + 0.7 * np.random.default_rng(3).random(o.level(0).numElements)).cuda()
+    s2.set_density(x)
+    s2.assemble()
+    r = torch.from_numpy(np.random.default_rng(8).standard_normal(o.level(0).numDOFs)).cuda()
+    za = s2.vcycle(r)
+    s2.set_coarse_persistent(False)
+    zb = s2.vcycle(r)
+    assert torch.equal(za, zb)
+
+
 def test_pcg_warm_start_and_unit_compliance(pair):
     _smooth_only(pair)
     o, s, _, _ = pair

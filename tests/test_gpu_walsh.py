@@ -83,7 +83,7 @@ def test_walsh_matvec_matches_oracle(model, shape, ctas):
     u = np.random.default_rng(ctas).standard_normal(o.level(0).numDOFs)
     ref = o.matvec(0, u)
     ud = torch.from_numpy(u).cuda()
-    for fp32, kind in ((False, 1), (True, 1), (True, 2), (False, 3), (True, 3)):
+    for fp32, kind in ((False, 1), (True, 1), (True, 2), (False, 3), (True, 3), (True, 4)):
         s.set_l0_kernel(fp32, kind, shape[0], shape[1], ctas)
         y = s.matvec(0, ud, fp32=fp32)
         assert _rel(y, ref) < (2e-6 if fp32 else 1e-13), (shape, ctas, fp32, kind)
@@ -110,8 +110,10 @@ def test_walsh_rejects_bad_shape(model):
         s.set_l0_kernel(False, 1, 12, 12, 4)
     with pytest.raises(TopGpuError):
         s.set_l0_kernel(False, 1, 16, 16, -1)
-    with pytest.raises(TopGpuError):          # paired-element kernel: FP32 only
+    with pytest.raises(TopGpuError):          # paired-element kernels: FP32 only
         s.set_l0_kernel(False, 2, 16, 8, 0)
+    with pytest.raises(TopGpuError):
+        s.set_l0_kernel(False, 4, 16, 8, 0)
     assert s.l0_kernel(False) == keep        # a rejected configuration changes nothing
 
 
@@ -123,7 +125,7 @@ def test_vcycle_and_pcg_with_walsh_match_oracle():
     assert _rel(s.vcycle(torch.from_numpy(r).cuda()), o.vcycle(r)) < 1e-11
 
 
-@pytest.mark.parametrize("kind", [1, 2, 3])
+@pytest.mark.parametrize("kind", [1, 2, 3, 4])
 def test_mixed_vcycle_kinds_agree(kind):
     """The FP32 V-cycle with either Walsh kernel stays within FP32 rounding
     of the FP64 V-cycle."""

@@ -123,7 +123,7 @@ __device__ __forceinline__ const int *done_of(const int *done, int k) { return d
 template <typename P> struct Comp3 {
     P p0, p1, p2;
     Comp3() = default;
-    Comp3(P base, int64_t cs) : p0(base), p1(base + cs), p2(base + 2 * cs) {}
+    __host__ __device__ Comp3(P base, int64_t cs) : p0(base), p1(base + cs), p2(base + 2 * cs) {}
     __device__ __forceinline__ P operator[](int c) const { return c == 0 ? p0 : (c == 1 ? p1 : p2); }
     __device__ __forceinline__ Comp3 shifted(int64_t o) const { Comp3 r = *this; r.p0 += o; r.p1 += o; r.p2 += o; return r; }
 };
@@ -131,7 +131,7 @@ template <typename P> struct Comp3 {
 template <typename T, typename TV>
 struct VecIn {
     Comp3<const TV *> u; int64_t vs;
-    VecIn(const TV *base, int64_t cs, int64_t vstride = 0) : u(base, cs), vs(vstride) {}
+    __host__ __device__ VecIn(const TV *base, int64_t cs, int64_t vstride = 0) : u(base, cs), vs(vstride) {}
     __device__ __forceinline__ VecIn shift(int k) const { VecIn r = *this; if (k) r.u = u.shifted(k * vs); return r; }
     __device__ __forceinline__ T operator()(int m, int c) const { return T(u[c][m]); }
 };
@@ -139,7 +139,7 @@ struct VecIn {
 template <typename T, typename TR>
 struct JacobiIn {
     Comp3<const TR *> r; Comp3<const T *> invD; T omega; int64_t vs;
-    JacobiIn(const TR *rb, const T *ib, int64_t cs, T om, int64_t vstride = 0) : r(rb, cs), invD(ib, cs), omega(om), vs(vstride) {}
+    __host__ __device__ JacobiIn(const TR *rb, const T *ib, int64_t cs, T om, int64_t vstride = 0) : r(rb, cs), invD(ib, cs), omega(om), vs(vstride) {}
     __device__ __forceinline__ JacobiIn shift(int k) const { JacobiIn o = *this; if (k) o.r = r.shifted(k * vs); return o; }
     __device__ __forceinline__ T operator()(int m, int c) const { return omega * invD[c][m] * T(r[c][m]); }
 };
@@ -148,7 +148,7 @@ struct JacobiIn {
 template <typename T, typename TY>
 struct StoreOut {   // y
     Comp3<TY *> y; int64_t vs;
-    StoreOut(TY *yb, int64_t cs, int64_t vstride = 0) : y(yb, cs), vs(vstride) {}
+    __host__ __device__ StoreOut(TY *yb, int64_t cs, int64_t vstride = 0) : y(yb, cs), vs(vstride) {}
     __device__ __forceinline__ StoreOut shift(int k) const { StoreOut o = *this; if (k) o.y = y.shifted(k * vs); return o; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     { for (int c = 0; c < 3; ++c) y[c][i] = TY(yv[c]); (void)dot; }
@@ -156,7 +156,7 @@ struct StoreOut {   // y
 template <typename T, typename TU, typename TY>
 struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
     Comp3<TY *> y; Comp3<const TU *> u; int64_t vs;
-    DotStoreOut(TY *yb, const TU *ub, int64_t cs, int64_t vstride = 0) : y(yb, cs), u(ub, cs), vs(vstride) {}
+    __host__ __device__ DotStoreOut(TY *yb, const TU *ub, int64_t cs, int64_t vstride = 0) : y(yb, cs), u(ub, cs), vs(vstride) {}
     __device__ __forceinline__ DotStoreOut shift(int k) const
     { DotStoreOut o = *this; if (k) { o.y = y.shifted(k * vs); o.u = u.shifted(k * vs); } return o; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
@@ -165,7 +165,7 @@ struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
 template <typename T, typename TR, typename TD>
 struct ResidOut {   // d = r - y
     Comp3<const TR *> r; Comp3<TD *> d; int64_t vsR, vsD;
-    ResidOut(const TR *rb, TD *db, int64_t cs, int64_t vsr = 0, int64_t vsd = -1)
+    __host__ __device__ ResidOut(const TR *rb, TD *db, int64_t cs, int64_t vsr = 0, int64_t vsd = -1)
         : r(rb, cs), d(db, cs), vsR(vsr), vsD(vsd < 0 ? vsr : vsd) {}
     __device__ __forceinline__ ResidOut shift(int k) const
     { ResidOut o = *this; if (k) { o.r = r.shifted(k * vsR); o.d = d.shifted(k * vsD); } return o; }
@@ -176,7 +176,7 @@ struct ResidOut {   // d = r - y
 template <typename T, typename TR, typename TZ>
 struct PostSmoothOut {
     Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega; int64_t vs;
-    PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om, int64_t vstride = 0)
+    __host__ __device__ PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om, int64_t vstride = 0)
         : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om), vs(vstride) {}
     __device__ __forceinline__ PostSmoothOut shift(int k) const
     {
@@ -331,22 +331,21 @@ coarse_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, c
 // threads of a warp read consecutive element slots (one coalesced run), and
 // the eight partial sums of a node are added in a fixed order.
 constexpr int kCoarseTileX = 32;
-template <typename T, class In, class Out>
-__global__ void __launch_bounds__(kCoarseTileX * 8)
-coarse_tile_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, const int *__restrict__ done0)
+// packed-entry offsets (entry * CS) of Ks(r, k) of a level, in shared memory
+__device__ __forceinline__ void coarse_offsets(int *offs, const Geom &g, int tid, int nthreads)
 {
-    const int vk = blockIdx.z;
-    const int *done = done_of(done0, vk);
-    if (done && *done) return;
-    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
-    __shared__ T part[8][3][kCoarseTileX];
-    __shared__ int offs[24 * 24];        // packed-entry offset (entry * CS) of Ks(r, k)
-    const int n = threadIdx.x, i = threadIdx.y;
-    for (int k = n + kCoarseTileX * i; k < 24 * 24; k += kCoarseTileX * 8)
-        offs[k] = sym_pack(k / 24, k % 24) * (int)g.cs;
-    __syncthreads();
-    const int q = blockIdx.x * kCoarseTileX + n;
-    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    for (int k = tid; k < 24 * 24; k += nthreads) offs[k] = sym_pack(k / 24, k % 24) * (int)g.cs;
+}
+// One tile: the 32 node slots q = bx*32 .. bx*32+31 of z layer bz; thread
+// (n, i) of the 256 takes incident element i of node n.  Every thread of the
+// CTA calls it; returns the dot contribution of the epilogue (threads i == 0).
+template <typename T, class In, class Out>
+__device__ __forceinline__ double coarse_tile_unit(const In &in, const Out &out, const T *__restrict__ Ks, const Geom &g,
+                                                   int bx, int bz, int n, int i, T (*part)[3][kCoarseTileX],
+                                                   const int *offs)
+{
+    const int q = bx * kCoarseTileX + n;
+    const int Y = q % g.PY, X = q / g.PY, Z = bz;
     const bool valid = Y < g.NY && X < g.NX;
     const int PY = g.PY, PL = (int)g.plane;
     const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
@@ -381,10 +380,26 @@ coarse_tile_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce re
         }
         out(idx, s, dot);
     }
+    __syncthreads();                     // part is reused by the next tile
+    return dot;
+}
+template <typename T, class In, class Out>
+__global__ void __launch_bounds__(kCoarseTileX * 8)
+coarse_tile_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, const int *__restrict__ done0)
+{
+    const int vk = blockIdx.z;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
+    __shared__ T part[8][3][kCoarseTileX];
+    __shared__ int offs[24 * 24];
+    coarse_offsets(offs, g, threadIdx.x + kCoarseTileX * threadIdx.y, kCoarseTileX * 8);
+    __syncthreads();
+    const double dot = coarse_tile_unit<T>(in, out, Ks, g, blockIdx.x, blockIdx.y, threadIdx.x, threadIdx.y, part, offs);
     if (red.result) block_sum_to<kCoarseTileX * 8>(dot, red.partials, red.counter, red.result, gridDim.x * gridDim.y,
                                                    blockIdx.x + gridDim.x * blockIdx.y);
 }
-inline dim3 coarse_tile_grid(const Geom &g)
+__host__ __device__ inline dim3 coarse_tile_grid(const Geom &g)
 {
     return dim3((unsigned)(((int64_t)g.PY * g.NX + kCoarseTileX - 1) / kCoarseTileX), (unsigned)g.NZ);
 }
@@ -406,17 +421,13 @@ inline unsigned coarse_blocks(const Geom &g)
 // its columns' 2S-1 y taps, the group adds up with shuffles.
 template <int S> struct RestrictLanes { static constexpr int value = (S >= 4) ? 32 : 8; };
 
+// lane-group restriction of one coarse node; gt = the thread's index in the
+// lane layout (LPN lanes per coarse node; every lane of a warp must call it)
 template <typename T, int S>
-__global__ void __launch_bounds__(kNodeThreads)
-restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
-                const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsF = 0, int64_t vsC = 0)
+__device__ __forceinline__ void restrict_lanes(const T *__restrict__ rf, const Geom &gf, T *__restrict__ rc, const Geom &gc,
+                                               const uint8_t *__restrict__ flagsC, int64_t gt)
 {
-    const int vk = blockIdx.y;
-    const int *done = done_of(done0, vk);
-    if (done && *done) return;
-    rf += vk * vsF; rc += vk * vsC;
     constexpr int LPN = RestrictLanes<S>::value, W = 2 * S - 1;
-    const int64_t gt = (int64_t)blockIdx.x * kNodeThreads + threadIdx.x;
     const int64_t node = gt / LPN;
     const int lane = int(gt % LPN);
     const int64_t nq = (int64_t)gc.PY * gc.NX * gc.NZ;
@@ -451,6 +462,17 @@ restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
 #pragma unroll
         for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
     }
+}
+template <typename T, int S>
+__global__ void __launch_bounds__(kNodeThreads)
+restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
+                const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsF = 0, int64_t vsC = 0)
+{
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    rf += vk * vsF; rc += vk * vsC;
+    restrict_lanes<T, S>(rf, gf, rc, gc, flagsC, (int64_t)blockIdx.x * kNodeThreads + threadIdx.x);
 }
 template <int S>
 inline unsigned restrict_blocks(const Geom &gc)
@@ -549,22 +571,13 @@ restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc
     for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
 }
 
-// x_f = base + P x_c, base = omega*invD.*r when r != nullptr (the pre-smoothed
-// iterate of the V-cycle, recomputed instead of stored), 0 otherwise.
+// one fine node (linear in-plane index q, layer Z) of the prolongation
 template <typename T, int S, typename TR>
-__global__ void __launch_bounds__(kNodeThreads)
-prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
-               const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
-               const T *__restrict__ invD, T omega, const int *__restrict__ done0,
-               int64_t vsC = 0, int64_t vsF = 0, int64_t vsR = 0)
+__device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geom &gc, T *__restrict__ xf, const Geom &gf,
+                                             const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
+                                             const T *__restrict__ invD, T omega, int q, int Z)
 {
-    const int vk = blockIdx.z;
-    const int *done = done_of(done0, vk);
-    if (done && *done) return;
-    xc += vk * vsC; xf += vk * vsF;
-    if (r) r += vk * vsR;
-    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
-    const int Y = q % gf.PY, X = q / gf.PY, Z = blockIdx.y;
+    const int Y = q % gf.PY, X = q / gf.PY;
     if (Y >= gf.NY || X >= gf.NX) return;
     const int64_t i = gf.origin + Y + (int64_t)gf.PY * X + gf.plane * Z;
     T v[3] = {T(0), T(0), T(0)};
@@ -596,6 +609,22 @@ prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
+}
+// x_f = base + P x_c, base = omega*invD.*r when r != nullptr (the pre-smoothed
+// iterate of the V-cycle, recomputed instead of stored), 0 otherwise.
+template <typename T, int S, typename TR>
+__global__ void __launch_bounds__(kNodeThreads)
+prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
+               const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
+               const T *__restrict__ invD, T omega, const int *__restrict__ done0,
+               int64_t vsC = 0, int64_t vsF = 0, int64_t vsR = 0)
+{
+    const int vk = blockIdx.z;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    xc += vk * vsC; xf += vk * vsF;
+    if (r) r += vk * vsR;
+    prolong_node<T, S, TR>(xc, gc, xf, gf, flagsF, r, invD, omega, blockIdx.x * kNodeThreads + threadIdx.x, blockIdx.y);
 }
 
 }  // namespace topgpu

@@ -35,7 +35,7 @@ bool walsh_shape_ok(int ty, int tx)
 }
 int tiles_of(const Geom &g, int kind, int ty, int tx)
 {
-    return kind == 2 ? walsh_pair_tiles(g, ty, tx) : walsh_tiles(g, ty, tx);
+    return (kind == 2 || kind == 4) ? walsh_pair_tiles(g, ty, tx) : walsh_tiles(g, ty, tx);
 }
 
 // grid of the Walsh kernel: the configured CTA count (0: the CTAs that fit
@@ -48,6 +48,7 @@ unsigned l0w_ctas(const top_solver *s, const top_solver::L0Kernel &k)
         cudaError_t e;
         if constexpr (KIND == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0p_kernel<T, A, B, In, Out>, A * B, 0);
         else if constexpr (KIND == 3) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0d_kernel<T, A, B, In, Out>, A * B, 0);
+        else if constexpr (KIND == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0q_kernel<T, A, B, In, Out>, A * B, 0);
         else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0w_kernel<T, A, B, In, Out>, A * B, 0);
         if (e != cudaSuccess) n = 1;
         return n > 0 ? n : 1;
@@ -86,6 +87,15 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
                 walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
         TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
+    } else if (k.kind == 4) {        // FP32 only, as kind 2
+        if constexpr (sizeof(T) == 4) {
+#define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
+            if (k.ty == A && k.tx == B)                                                                       \
+                l0q_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 4>(s, k), K), A * B, 0, s->st>>>( \
+                    walshpair<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
+            TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
+#undef TOPGPU_LAUNCH_SHAPE
+        }
     } else if (k.kind == 2) {        // FP32 only: the FP64 pair state does not fit in registers
         if constexpr (sizeof(T) == 4) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
@@ -106,7 +116,8 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 {
     top_solver::L0Kernel &k = s->l0k[p];
     if (kind == 0) { k.kind = 0; ++s->opGen; return TOP_OK; }
-    if ((kind != 1 && kind != 3 && !(kind == 2 && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0) return TOP_ERR_ARGS;
+    if ((kind != 1 && kind != 3 && !((kind == 2 || kind == 4) && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0)
+        return TOP_ERR_ARGS;
     DevLevel &l0 = s->L[0];
     const int tiles = tiles_of(l0.g, kind, ty, tx);
     if (ctas > s->nPartials) {                         // one reduction partial per CTA and right-hand side
@@ -118,7 +129,7 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
     if (cudaMalloc(&k.mask, (size_t)tiles) != cudaSuccess) { k.mask = nullptr; k.kind = 0; return TOP_ERR_NOMEM; }
 #define TOPGPU_MASK_SHAPE(A, B)                                                                    \
     if (ty == A && tx == B) {                                                                      \
-        if (kind == 2) walsh_pair_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask); \
+        if (kind == 2 || kind == 4) walsh_pair_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask); \
         else walsh_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask);            \
     }
     TOPGPU_WALSH_SHAPES(TOPGPU_MASK_SHAPE)
@@ -171,8 +182,8 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
         double tBest = rc == TOP_OK ? time_l0(s, p, nrep, flush, (size_t)flushBytes, a, b) : -1.0;
         if (tBest < 0) { rc = TOP_ERR_CUDA; break; }
         if (s->walshOK) {
-            for (int kind = 1; kind <= 3 && rc == TOP_OK; ++kind) {
-                if (kind == 2 && p == 0) continue;
+            for (int kind = 1; kind <= 4 && rc == TOP_OK; ++kind) {
+                if ((kind == 2 || kind == 4) && p == 0) continue;
                 for (const auto &sh : shapes)
                     for (int m : mults) {
                         const int ctas = m * s->numSMs;

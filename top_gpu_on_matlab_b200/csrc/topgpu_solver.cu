@@ -14,6 +14,7 @@
 #include <vector>
 #include "topgpu_kernels.cuh"
 #include "topgpu_solver_impl.cuh"
+#include "topgpu_coarse.cuh"
 
 namespace topgpu {
 int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
@@ -504,6 +505,16 @@ void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, co
     else coarse_op<T>(s, l, in, out, red, done);
 }
 
+// the persistent coarse kernel covers levels 1 .. nL-1 when every transfer
+// among them is span 2 (and the solver was not told to launch per level)
+bool coarse_persistent_ok(const top_solver *s)
+{
+    if (!s->coarsePersistent || s->nL < 2 || s->nL - 1 > kCoarseMaxLevels) return false;
+    for (int l = 2; l < s->nL; ++l)
+        if (s->L[l].span != 2) return false;
+    return true;
+}
+
 // V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
 // residuals r0 (type TR, grid layout, nv right-hand sides at stride vs0);
 // writes z0 (type TZ, same stride) and, when zr is set, z0 . r0 into zr
@@ -515,8 +526,10 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     const T omega = T(s->p.omega);
     const Reduce none{nullptr, nullptr, nullptr};
     const unsigned K = (unsigned)nv;
+    // levels below 0 as one persistent kernel where their transfers are span 2
+    const bool persist = coarse_persistent_ok(s);
     // restriction leg
-    for (int l = 0; l < nL - 1; ++l) {
+    for (int l = 0; l < (persist ? 1 : nL - 1); ++l) {
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
         const int64_t vs = lvs(lv);
@@ -528,16 +541,36 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
                          none, done, nv);
         restrict_op<T>(s, l, d, vr<T>(lc), done, nv);
     }
-    // coarsest direct solve, FP64
     DevLevel &lc = s->L[nL - 1];
     const int64_t n = 3 * lc.Nn;
-    coarsest_gather_kernel<T><<<dim3(nb256(n), K), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
-    TOPGPU_COUNT_LAUNCH();
-    coarsest_gemv_kernel<T><<<dim3((unsigned)((n * 32 + 255) / 256), K), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
-                                                                                            lc.nodeGrid, done, lvs(lc));
-    TOPGPU_COUNT_LAUNCH();
+    if (persist) {
+        CoarseVc<T> A{};
+        A.n = nL - 1;
+        for (int l = 1; l < nL; ++l) {
+            DevLevel &d = s->L[l];
+            A.L[l - 1] = CoarseLv<T>{d.g, l < nL - 1 ? ks_packed<T>(d) : nullptr, vr<T>(d), vx<T>(d), vt<T>(d), invd<T>(d), d.flags};
+        }
+        A.omega = omega; A.Ainv = s->Ainv; A.cr = s->cr; A.nC = n; A.nodeGridC = lc.nodeGrid; A.nv = nv;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3((unsigned)coarse_vcycle_ctas<T>(s->numSMs));
+        cfg.blockDim = dim3(kCoarseThreads);
+        cfg.stream = s->st;
+        cfg.attrs = attr; cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, coarse_vcycle_kernel<T>, A, done);
+        TOPGPU_COUNT_LAUNCH();
+    } else {
+        // coarsest direct solve, FP64
+        coarsest_gather_kernel<T><<<dim3(nb256(n), K), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
+        TOPGPU_COUNT_LAUNCH();
+        coarsest_gemv_kernel<T><<<dim3((unsigned)((n * 32 + 255) / 256), K), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
+                                                                                                lc.nodeGrid, done, lvs(lc));
+        TOPGPU_COUNT_LAUNCH();
+    }
     // interpolation leg
-    for (int l = nL - 2; l >= 0; --l) {
+    for (int l = (persist ? 0 : nL - 2); l >= 0; --l) {
         DevLevel &lv = s->L[l], &lcn = s->L[l + 1];
         const T *xc = vt<T>(lcn);
         T *x = vx<T>(lv);
@@ -871,6 +904,14 @@ extern "C" int top_solver_autotune(top_solver *s, int nrep, int64_t flushBytes, 
     const int rc = autotune_l0(s, nrep, flushBytes, msBest2, configs8);
     if (rc != TOP_OK) set_error("top_solver_autotune: failed (%d)", rc);
     return rc;
+}
+
+extern "C" int top_solver_set_coarse_persistent(top_solver *s, int on)
+{
+    if (!s) return TOP_ERR_ARGS;
+    s->coarsePersistent = on != 0;
+    ++s->opGen;                      // captured PCG graphs change
+    return TOP_OK;
 }
 
 extern "C" int top_solver_set_graphs(top_solver *s, int on)

@@ -709,4 +709,197 @@ l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, con
     if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 
+// ---------------------------------------------------------------------------
+// Paired direct-load variant (FP32): two element columns per thread as in
+// l0p_kernel, paired FP32 arithmetic, and the corner nodes of both columns
+// (three rows x two columns) loaded straight from global memory one layer
+// ahead, as in l0d_kernel; node sums double-buffered in shared memory.
+template <typename T, int TYP, int TX, bool MASK, class In, class Out>
+__device__ __forceinline__ void l0q_march(const WalshPairParam<T> &B, const In &in, const Out &out,
+                                          const T *__restrict__ E, const uint8_t *__restrict__ flags,
+                                          const Geom &g, int y0, int x0, int z0, int z1, T E0,
+                                          T *so, double &dot)
+{
+    using P2 = typename PairOf<T>::type;
+    constexpr int NT = TYP * TX;
+    const int tid = threadIdx.x, ty = tid % TYP, tx = tid / TYP;
+    const int PY = g.PY, PL = (int)g.plane;
+    const int ey = y0 - 1 + 2 * ty, ex = x0 - 1 + tx;
+    // node rows ey .. ey+2 and columns ex, ex+1: in [-1, NY] x [-1, NX] (guard slots
+    // included) when the first element column is at most one past the last element;
+    // the third row may then reach NY + 1 only if ey + 1 > NY - 1, i.e. element B void
+    const bool cOn = ey <= g.NY - 1 && ex <= g.NX - 1;
+    const bool row2 = ey + 2 <= g.NY;
+    const int base = cOn ? (int)(g.origin + ey + (int64_t)PY * ex) : 0;
+    const bool outA = ty >= 1 && tx >= 1 && ey < g.NY && ex < g.NX;
+    const bool outB = tx >= 1 && ey + 1 < g.NY && ex < g.NX;
+    auto load = [&](int z, T v[3][2][3]) {      // [comp][column][row]
+#pragma unroll
+        for (int bx = 0; bx < 2; ++bx)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const bool on = cOn && (r < 2 || row2);
+                const int m = base + r + PY * bx + PL * z;
+                uint8_t f = 0;
+                if (MASK && on) f = flags[m];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    T u = on ? in(m, c) : T(0);
+                    if (MASK && (f & (1 << c))) u = T(0);
+                    v[c][bx][r] = u;
+                }
+            }
+    };
+    // (y, x) Walsh transform of a node layer as (A, B) pairs
+    auto walsh_layer = [&](const T v[3][2][3], P2 h[3][4]) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            P2 w[4];
+#pragma unroll
+            for (int bx = 0; bx < 2; ++bx) {
+                w[2 * bx].x = v[c][bx][0]; w[2 * bx].y = v[c][bx][1];
+                w[2 * bx + 1].x = v[c][bx][1]; w[2 * bx + 1].y = v[c][bx][2];
+            }
+            const P2 p0 = padd(w[0], w[1]), m0 = psub(w[0], w[1]);
+            const P2 p1 = padd(w[2], w[3]), m1 = psub(w[2], w[3]);
+            h[c][0] = padd(p0, p1); h[c][1] = padd(m0, m1); h[c][2] = psub(p0, p1); h[c][3] = psub(m0, m1);
+        }
+    };
+    auto eload = [&](int z) {
+        P2 e;
+        e.x = cOn ? E[base + PL * z] : T(0);
+        e.y = cOn ? E[base + 1 + PL * z] : T(0);       // element ey+1 <= NY-1 or a guard slot (E = 0)
+        return e;
+    };
+
+    P2 hb[3][4], gt[3][4];
+    T pre[3][2][3];
+    __syncthreads();                     // the previous range's reads of so are done
+    {
+        T v[3][2][3];
+        load(z0 - 1, v);
+        walsh_layer(v, hb);
+    }
+    load(z0, pre);
+    P2 eNext = eload(z0 - 1);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { gt[c][k].x = T(0); gt[c][k].y = T(0); }
+
+    for (int ez = z0 - 1; ez < z1; ++ez) {
+        P2 U[3][8];
+        {
+            P2 ht[3][4];
+            walsh_layer(pre, ht);
+            if (ez + 2 <= z1) load(ez + 2, pre);
+            const P2 Ee = eNext;
+            if (ez + 1 < z1) eNext = eload(ez + 1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    U[c][k] = pmul(Ee, padd(hb[c][k], ht[c][k]));
+                    U[c][k + 4] = pmul(Ee, psub(hb[c][k], ht[c][k]));
+                    hb[c][k] = ht[c][k];
+                }
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            P2 v[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                P2 acc; acc.x = T(0); acc.y = T(0);
+                bool first = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if ((walsh_pattern(t) >> (3 * c + d)) & 1u) {
+                        const P2 u = U[d][t ^ walsh_axis_bit(d)];
+                        acc = first ? pmul(B.b[t][3 * c + d], u) : pfma(B.b[t][3 * c + d], u, acc);
+                        first = false;
+                    }
+                v[c] = acc;
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) U[c][t ^ walsh_axis_bit(c)] = v[c];
+        }
+        P2 G[3][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                G[c][k] = padd(gt[c][k], padd(U[c][k], U[c][k + 4]));
+                gt[c][k] = psub(U[c][k], U[c][k + 4]);
+            }
+        if (ez < z0) continue;
+        T *buf = so + (ez & 1) * 12 * NT;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const P2 p0 = padd(G[c][0], G[c][1]), m0 = psub(G[c][0], G[c][1]);
+            const P2 p1 = padd(G[c][2], G[c][3]), m1 = psub(G[c][2], G[c][3]);
+            G[c][0] = padd(p0, p1); G[c][1] = padd(m0, m1); G[c][2] = psub(p0, p1); G[c][3] = psub(m0, m1);
+            buf[(0 * 3 + c) * NT + tid] = G[c][1].y;                         // B(1,0) -> (ty+1, tx)
+            P2 x12; x12.x = G[c][2].x; x12.y = G[c][2].y + G[c][3].x;        // A(0,1), B(0,1)+A(1,1) -> (ty, tx+1)
+            reinterpret_cast<P2 *>(buf + 3 * NT)[c * NT + tid] = x12;
+            buf[(9 + c) * NT + tid] = G[c][3].y;                             // B(1,1) -> (ty+1, tx+1)
+        }
+        __syncthreads();
+        T yA[3], yB[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            P2 x12; x12.x = T(0); x12.y = T(0);
+            if (tx >= 1) x12 = reinterpret_cast<const P2 *>(buf + 3 * NT)[c * NT + tid - TYP];
+            const T x0v = ty >= 1 ? buf[(0 * 3 + c) * NT + tid - 1] : T(0);
+            const T x3 = (ty >= 1 && tx >= 1) ? buf[(9 + c) * NT + tid - TYP - 1] : T(0);
+            yA[c] = G[c][0].x + x0v + x12.x + x3;
+            yB[c] = G[c][0].y + G[c][1].x + x12.y;
+        }
+        const int idx = base + PL * ez;
+        if (outA) {
+            if (MASK) {
+                const uint8_t f = flags[idx];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) yA[c] = E0 * in(idx, c);
+            }
+            out(idx, yA, dot);
+        }
+        if (outB) {
+            if (MASK) {
+                const uint8_t f = flags[idx + 1];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) yB[c] = E0 * in(idx + 1, c);
+            }
+            out(idx + 1, yB, dot);
+        }
+    }
+}
+
+template <typename T, int TYP, int TX, class In, class Out>
+__global__ void __launch_bounds__(TYP * TX, WalshPairOcc<T, TYP * TX>::value)
+l0q_kernel(const WalshPairParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
+           const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
+{
+    const int vk = blockIdx.y;          // right-hand side of a batched launch
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
+    __shared__ __align__(16) T so[2 * 12 * TYP * TX];
+    const int tilesY = (g.NY + 2 * TYP - 2) / (2 * TYP - 1);
+    const int64_t total = (int64_t)walsh_pair_tiles(g, TYP, TX) * g.NZ;
+    int64_t a = total * blockIdx.x / gridDim.x;
+    const int64_t b = total * (blockIdx.x + 1) / gridDim.x;
+    double dot = 0.0;
+    while (a < b) {
+        const int tile = (int)(a / g.NZ), z0 = (int)(a % g.NZ);
+        const int z1 = (int)(z0 + (b - a) < g.NZ ? z0 + (b - a) : g.NZ);
+        const int y0 = (tile % tilesY) * (2 * TYP - 1), x0 = (tile / tilesY) * (TX - 1);
+        if (tileMask[tile])
+            l0q_march<T, TYP, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        else
+            l0q_march<T, TYP, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        a += z1 - z0;
+    }
+    if (red.result) block_sum_to<TYP * TX>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
+}
+
 }  // namespace topgpu

@@ -323,6 +323,10 @@ class Solver:
         check(lib().top_solver_super_filter(self._h, src.data_ptr(), out.data_ptr(), mode), "top_solver_super_filter")
         return out
 
+    def set_coarse_persistent(self, on):
+        """V-cycle levels below 0 in one cooperative launch (default) or one launch per step."""
+        check(lib().top_solver_set_coarse_persistent(self._h, int(bool(on))), "top_solver_set_coarse_persistent")
+
     def set_graphs(self, on):
         """Run PCG iterations as captured CUDA graphs (default) or launch by launch."""
         check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
