@@ -119,7 +119,13 @@ __device__ __forceinline__ const int *done_of(const int *done, int k) { return d
 // Functors carry one base pointer per component (set on the host), so device
 // code indexes each component with 32-bit in-array offsets.
 // Batched launches (several right-hand sides) keep the vectors of a level at
-// a fixed stride vs (3 CS); shift(k) moves a functor to vector k.
+// a fixed stride vs (3 CS); shift(k) moves a functor to vector k.  Operand
+// functors (read at every corner load of the product) move their pointers;
+// epilogues (one call per node) add a 32-bit offset k vs to the index of
+// each access instead, so that their many pointers stay kernel parameters
+// rather than occupying registers through the whole kernel (the solver
+// checks that kMax vs fits).  Vectors shared by all right-hand sides (invD)
+// take no offset.
 template <typename P> struct Comp3 {
     P p0, p1, p2;
     Comp3() = default;
@@ -147,50 +153,43 @@ struct JacobiIn {
 // Epilogues: what a node kernel does with y = (K u)(node).
 template <typename T, typename TY>
 struct StoreOut {   // y
-    Comp3<TY *> y; int64_t vs;
-    __host__ __device__ StoreOut(TY *yb, int64_t cs, int64_t vstride = 0) : y(yb, cs), vs(vstride) {}
-    __device__ __forceinline__ StoreOut shift(int k) const { StoreOut o = *this; if (k) o.y = y.shifted(k * vs); return o; }
+    Comp3<TY *> y; int vs, o = 0;
+    __host__ __device__ StoreOut(TY *yb, int64_t cs, int64_t vstride = 0) : y(yb, cs), vs((int)vstride) {}
+    __device__ __forceinline__ StoreOut shift(int k) const { StoreOut r = *this; r.o = k * vs; return r; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) y[c][i] = TY(yv[c]); (void)dot; }
+    { for (int c = 0; c < 3; ++c) y[c][i + o] = TY(yv[c]); (void)dot; }
 };
 template <typename T, typename TU, typename TY>
 struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
-    Comp3<TY *> y; Comp3<const TU *> u; int64_t vs;
-    __host__ __device__ DotStoreOut(TY *yb, const TU *ub, int64_t cs, int64_t vstride = 0) : y(yb, cs), u(ub, cs), vs(vstride) {}
-    __device__ __forceinline__ DotStoreOut shift(int k) const
-    { DotStoreOut o = *this; if (k) { o.y = y.shifted(k * vs); o.u = u.shifted(k * vs); } return o; }
+    Comp3<TY *> y; Comp3<const TU *> u; int vs, o = 0;
+    __host__ __device__ DotStoreOut(TY *yb, const TU *ub, int64_t cs, int64_t vstride = 0) : y(yb, cs), u(ub, cs), vs((int)vstride) {}
+    __device__ __forceinline__ DotStoreOut shift(int k) const { DotStoreOut r = *this; r.o = k * vs; return r; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) { y[c][i] = TY(yv[c]); dot += double(u[c][i]) * double(yv[c]); } }
+    { for (int c = 0; c < 3; ++c) { y[c][i + o] = TY(yv[c]); dot += double(u[c][i + o]) * double(yv[c]); } }
 };
 template <typename T, typename TR, typename TD>
 struct ResidOut {   // d = r - y
-    Comp3<const TR *> r; Comp3<TD *> d; int64_t vsR, vsD;
+    Comp3<const TR *> r; Comp3<TD *> d; int vsR, vsD, oR = 0, oD = 0;
     __host__ __device__ ResidOut(const TR *rb, TD *db, int64_t cs, int64_t vsr = 0, int64_t vsd = -1)
-        : r(rb, cs), d(db, cs), vsR(vsr), vsD(vsd < 0 ? vsr : vsd) {}
-    __device__ __forceinline__ ResidOut shift(int k) const
-    { ResidOut o = *this; if (k) { o.r = r.shifted(k * vsR); o.d = d.shifted(k * vsD); } return o; }
+        : r(rb, cs), d(db, cs), vsR((int)vsr), vsD((int)(vsd < 0 ? vsr : vsd)) {}
+    __device__ __forceinline__ ResidOut shift(int k) const { ResidOut w = *this; w.oR = k * vsR; w.oD = k * vsD; return w; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) d[c][i] = TD(T(r[c][i]) - yv[c]); (void)dot; }
+    { for (int c = 0; c < 3; ++c) d[c][i + oD] = TD(T(r[c][i + oR]) - yv[c]); (void)dot; }
 };
 // z = x + omega*invD.*(r - y), optionally dot += z . r  (post-smoothing)
 template <typename T, typename TR, typename TZ>
 struct PostSmoothOut {
-    Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega; int64_t vs;
+    Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega; int vs, o = 0;
     __host__ __device__ PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om, int64_t vstride = 0)
-        : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om), vs(vstride) {}
-    __device__ __forceinline__ PostSmoothOut shift(int k) const
-    {
-        PostSmoothOut o = *this;
-        if (k) { o.x = x.shifted(k * vs); o.r = r.shifted(k * vs); o.z = z.shifted(k * vs); }
-        return o;
-    }
+        : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om), vs((int)vstride) {}
+    __device__ __forceinline__ PostSmoothOut shift(int k) const { PostSmoothOut w = *this; w.o = k * vs; return w; }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
     {
         for (int c = 0; c < 3; ++c) {
-            const T rv = T(r[c][i]);
-            const T zv = x[c][i] + omega * invD[c][i] * (rv - yv[c]);
-            z[c][i] = TZ(zv);
-            dot += double(zv) * double(r[c][i]);
+            const T rv = T(r[c][i + o]);
+            const T zv = x[c][i + o] + omega * invD[c][i] * (rv - yv[c]);
+            z[c][i + o] = TZ(zv);
+            dot += double(zv) * double(r[c][i + o]);
         }
     }
 };
@@ -571,8 +570,9 @@ restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc
     for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
 }
 
-// one fine node (linear in-plane index q, layer Z) of the prolongation
-template <typename T, int S, typename TR>
+// one fine node (linear in-plane index q, layer Z) of the prolongation;
+// XB: the base omega*invD.*r was stored in xf beforehand (added in place)
+template <typename T, int S, typename TR, bool XB = false>
 __device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geom &gc, T *__restrict__ xf, const Geom &gf,
                                              const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
                                              const T *__restrict__ invD, T omega, int q, int Z)
@@ -602,7 +602,10 @@ __device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geo
                 }
             }
         }
-        if (r) {
+        if (XB) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] += xf[c * gf.cs + i];
+        } else if (r) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) v[c] += omega * invD[c * gf.cs + i] * T(r[c * gf.cs + i]);
         }
@@ -611,8 +614,8 @@ __device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geo
     for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
 }
 // x_f = base + P x_c, base = omega*invD.*r when r != nullptr (the pre-smoothed
-// iterate of the V-cycle, recomputed instead of stored), 0 otherwise.
-template <typename T, int S, typename TR>
+// iterate of the V-cycle, recomputed), the value x_f holds when XB, else 0.
+template <typename T, int S, typename TR, bool XB = false>
 __global__ void __launch_bounds__(kNodeThreads)
 prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
                const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
@@ -624,7 +627,7 @@ prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
     if (done && *done) return;
     xc += vk * vsC; xf += vk * vsF;
     if (r) r += vk * vsR;
-    prolong_node<T, S, TR>(xc, gc, xf, gf, flagsF, r, invD, omega, blockIdx.x * kNodeThreads + threadIdx.x, blockIdx.y);
+    prolong_node<T, S, TR, XB>(xc, gc, xf, gf, flagsF, r, invD, omega, blockIdx.x * kNodeThreads + threadIdx.x, blockIdx.y);
 }
 
 }  // namespace topgpu

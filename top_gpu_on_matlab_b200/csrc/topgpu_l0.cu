@@ -205,13 +205,13 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
 
 // the operand / epilogue pairs of the solver's level-0 products
 using VIdd = VecIn<double, double>;  using VIff = VecIn<float, float>;  using VIfd = VecIn<float, double>;
-using JIdd = JacobiIn<double, double>; using JIfd = JacobiIn<float, double>;
+using JIdd = JacobiIn<double, double>;
 template void l0_op<double, VIdd, StoreOut<double, double>>(top_solver *, const VIdd &, const StoreOut<double, double> &, Reduce, const int *, int);
 template void l0_op<double, JIdd, ResidOut<double, double, double>>(top_solver *, const JIdd &, const ResidOut<double, double, double> &, Reduce, const int *, int);
 template void l0_op<double, VIdd, PostSmoothOut<double, double, double>>(top_solver *, const VIdd &, const PostSmoothOut<double, double, double> &, Reduce, const int *, int);
 template void l0_op<double, VIdd, DotStoreOut<double, double, double>>(top_solver *, const VIdd &, const DotStoreOut<double, double, double> &, Reduce, const int *, int);
 template void l0_op<double, VIdd, ResidOut<double, double, double>>(top_solver *, const VIdd &, const ResidOut<double, double, double> &, Reduce, const int *, int);
-template void l0_op<float, JIfd, ResidOut<float, double, float>>(top_solver *, const JIfd &, const ResidOut<float, double, float> &, Reduce, const int *, int);
+template void l0_op<float, VIff, ResidOut<float, double, float>>(top_solver *, const VIff &, const ResidOut<float, double, float> &, Reduce, const int *, int);
 template void l0_op<float, VIff, PostSmoothOut<float, double, double>>(top_solver *, const VIff &, const PostSmoothOut<float, double, double> &, Reduce, const int *, int);
 template void l0_op<float, VIff, PostSmoothOut<float, double, float>>(top_solver *, const VIff &, const PostSmoothOut<float, double, float> &, Reduce, const int *, int);
 template void l0_op<float, VIfd, DotStoreOut<float, double, double>>(top_solver *, const VIfd &, const DotStoreOut<float, double, double> &, Reduce, const int *, int);

@@ -291,13 +291,19 @@ __global__ void coarsest_gemv_kernel(const double *__restrict__ Ainv, const doub
 // ---- PCG vector kernels (FP64, level-0 grid arrays) ----
 // PCG vector kernels run over whole grid vectors, margins and guard slots
 // included (all zero), as one contiguous range of n = 3 CS values
+// x += lambda p, r -= lambda v, r.r; and, when z1 is set, the FP32 V-cycle's
+// level-0 Jacobi pre-smoothing iterate z1 = omega*invD.*r (stored in the
+// level-0 x vector the V-cycle prolongs into)
+template <typename T>
 __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                                  const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0)
+                                  const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0,
+                                  T *__restrict__ z1, const T *__restrict__ invD, T omega)
 {
     const int vk = blockIdx.y;           // right-hand side; vectors at stride n
     st += vk;
     if (st->done) return;
     x += vk * n; r += vk * n; p += vk * n; v += vk * n;
+    if (z1) z1 += vk * n;
     const Reduce red = red0.at(vk);
     const double lambda = st->rho / st->pv;
     double rr = 0;
@@ -305,9 +311,23 @@ __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r
         x[i] += lambda * p[i];
         const double rv = r[i] - lambda * v[i];
         r[i] = rv;
+        if (z1) z1[i] = omega * invD[i] * T(rv);
         rr += rv * rv;
     }
     block_sum_to<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
+}
+// z1 = omega*invD.*r on whole grid vectors (n = 3 CS values per right-hand
+// side; r at stride vsR, z1 at stride n; invD shared)
+template <typename T, typename TR>
+__global__ void jacobi_base_kernel(const TR *__restrict__ r, const T *__restrict__ invD, T *__restrict__ z1, T omega,
+                                   int64_t n, int64_t vsR, const int *__restrict__ done0)
+{
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    r += vk * vsR; z1 += vk * n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        z1[i] = omega * invD[i] * T(r[i]);
 }
 __global__ void pcg_check_kernel(PcgState *st, int nv)
 {   // TOP_GPU.m:630-649, one thread per right-hand side
@@ -519,8 +539,15 @@ bool coarse_persistent_ok(const top_solver *s)
 // residuals r0 (type TR, grid layout, nv right-hand sides at stride vs0);
 // writes z0 (type TZ, same stride) and, when zr is set, z0 . r0 into zr
 // (per right-hand side: consecutive PcgState's when nv > 1).
+// FP32: the level-0 Jacobi iterate z1 = omega*invD.*r0 is stored in the
+// level-0 x vector first (by this function, or already by the PCG update when
+// z1Ready): the first product reads it once per node instead of converting
+// r0 and recomputing z1 at every corner load, and the prolongation adds onto
+// it.  FP64 evaluates z1 on the fly (its product is bound by the FP64 pipe,
+// not by those loads, and the extra vector pass would cost more).
 template <typename T, typename TR, typename TZ>
-void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, int nv = 1, int64_t vs0 = 0)
+void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, int nv = 1, int64_t vs0 = 0,
+            bool z1Ready = false)
 {
     const int nL = s->nL;
     const T omega = T(s->p.omega);
@@ -528,12 +555,22 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     const unsigned K = (unsigned)nv;
     // levels below 0 as one persistent kernel where their transfers are span 2
     const bool persist = coarse_persistent_ok(s);
+    constexpr bool useZ1 = sizeof(T) == 4;
+    if (useZ1 && !z1Ready) {
+        DevLevel &l0 = s->L[0];
+        const int64_t n0 = lvs(l0), M = kMargin;
+        jacobi_base_kernel<T, TR><<<dim3((unsigned)vec_blocks(n0), K), 256, 0, s->st>>>(r0 - M, invd<T>(l0) - M, vx<T>(l0) - M,
+                                                                                      omega, n0, vs0, done);
+        TOPGPU_COUNT_LAUNCH();
+    }
     // restriction leg
     for (int l = 0; l < (persist ? 1 : nL - 1); ++l) {
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
         const int64_t vs = lvs(lv);
-        if (l == 0)
+        if (l == 0 && useZ1)
+            l0_op<T>(s, VecIn<T, T>{vx<T>(lv), lv.g.cs, vs}, ResidOut<T, TR, T>{r0, d, lv.g.cs, vs0, vs}, none, done, nv);
+        else if (l == 0)
             l0_op<T>(s, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega, vs0}, ResidOut<T, TR, T>{r0, d, lv.g.cs, vs0, vs},
                      none, done, nv);
         else
@@ -576,8 +613,12 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         T *x = vx<T>(lv);
         const int64_t vs = lvs(lv), vsc = lvs(lcn);
         dim3 gr = node_grid(lv.g); gr.z = K;
-        if (l == 0) {
-            if (lcn.span == 4)
+        if (l == 0) {   // x = z1 + P t_c (FP32: x holds z1)
+            if (useZ1 && lcn.span == 4)
+                prolong_kernel<T, 4, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
+            else if (useZ1)
+                prolong_kernel<T, 2, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
+            else if (lcn.span == 4)
                 prolong_kernel<T, 4, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
             else
                 prolong_kernel<T, 2, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
@@ -638,7 +679,9 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         d.g = make_geom(d.ny, d.nx, d.nz);
         d.Ne = M.Ne; d.Nn = M.Nn; d.ng = d.g.cs - 2 * kMargin;
         const int64_t cs = d.g.cs;
-        if (cs >= (int64_t(1) << 31) - 1 || (l > 0 && 300 * cs >= (int64_t(1) << 31))) {
+        // 32-bit in-array indices: the vectors of all right-hand sides (batched
+        // launches index vector k at k * 3 CS) and the packed coarse matrices
+        if ((int64_t)s->kMax * 3 * cs >= (int64_t(1) << 31) - 1 || (l > 0 && 300 * cs >= (int64_t(1) << 31))) {
             set_error("top_solver_create: level %d grid too large for 32-bit in-array indices", l); top_solver_destroy(s); return TOP_ERR_SHAPE;
         }
         // host-side flags, node and element maps
@@ -1237,9 +1280,10 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
         l0_op<double>(s, VecIn<double, double>{xg, cs, nv}, ResidOut<double, double, double>{bGrid, s->r, cs, nv},
                       Reduce{nullptr, nullptr, nullptr}, done, nrhs);
     // z = M r ; rho = z . r ; p = z
-    auto precond_p = [&](cudaStream_t q, int first) {                                         // z = M r, z.r; p = z + beta p
+    // z = M r, z.r; p = z + beta p (z1Ready: the update kernel stored the FP32 V-cycle's Jacobi iterate)
+    auto precond_p = [&](cudaStream_t q, int first) {
         if (z32) {
-            vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv);
+            vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv, !first);
             pcg_p_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first);
         } else {
             vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv);
@@ -1254,7 +1298,12 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     // one PCG iteration (TOP_GPU.m:620-655); every kernel returns at once for a converged right-hand side
     auto iteration = [&](cudaStream_t q) {
         outer_op(s, s->pv, s->v, &s->state->pv, done, nrhs, nv);                             // v = A p, p.v
-        pcg_update_kernel<<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr));
+        if (z32)
+            pcg_update_kernel<float><<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr),
+                                                                l0.x32 - M, l0.invD32 - M, float(s->p.omega));
+        else
+            pcg_update_kernel<double><<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr),
+                                                                 nullptr, nullptr, 0.0);
         TOPGPU_COUNT_LAUNCH();
         pcg_check_kernel<<<1, 32, 0, q>>>(s->state, nrhs);
         TOPGPU_COUNT_LAUNCH();
