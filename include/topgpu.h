@@ -308,8 +308,9 @@ int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);
 int top_solver_set_graphs(top_solver *s, int on);
 /* The V-cycle below level 0 (coarse products, span-2 transfers, coarsest
  * solve) as one persistent cooperative launch with grid-wide barriers
- * (on = 1, default) or one launch per step (0); identical results.  No
- * counterpart in the reference. */
+ * (on = 1) or one launch per step (0, default: inside the captured PCG
+ * iteration graphs the separate launches run faster); identical results.
+ * No counterpart in the reference. */
 int top_solver_set_coarse_persistent(top_solver *s, int on);
 /* Autotuner: times each level-0 kernel configuration (kind, tile shape, CTA
  * count; nrep launches each, L2 flushed by writing flushBytes before every

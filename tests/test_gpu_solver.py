@@ -151,6 +151,7 @@ def test_persistent_coarse_vcycle_matches_per_level_launches(pair, mixed):
     s2.set_density(x)
     s2.assemble()
     r = torch.from_numpy(np.random.default_rng(8).standard_normal(o.level(0).numDOFs)).cuda()
+    s2.set_coarse_persistent(True)
     za = s2.vcycle(r)
     s2.set_coarse_persistent(False)
     zb = s2.vcycle(r)

@@ -150,48 +150,67 @@ struct JacobiIn {
     __device__ __forceinline__ T operator()(int m, int c) const { return omega * invD[c][m] * T(r[c][m]); }
 };
 
-// Epilogues: what a node kernel does with y = (K u)(node).
+// Epilogues: what a node kernel does with y = (K u)(node).  pre(i) loads
+// the node's epilogue inputs (a kernel may issue it well before y is ready,
+// to hide the load latency); apply(i, y, pre, dot) finishes the node;
+// operator() does both at once.
 template <typename T, typename TY>
 struct StoreOut {   // y
     Comp3<TY *> y; int vs, o = 0;
+    struct Pre {};
     __host__ __device__ StoreOut(TY *yb, int64_t cs, int64_t vstride = 0) : y(yb, cs), vs((int)vstride) {}
     __device__ __forceinline__ StoreOut shift(int k) const { StoreOut r = *this; r.o = k * vs; return r; }
-    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) y[c][i + o] = TY(yv[c]); (void)dot; }
+    __device__ __forceinline__ Pre pre(int) const { return Pre{}; }
+    __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &, double &) const
+    { for (int c = 0; c < 3; ++c) y[c][i + o] = TY(yv[c]); }
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
 };
 template <typename T, typename TU, typename TY>
 struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
     Comp3<TY *> y; Comp3<const TU *> u; int vs, o = 0;
+    struct Pre { TU u[3]; };
     __host__ __device__ DotStoreOut(TY *yb, const TU *ub, int64_t cs, int64_t vstride = 0) : y(yb, cs), u(ub, cs), vs((int)vstride) {}
     __device__ __forceinline__ DotStoreOut shift(int k) const { DotStoreOut r = *this; r.o = k * vs; return r; }
-    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) { y[c][i + o] = TY(yv[c]); dot += double(u[c][i + o]) * double(yv[c]); } }
+    __device__ __forceinline__ Pre pre(int i) const { Pre p; for (int c = 0; c < 3; ++c) p.u[c] = u[c][i + o]; return p; }
+    __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &p, double &dot) const
+    { for (int c = 0; c < 3; ++c) { y[c][i + o] = TY(yv[c]); dot += double(p.u[c]) * double(yv[c]); } }
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
 };
 template <typename T, typename TR, typename TD>
 struct ResidOut {   // d = r - y
     Comp3<const TR *> r; Comp3<TD *> d; int vsR, vsD, oR = 0, oD = 0;
+    struct Pre { TR r[3]; };
     __host__ __device__ ResidOut(const TR *rb, TD *db, int64_t cs, int64_t vsr = 0, int64_t vsd = -1)
         : r(rb, cs), d(db, cs), vsR((int)vsr), vsD((int)(vsd < 0 ? vsr : vsd)) {}
     __device__ __forceinline__ ResidOut shift(int k) const { ResidOut w = *this; w.oR = k * vsR; w.oD = k * vsD; return w; }
-    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
-    { for (int c = 0; c < 3; ++c) d[c][i + oD] = TD(T(r[c][i + oR]) - yv[c]); (void)dot; }
+    __device__ __forceinline__ Pre pre(int i) const { Pre p; for (int c = 0; c < 3; ++c) p.r[c] = r[c][i + oR]; return p; }
+    __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &p, double &) const
+    { for (int c = 0; c < 3; ++c) d[c][i + oD] = TD(T(p.r[c]) - yv[c]); }
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
 };
 // z = x + omega*invD.*(r - y), optionally dot += z . r  (post-smoothing)
 template <typename T, typename TR, typename TZ>
 struct PostSmoothOut {
     Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega; int vs, o = 0;
+    struct Pre { TR r[3]; };   // x (the product's own operand, cache-hot) and invD are read in apply
     __host__ __device__ PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om, int64_t vstride = 0)
         : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om), vs((int)vstride) {}
     __device__ __forceinline__ PostSmoothOut shift(int k) const { PostSmoothOut w = *this; w.o = k * vs; return w; }
-    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const
+    __device__ __forceinline__ Pre pre(int i) const
+    {
+        Pre p;
+        for (int c = 0; c < 3; ++c) p.r[c] = r[c][i + o];
+        return p;
+    }
+    __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &p, double &dot) const
     {
         for (int c = 0; c < 3; ++c) {
-            const T rv = T(r[c][i + o]);
-            const T zv = x[c][i + o] + omega * invD[c][i] * (rv - yv[c]);
+            const T zv = x[c][i + o] + omega * invD[c][i] * (T(p.r[c]) - yv[c]);
             z[c][i + o] = TZ(zv);
-            dot += double(zv) * double(r[c][i + o]);
+            dot += double(zv) * double(p.r[c]);
         }
     }
+    __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
 };
 
 // ---------------------------------------------------------------------------

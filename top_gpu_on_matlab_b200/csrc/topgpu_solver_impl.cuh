@@ -42,7 +42,7 @@ struct top_solver {
     cudaStream_t capStream = nullptr; cudaEvent_t capIn = nullptr, capOut = nullptr;
     bool useGraphs = true;
     bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
-    bool coarsePersistent = true;    // levels below 0 of the V-cycle in one cooperative launch
+    bool coarsePersistent = false;   // levels below 0 of the V-cycle in one cooperative launch
     int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
     std::vector<DevLevel> L;

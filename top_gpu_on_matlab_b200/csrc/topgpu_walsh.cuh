@@ -568,7 +568,9 @@ walsh_pair_mask_kernel(const uint8_t *__restrict__ flags, Geom g, uint8_t *__res
 // Direct-load variant of the single-column kernel: each thread reads the
 // four top corner nodes of its element column straight from global memory
 // (L1-cached: every node is read by the four columns around it, two of them
-// in the same warp), one layer ahead in registers.  Only the node sums go
+// in the same warp), one layer ahead in registers; the epilogue's inputs at
+// the thread's output node are loaded at the start of the layer, so their
+// latency hides behind the layer's arithmetic.  Only the node sums go
 // through shared memory, double-buffered, so a layer costs one barrier.
 template <typename T, int TY, int TX, bool MASK, class In, class Out>
 __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, const Out &out,
@@ -614,6 +616,9 @@ __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, 
         for (int k = 0; k < 4; ++k) gt[c][k] = T(0);
 
     for (int ez = z0 - 1; ez < z1; ++ez) {
+        // this layer's epilogue inputs, loaded now and used after the product
+        typename Out::Pre po{};
+        if (nOut && ez >= z0) po = out.pre(base + PL * ez);
         T ht[3][4];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
@@ -676,7 +681,7 @@ __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, 
 #pragma unroll
                 for (int c = 0; c < 3; ++c) if (f & (1 << c)) y[c] = E0 * in(idx, c);
             }
-            out(idx, y, dot);
+            out.apply(idx, y, po, dot);
         }
     }
 }
