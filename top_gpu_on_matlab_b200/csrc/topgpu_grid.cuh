@@ -192,20 +192,20 @@ struct ResidOut {   // d = r - y
 template <typename T, typename TR, typename TZ>
 struct PostSmoothOut {
     Comp3<const T *> x; Comp3<const TR *> r; Comp3<const T *> invD; Comp3<TZ *> z; T omega; int vs, o = 0;
-    struct Pre { TR r[3]; };   // x (the product's own operand, cache-hot) and invD are read in apply
+    struct Pre { T x[3], d[3]; TR r[3]; };
     __host__ __device__ PostSmoothOut(const T *xb, const TR *rb, const T *ib, TZ *zb, int64_t cs, T om, int64_t vstride = 0)
         : x(xb, cs), r(rb, cs), invD(ib, cs), z(zb, cs), omega(om), vs((int)vstride) {}
     __device__ __forceinline__ PostSmoothOut shift(int k) const { PostSmoothOut w = *this; w.o = k * vs; return w; }
     __device__ __forceinline__ Pre pre(int i) const
     {
         Pre p;
-        for (int c = 0; c < 3; ++c) p.r[c] = r[c][i + o];
+        for (int c = 0; c < 3; ++c) { p.x[c] = x[c][i + o]; p.d[c] = invD[c][i]; p.r[c] = r[c][i + o]; }
         return p;
     }
     __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &p, double &dot) const
     {
         for (int c = 0; c < 3; ++c) {
-            const T zv = x[c][i + o] + omega * invD[c][i] * (T(p.r[c]) - yv[c]);
+            const T zv = p.x[c] + omega * p.d[c] * (T(p.r[c]) - yv[c]);
             z[c][i + o] = TZ(zv);
             dot += double(zv) * double(p.r[c]);
         }

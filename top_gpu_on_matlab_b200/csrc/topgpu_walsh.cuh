@@ -245,6 +245,12 @@ __device__ __forceinline__ void l0w_march(const WalshParam<T> &B, const In &in, 
 template <typename T, int NT> struct WalshOcc {
     static constexpr int value = sizeof(T) == 4 ? (NT >= 256 ? 3 : 6) : (NT >= 256 ? 1 : 3);
 };
+// the direct-load kernel keeps its epilogue's prefetched inputs in registers:
+// one resident CTA fewer for an FP32 epilogue that prefetches more than
+// three values (post-smoothing: x, invD, r), which would spill at 80 registers
+template <typename T, int NT, class Out> struct WalshOccD {
+    static constexpr int value = WalshOcc<T, NT>::value - ((sizeof(T) == 4 && sizeof(typename Out::Pre) > 24) ? 1 : 0);
+};
 
 template <typename T, int TY, int TX, class In, class Out>
 __global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
@@ -687,7 +693,7 @@ __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, 
 }
 
 template <typename T, int TY, int TX, class In, class Out>
-__global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
+__global__ void __launch_bounds__(TY * TX, (WalshOccD<T, TY * TX, Out>::value))
 l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
            const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
