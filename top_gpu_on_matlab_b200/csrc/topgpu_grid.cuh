@@ -589,6 +589,98 @@ restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc
     for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
 }
 
+// Span-4 prolongation, four fine y nodes per thread: the fine nodes
+// Y = 4 QY + ry (ry = 0..3) of one fine (X, Z) column share their coarse
+// corner values, which are loaded once.  Per node the weights, skipped
+// zero-weight corners and the order of the sum are those of prolong_node
+// (identical results).  XB: the base is the value xf holds; otherwise
+// omega*invD.*r (or 0 when r is null).
+template <typename T, typename TR, bool XB>
+__global__ void __launch_bounds__(kNodeThreads)
+prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
+                const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
+                const T *__restrict__ invD, T omega, const int *__restrict__ done0,
+                int64_t vsC = 0, int64_t vsF = 0, int64_t vsR = 0)
+{
+    constexpr int S = 4;
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    xc += vk * vsC; xf += vk * vsF;
+    if (r) r += vk * vsR;
+    const int nqy = (gf.NY + S - 1) / S;
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)nqy * gf.NX * gf.NZ) return;
+    const int qy = (int)(k % nqy), X = (int)((k / nqy) % gf.NX), Z = (int)(k / ((int64_t)nqy * gf.NX));
+    const int qx = X / S, rx = X - qx * S, qz = Z / S, rz = Z - qz * S;
+    const T wx[2] = {T(S - rx) / T(S), T(rx) / T(S)};
+    const T wz[2] = {T(S - rz) / T(S), T(rz) / T(S)};
+    // coarse corner values [bz][bx][by][c]; by = 1 is read only where some ry > 0 uses it
+    T cv[2][2][2][3];
+    const bool yNext = S * qy + 1 < gf.NY;
+#pragma unroll
+    for (int bz = 0; bz < 2; ++bz)
+#pragma unroll
+        for (int bx = 0; bx < 2; ++bx)
+#pragma unroll
+            for (int by = 0; by < 2; ++by) {
+                const bool need = (bz == 0 || rz != 0) && (bx == 0 || rx != 0) && (by == 0 || yNext);
+                const int64_t kc = gc.origin + (qy + by) + (int64_t)gc.PY * (qx + bx) + gc.plane * (qz + bz);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) cv[bz][bx][by][c] = need ? xc[c * gc.cs + kc] : T(0);
+            }
+    const int64_t i0 = gf.origin + S * qy + (int64_t)gf.PY * X + gf.plane * Z;
+    // every fine load (flags, base) issued before the arithmetic
+    // (XB: bs is the stored base; else bs = invD and br = r, combined at the
+    // add exactly as prolong_node does)
+    uint8_t fl[S];
+    T bs[S][3], br[S][3];
+#pragma unroll
+    for (int ry = 0; ry < S; ++ry) {
+        const bool on = S * qy + ry < gf.NY;
+        const int64_t i = i0 + ry;
+        fl[ry] = on ? flagsF[i] : uint8_t(0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            bs[ry][c] = !on ? T(0) : XB ? xf[c * gf.cs + i] : r ? invD[c * gf.cs + i] : T(0);
+            br[ry][c] = (!on || XB || !r) ? T(0) : T(r[c * gf.cs + i]);
+        }
+    }
+#pragma unroll
+    for (int ry = 0; ry < S; ++ry) {
+        if (S * qy + ry >= gf.NY) break;
+        const int64_t i = i0 + ry;
+        const T wy[2] = {T(S - ry) / T(S), T(ry) / T(S)};
+        T v[3] = {T(0), T(0), T(0)};
+        if (fl[ry] & kActive) {
+#pragma unroll
+            for (int bz = 0; bz < 2; ++bz) {
+                if (bz && rz == 0) continue;
+#pragma unroll
+                for (int bx = 0; bx < 2; ++bx) {
+                    if (bx && rx == 0) continue;
+#pragma unroll
+                    for (int by = 0; by < 2; ++by) {
+                        if (by && ry == 0) continue;
+                        const T w = wz[bz] * wx[bx] * wy[by];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) v[c] = fma(w, cv[bz][bx][by][c], v[c]);
+                    }
+                }
+            }
+            if (XB) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) v[c] += bs[ry][c];
+            } else if (r) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) v[c] += omega * bs[ry][c] * br[ry][c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
+    }
+}
+
 // one fine node (linear in-plane index q, layer Z) of the prolongation;
 // XB: the base omega*invD.*r was stored in xf beforehand (added in place)
 template <typename T, int S, typename TR, bool XB = false>

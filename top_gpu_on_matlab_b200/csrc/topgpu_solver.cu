@@ -614,12 +614,13 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         const int64_t vs = lvs(lv), vsc = lvs(lcn);
         dim3 gr = node_grid(lv.g); gr.z = K;
         if (l == 0) {   // x = z1 + P t_c (FP32: x holds z1)
+            const dim3 g4((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K);
             if (useZ1 && lcn.span == 4)
-                prolong_kernel<T, 4, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
+                prolong4_kernel<T, TR, true><<<g4, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
             else if (useZ1)
                 prolong_kernel<T, 2, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
             else if (lcn.span == 4)
-                prolong_kernel<T, 4, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
+                prolong4_kernel<T, TR, false><<<g4, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
             else
                 prolong_kernel<T, 2, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
             TOPGPU_COUNT_LAUNCH();
@@ -627,7 +628,8 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
             l0_op<T>(s, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega, vs0}, rz, done, nv);
         } else {
             if (lcn.span == 4)
-                prolong_kernel<T, 4, T><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
+                prolong4_kernel<T, T, false><<<dim3((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K),
+                                                kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             else
                 prolong_kernel<T, 2, T><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             TOPGPU_COUNT_LAUNCH();
@@ -1461,7 +1463,8 @@ extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_
         } break;
         case 5: if (s->nL > 2) {   // level-1 -> level-0 prolongation with the Jacobi base, FP32
             DevLevel &f = s->L[0], &c = s->L[1];
-            if (c.span == 4) prolong_kernel<float, 4, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
+            const dim3 g4((unsigned)(((int64_t)((f.g.NY + 3) / 4) * f.g.NX * f.g.NZ + kNodeThreads - 1) / kNodeThreads));
+            if (c.span == 4) prolong4_kernel<float, double, false><<<g4, kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
             else prolong_kernel<float, 2, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
             TOPGPU_COUNT_LAUNCH();
         } break;
