@@ -270,22 +270,51 @@ __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const in
     if (t >= 3 * Nn) return;
     cr[t] = double(r[(t % 3) * g.cs + nodeGrid[t / 3]]);
 }
+// one warp per row of A^-1 for every right-hand side (up to four per pass
+// over the row); each lane keeps eight loads of its row in flight, and adds
+// its products in the same order as a plain strided loop would
 template <typename T>
-__global__ void coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__ cr, int64_t n,
-                                     T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
-                                     const int *__restrict__ done0, int64_t vs)
+__global__ void __launch_bounds__(256)
+coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__ cr, int64_t n,
+                     T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
+                     const int *__restrict__ done0, int64_t vs, int nv)
 {
-    const int vk = blockIdx.y;
-    const int *done = done_of(done0, vk);
-    if (done && *done) return;
-    cr += vk * n; x += vk * vs;
+    constexpr int U = 8, Q = 4;
     const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= n) return;
-    double s = 0;
-    for (int64_t j = lane; j < n; j += 32) s += Ainv[j + n * row] * cr[j];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) x[(row % 3) * g.cs + nodeGrid[row / 3]] = T(s);
+    const double *a = Ainv + n * row;
+    for (int v0 = 0; v0 < nv; v0 += Q) {
+        bool act[Q];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int *d = done_of(done0, v0 + q);
+            act[q] = v0 + q < nv && !(d && *d);
+            any = any || act[q];
+        }
+        if (!any) continue;                      // uniform in the warp
+        double s[Q] = {0.0, 0.0, 0.0, 0.0};
+        for (int64_t j0 = lane; j0 < n; j0 += 32 * U) {
+            double av[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) av[u] = j0 + 32 * u < n ? a[j0 + 32 * u] : 0.0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (j0 + 32 * u >= n) break;
+#pragma unroll
+                for (int q = 0; q < Q; ++q)
+                    if (act[q]) s[q] = fma(av[u], cr[(v0 + q) * n + j0 + 32 * u], s[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (!act[q]) continue;                // uniform in the warp
+            double sq = s[q];
+            for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
+            if (lane == 0) x[(v0 + q) * vs + (row % 3) * g.cs + nodeGrid[row / 3]] = T(sq);
+        }
+    }
 }
 
 // ---- PCG vector kernels (FP64, level-0 grid arrays) ----
@@ -602,8 +631,8 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         // coarsest direct solve, FP64
         coarsest_gather_kernel<T><<<dim3(nb256(n), K), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
         TOPGPU_COUNT_LAUNCH();
-        coarsest_gemv_kernel<T><<<dim3((unsigned)((n * 32 + 255) / 256), K), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
-                                                                                                lc.nodeGrid, done, lvs(lc));
+        coarsest_gemv_kernel<T><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
+                                                                                   lc.nodeGrid, done, lvs(lc), nv);
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
