@@ -46,6 +46,8 @@ coarse_vcycle_kernel(const CoarseVc<T> A, const int *__restrict__ done0)
     cgs::grid_group grid = cgs::this_grid();
     __shared__ T part[8][3][kCoarseTileX];
     __shared__ int offs[24 * 24];
+    __shared__ double red[kCoarsestThreads / 32][4];
+    static_assert(kCoarseThreads == kCoarsestThreads, "the coarsest rows use the whole CTA");
     const int tid = threadIdx.x, n = tid % kCoarseTileX, i = tid / kCoarseTileX;
     const int64_t nb = gridDim.x, b = blockIdx.x;
     auto vdone = [&](int vk) { const int *d = done_of(done0, vk); return d && *d; };
@@ -78,7 +80,7 @@ coarse_vcycle_kernel(const CoarseVc<T> A, const int *__restrict__ done0)
         }
         grid.sync();
     }
-    // coarsest direct solve: gather the right-hand side, then one warp per row of A^-1
+    // coarsest direct solve: gather the right-hand side, then one CTA per row of A^-1
     {
         const CoarseLv<T> &lc = A.L[NL - 1];
         const int64_t vsc = 3 * lc.g.cs, nC = A.nC;
@@ -89,17 +91,23 @@ coarse_vcycle_kernel(const CoarseVc<T> A, const int *__restrict__ done0)
             A.cr[vk * nC + t] = double(lc.r[vk * vsc + (t % 3) * lc.g.cs + A.nodeGridC[t / 3]]);
         }
         grid.sync();
-        const int wid = tid / 32, lane = tid % 32;
-        for (int64_t rw = b * (kCoarseThreads / 32) + wid; rw < nC * A.nv; rw += nb * (kCoarseThreads / 32)) {
-            const int vk = (int)(rw / nC);
-            const int64_t row = rw % nC;
-            if (vdone(vk)) continue;                              // uniform in the warp
-            const double *c = A.cr + vk * nC;
-            double s = 0;
-            for (int64_t j = lane; j < nC; j += 32) s += A.Ainv[j + nC * row] * c[j];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) lc.t[vk * vsc + (row % 3) * lc.g.cs + A.nodeGridC[row / 3]] = T(s);
-        }
+        for (int64_t row = b; row < nC; row += nb)
+            for (int v0 = 0; v0 < A.nv; v0 += 4) {
+                bool act[4];
+                bool any = false;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    act[q] = v0 + q < A.nv && !vdone(v0 + q);
+                    any = any || act[q];
+                }
+                if (!any) continue;                               // uniform in the CTA
+                double out[4];
+                coarsest_row(A.Ainv + nC * row, A.cr, nC, v0, act, red, out);
+                if (tid == 0)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (act[q]) lc.t[(v0 + q) * vsc + (row % 3) * lc.g.cs + A.nodeGridC[row / 3]] = T(out[q]);
+            }
         grid.sync();
     }
     // interpolation leg

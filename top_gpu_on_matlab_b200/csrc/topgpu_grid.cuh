@@ -589,6 +589,49 @@ restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc
     for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
 }
 
+// One row of the coarsest direct solve, x(row) = A^-1(row, :) c, for the
+// right-hand sides v0 .. v0+3 whose act flag is set (c of right-hand side k
+// at cr + k n).  All kCoarsestThreads threads of the CTA call it: each keeps
+// eight loads of the row in flight, the warps reduce by shuffles and thread
+// 0 adds the warp sums in a fixed order and returns them in out.
+constexpr int kCoarsestThreads = 256;
+__device__ __forceinline__ void coarsest_row(const double *__restrict__ a, const double *__restrict__ cr, int64_t n, int v0,
+                                             const bool act[4], double (*red)[4], double out[4])
+{
+    constexpr int U = 8, NW = kCoarsestThreads / 32;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t j0 = tid; j0 < n; j0 += (int64_t)kCoarsestThreads * U) {
+        double av[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) av[u] = j0 + kCoarsestThreads * u < n ? a[j0 + kCoarsestThreads * u] : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t j = j0 + kCoarsestThreads * u;
+            if (j >= n) break;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (act[q]) s[q] = fma(av[u], cr[(v0 + q) * n + j], s[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) red[wid][q] = s[q];
+    __syncthreads();
+    if (tid == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            double v = red[0][q];
+            for (int w = 1; w < NW; ++w) v += red[w][q];
+            out[q] = v;
+        }
+    __syncthreads();                     // red is reused by the next call
+}
+
 // Span-4 prolongation, four fine y nodes per thread: the fine nodes
 // Y = 4 QY + ry (ry = 0..3) of one fine (X, Z) column share their coarse
 // corner values, which are loaded once.  Per node the weights, skipped

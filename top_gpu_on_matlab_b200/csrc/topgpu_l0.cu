@@ -205,9 +205,7 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
 
 // the operand / epilogue pairs of the solver's level-0 products
 using VIdd = VecIn<double, double>;  using VIff = VecIn<float, float>;  using VIfd = VecIn<float, double>;
-using JIdd = JacobiIn<double, double>;
 template void l0_op<double, VIdd, StoreOut<double, double>>(top_solver *, const VIdd &, const StoreOut<double, double> &, Reduce, const int *, int);
-template void l0_op<double, JIdd, ResidOut<double, double, double>>(top_solver *, const JIdd &, const ResidOut<double, double, double> &, Reduce, const int *, int);
 template void l0_op<double, VIdd, PostSmoothOut<double, double, double>>(top_solver *, const VIdd &, const PostSmoothOut<double, double, double> &, Reduce, const int *, int);
 template void l0_op<double, VIdd, DotStoreOut<double, double, double>>(top_solver *, const VIdd &, const DotStoreOut<double, double, double> &, Reduce, const int *, int);
 template void l0_op<double, VIdd, ResidOut<double, double, double>>(top_solver *, const VIdd &, const ResidOut<double, double, double> &, Reduce, const int *, int);

@@ -270,59 +270,40 @@ __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const in
     if (t >= 3 * Nn) return;
     cr[t] = double(r[(t % 3) * g.cs + nodeGrid[t / 3]]);
 }
-// one warp per row of A^-1 for every right-hand side (up to four per pass
-// over the row); each lane keeps eight loads of its row in flight, and adds
-// its products in the same order as a plain strided loop would
+// one CTA per row of A^-1, every right-hand side (up to four per pass over the row)
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kCoarsestThreads)
 coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__ cr, int64_t n,
                      T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
                      const int *__restrict__ done0, int64_t vs, int nv)
 {
-    constexpr int U = 8, Q = 4;
-    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const double *a = Ainv + n * row;
-    for (int v0 = 0; v0 < nv; v0 += Q) {
-        bool act[Q];
+    __shared__ double red[kCoarsestThreads / 32][4];
+    const int64_t row = blockIdx.x;
+    for (int v0 = 0; v0 < nv; v0 += 4) {
+        bool act[4];
         bool any = false;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
+        for (int q = 0; q < 4; ++q) {
             const int *d = done_of(done0, v0 + q);
             act[q] = v0 + q < nv && !(d && *d);
             any = any || act[q];
         }
-        if (!any) continue;                      // uniform in the warp
-        double s[Q] = {0.0, 0.0, 0.0, 0.0};
-        for (int64_t j0 = lane; j0 < n; j0 += 32 * U) {
-            double av[U];
+        if (!any) continue;                      // uniform in the CTA
+        double out[4];
+        coarsest_row(Ainv + n * row, cr, n, v0, act, red, out);
+        if (threadIdx.x == 0)
 #pragma unroll
-            for (int u = 0; u < U; ++u) av[u] = j0 + 32 * u < n ? a[j0 + 32 * u] : 0.0;
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                if (j0 + 32 * u >= n) break;
-#pragma unroll
-                for (int q = 0; q < Q; ++q)
-                    if (act[q]) s[q] = fma(av[u], cr[(v0 + q) * n + j0 + 32 * u], s[q]);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            if (!act[q]) continue;                // uniform in the warp
-            double sq = s[q];
-            for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-            if (lane == 0) x[(v0 + q) * vs + (row % 3) * g.cs + nodeGrid[row / 3]] = T(sq);
-        }
+            for (int q = 0; q < 4; ++q)
+                if (act[q]) x[(v0 + q) * vs + (row % 3) * g.cs + nodeGrid[row / 3]] = T(out[q]);
     }
 }
 
 // ---- PCG vector kernels (FP64, level-0 grid arrays) ----
 // PCG vector kernels run over whole grid vectors, margins and guard slots
 // included (all zero), as one contiguous range of n = 3 CS values
-// x += lambda p, r -= lambda v, r.r; and, when z1 is set, the FP32 V-cycle's
-// level-0 Jacobi pre-smoothing iterate z1 = omega*invD.*r (stored in the
-// level-0 x vector the V-cycle prolongs into)
+// x += lambda p, r -= lambda v, r.r; and the V-cycle's level-0 Jacobi
+// pre-smoothing iterate z1 = omega*invD.*r in the V-cycle's precision T
+// (stored in the level-0 x vector the V-cycle prolongs into)
 template <typename T>
 __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
                                   const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0,
@@ -332,7 +313,7 @@ __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r
     st += vk;
     if (st->done) return;
     x += vk * n; r += vk * n; p += vk * n; v += vk * n;
-    if (z1) z1 += vk * n;
+    z1 += vk * n;
     const Reduce red = red0.at(vk);
     const double lambda = st->rho / st->pv;
     double rr = 0;
@@ -340,7 +321,7 @@ __global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r
         x[i] += lambda * p[i];
         const double rv = r[i] - lambda * v[i];
         r[i] = rv;
-        if (z1) z1[i] = omega * invD[i] * T(rv);
+        z1[i] = omega * invD[i] * T(rv);
         rr += rv * rv;
     }
     block_sum_to<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
@@ -568,12 +549,11 @@ bool coarse_persistent_ok(const top_solver *s)
 // residuals r0 (type TR, grid layout, nv right-hand sides at stride vs0);
 // writes z0 (type TZ, same stride) and, when zr is set, z0 . r0 into zr
 // (per right-hand side: consecutive PcgState's when nv > 1).
-// FP32: the level-0 Jacobi iterate z1 = omega*invD.*r0 is stored in the
-// level-0 x vector first (by this function, or already by the PCG update when
+// The level-0 Jacobi iterate z1 = omega*invD.*r0 is stored in the level-0 x
+// vector first (by this function, or already by the PCG update when
 // z1Ready): the first product reads it once per node instead of converting
 // r0 and recomputing z1 at every corner load, and the prolongation adds onto
-// it.  FP64 evaluates z1 on the fly (its product is bound by the FP64 pipe,
-// not by those loads, and the extra vector pass would cost more).
+// it.
 template <typename T, typename TR, typename TZ>
 void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, int nv = 1, int64_t vs0 = 0,
             bool z1Ready = false)
@@ -584,8 +564,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     const unsigned K = (unsigned)nv;
     // levels below 0 as one persistent kernel where their transfers are span 2
     const bool persist = coarse_persistent_ok(s);
-    constexpr bool useZ1 = sizeof(T) == 4;
-    if (useZ1 && !z1Ready) {
+    if (!z1Ready) {
         DevLevel &l0 = s->L[0];
         const int64_t n0 = lvs(l0), M = kMargin;
         jacobi_base_kernel<T, TR><<<dim3((unsigned)vec_blocks(n0), K), 256, 0, s->st>>>(r0 - M, invd<T>(l0) - M, vx<T>(l0) - M,
@@ -597,11 +576,8 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
         const int64_t vs = lvs(lv);
-        if (l == 0 && useZ1)
+        if (l == 0)
             l0_op<T>(s, VecIn<T, T>{vx<T>(lv), lv.g.cs, vs}, ResidOut<T, TR, T>{r0, d, lv.g.cs, vs0, vs}, none, done, nv);
-        else if (l == 0)
-            l0_op<T>(s, JacobiIn<T, TR>{r0, invd<T>(lv), lv.g.cs, omega, vs0}, ResidOut<T, TR, T>{r0, d, lv.g.cs, vs0, vs},
-                     none, done, nv);
         else
             coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega, vs}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs, vs},
                          none, done, nv);
@@ -631,8 +607,8 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         // coarsest direct solve, FP64
         coarsest_gather_kernel<T><<<dim3(nb256(n), K), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
         TOPGPU_COUNT_LAUNCH();
-        coarsest_gemv_kernel<T><<<(unsigned)((n * 32 + 255) / 256), 256, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
-                                                                                   lc.nodeGrid, done, lvs(lc), nv);
+        coarsest_gemv_kernel<T><<<(unsigned)n, kCoarsestThreads, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
+                                                                           lc.nodeGrid, done, lvs(lc), nv);
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
@@ -642,16 +618,12 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         T *x = vx<T>(lv);
         const int64_t vs = lvs(lv), vsc = lvs(lcn);
         dim3 gr = node_grid(lv.g); gr.z = K;
-        if (l == 0) {   // x = z1 + P t_c (FP32: x holds z1)
+        if (l == 0) {   // x = z1 + P t_c (x holds z1)
             const dim3 g4((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K);
-            if (useZ1 && lcn.span == 4)
+            if (lcn.span == 4)
                 prolong4_kernel<T, TR, true><<<g4, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
-            else if (useZ1)
-                prolong_kernel<T, 2, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
-            else if (lcn.span == 4)
-                prolong4_kernel<T, TR, false><<<g4, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
             else
-                prolong_kernel<T, 2, TR><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, r0, invd<T>(lv), omega, done, vsc, vs, vs0);
+                prolong_kernel<T, 2, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
             TOPGPU_COUNT_LAUNCH();
             const Reduce rz = zr ? (nv > 1 ? s->redk(zr) : s->red(zr)) : none;
             l0_op<T>(s, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega, vs0}, rz, done, nv);
@@ -1311,13 +1283,13 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
         l0_op<double>(s, VecIn<double, double>{xg, cs, nv}, ResidOut<double, double, double>{bGrid, s->r, cs, nv},
                       Reduce{nullptr, nullptr, nullptr}, done, nrhs);
     // z = M r ; rho = z . r ; p = z
-    // z = M r, z.r; p = z + beta p (z1Ready: the update kernel stored the FP32 V-cycle's Jacobi iterate)
+    // z = M r, z.r; p = z + beta p (z1Ready: the update kernel stored the V-cycle's Jacobi iterate)
     auto precond_p = [&](cudaStream_t q, int first) {
         if (z32) {
             vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv, !first);
             pcg_p_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first);
         } else {
-            vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv);
+            vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv, !first);
             pcg_p_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first);
         }
         TOPGPU_COUNT_LAUNCH();
@@ -1334,7 +1306,7 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
                                                                 l0.x32 - M, l0.invD32 - M, float(s->p.omega));
         else
             pcg_update_kernel<double><<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr),
-                                                                 nullptr, nullptr, 0.0);
+                                                                 l0.x64 - M, l0.invD64 - M, double(s->p.omega));
         TOPGPU_COUNT_LAUNCH();
         pcg_check_kernel<<<1, 32, 0, q>>>(s->state, nrhs);
         TOPGPU_COUNT_LAUNCH();
