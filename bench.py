@@ -321,12 +321,12 @@ def run_kernels_only(args):
     mesh = Mesh(np.ones(SHAPE, bool), control=CONTROL)
     mesh.apply_optcase(1)
     s = Solver(mesh, E0=E0, Emin=EMIN, penal=PENAL, tol=TOL, maxIT=MAXIT, omega=OMEGA, mixed=True)
-    for spec in args.l0 or []:
-        prec, vals = spec.split("=")
-        s.set_l0_kernel(prec == "fp32", *[int(v) for v in vals.split(",")])
     ne = mesh.info()[0]["numElements"]
     s.set_density(torch.full((ne,), V0, dtype=torch.float64, device="cuda"))
     s.assemble()
+    for spec in args.l0 or []:
+        prec, vals = spec.split("=")
+        s.set_l0_kernel(prec == "fp32", *[int(v) for v in vals.split(",")])
     out = {}
     for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32")):
         ms = C.c_double(0)

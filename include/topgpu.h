@@ -297,7 +297,11 @@ int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushByte
  * column's corner nodes directly, kind 4 (FP32 only) combines the two.
  * Tile shapes 16x16 and 16x8.  Kinds 1-4
  * need Ke with the cube's reflection symmetry (always the case for the
- * reference's isotropic voxel); kind 3 is the default then.  get returns
+ * reference's isotropic voxel); kind 3 is the default then.  Kind 5 (FP32
+ * only, 16x8, any Ke) computes the element products on the tensor cores
+ * (tcgen05.mma, TF32 hi/lo split to FP32 accuracy, TMEM accumulator); it is
+ * checked against kind 0 on the model when set (set the densities first;
+ * TOP_ERR_STATE otherwise, TOP_ERR_CUDA if the check fails).  get returns
  * {kind, ty, tx, ctas}.  No counterpart in the reference. */
 int top_solver_set_l0_kernel(top_solver *s, int fp32, int kind, int ty, int tx, int ctas);
 int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);

@@ -4,6 +4,8 @@
 // operand/epilogue combinations the solver uses instantiated here.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
+#include <cstring>
 #include "topgpu_solver_impl.cuh"
 
 namespace topgpu {
@@ -49,6 +51,7 @@ unsigned l0w_ctas(const top_solver *s, const top_solver::L0Kernel &k)
         if constexpr (KIND == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0p_kernel<T, A, B, In, Out>, A * B, 0);
         else if constexpr (KIND == 3) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0d_kernel<T, A, B, In, Out>, A * B, 0);
         else if constexpr (KIND == 4) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0q_kernel<T, A, B, In, Out>, A * B, 0);
+        else if constexpr (KIND == 5) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0t_kernel<A, B, In, Out>, A * B, tc::kSmemBytes);
         else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0w_kernel<T, A, B, In, Out>, A * B, 0);
         if (e != cudaSuccess) n = 1;
         return n > 0 ? n : 1;
@@ -87,6 +90,14 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
                 walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
         TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
+    } else if (k.kind == 5) {        // FP32 only: tensor cores, 16 x 8 element columns
+        if constexpr (sizeof(T) == 4) {
+            static const bool attr = cudaFuncSetAttribute(l0t_kernel<16, 8, In, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          tc::kSmemBytes) == cudaSuccess;
+            (void)attr;
+            l0t_kernel<16, 8, In, Out><<<dim3(l0w_ctas<T, 16, 8, In, Out, 5>(s, k), K), 128, tc::kSmemBytes, s->st>>>(
+                s->tcB, in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done, s->tcErr);
+        }
     } else if (k.kind == 4) {        // FP32 only, as kind 2
         if constexpr (sizeof(T) == 4) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
@@ -112,11 +123,115 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
     TOPGPU_COUNT_LAUNCH();
 }
 
+namespace {
+// round an FP32 value to TF32 (nearest, ties away from zero): 10 mantissa bits
+float tf32_round(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) u = (u + 0x1000u) & 0xFFFFE000u;
+    std::memcpy(&x, &u, 4);
+    return x;
+}
+// Bk for the tensor-core kind: rows n (12 bottom-corner outputs, 12 top,
+// 8 zero) x columns k (12 bottom-corner inputs, 4 zero, 12 top, 4 zero),
+// corner (by, bx) -> slot 3 (by + 2 bx) + c; Ke's local DOF of corner
+// (by, bx, bz), component c is 3 a + c with (cdy, cdx, cdz)(a) = (by, bx, bz)
+int tc_operand(top_solver *s)
+{
+    if (s->tcB) return TOP_OK;
+    int corner[2][2][2];
+    for (int a = 0; a < 8; ++a) corner[cdy(a)][cdx(a)][cdz(a)] = a;
+    auto dof = [&](int j, bool isRow) {        // operand index -> Ke local DOF, or -1 for a pad
+        int bz;
+        if (isRow) { if (j >= 24) return -1; bz = j / 12; j %= 12; }
+        else { if ((j & 15) >= 12) return -1; bz = j >> 4; j &= 15; }
+        const int k4 = j / 3, c = j % 3;
+        return 3 * corner[k4 & 1][k4 >> 1][bz] + c;
+    };
+    std::vector<float> img(2 * tc::kBBytes / 4, 0.f);
+    for (int n = 0; n < tc::kN; ++n)
+        for (int k = 0; k < 32; ++k) {
+            const int r = dof(n, true), c = dof(k, false);
+            const float v = (r < 0 || c < 0) ? 0.f : s->Ke32.k[r * 24 + c];
+            const float hi = tf32_round(v), lo = tf32_round(v - hi);
+            const int o = tc::kmajor_off(n, k, 1024) / 4;
+            img[o] = hi;
+            img[tc::kBBytes / 4 + o] = lo;
+        }
+    s->tcB = s->dalloc<TcOperandB>(1);
+    s->tcErr = s->dalloc<int>(1);
+    if (!s->tcB || !s->tcErr) return TOP_ERR_NOMEM;
+    if (cudaMemcpy(s->tcB, img.data(), sizeof(float) * img.size(), cudaMemcpyHostToDevice) != cudaSuccess) return TOP_ERR_CUDA;
+    return TOP_OK;
+}
+// pseudo-random values at the active nodes (guard slots stay zero)
+__global__ void tc_probe_fill_kernel(float *x, int64_t cs, const int32_t *nodeGrid, int64_t Nn)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * Nn; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t h = (uint32_t)(i * 2654435761u) >> 8;
+        x[(i % 3) * cs + nodeGrid[i / 3]] = float(h) * (1.f / 16777216.f) - 0.5f;
+    }
+}
+__global__ void tc_probe_diff_kernel(const float *a, const float *b, int64_t n, double *out)
+{
+    double dd = 0.0, nn = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double d = double(a[i]) - double(b[i]);
+        dd += d * d; nn += double(b[i]) * double(b[i]);
+    }
+    atomicAdd(out, dd); atomicAdd(out + 1, nn);
+}
+// the tensor-core kind against the dense kernel on one pseudo-random vector,
+// with the model's current moduli: relative 2-norm difference below 1e-5 and
+// no MMA wait gave up
+int tc_selftest(top_solver *s, const top_solver::L0Kernel &cand)
+{
+    DevLevel &l0 = s->L[0];
+    const int64_t n = 3 * l0.g.cs;
+    const int64_t M = kMargin;
+    const Reduce none{nullptr, nullptr, nullptr};
+    top_solver::L0Kernel saved = s->l0k[1];
+    double *dev = s->scal;                   // two scratch scalars
+    cudaMemsetAsync(l0.x32 - M, 0, sizeof(float) * n, s->st);
+    tc_probe_fill_kernel<<<512, 256, 0, s->st>>>(l0.x32, l0.g.cs, l0.nodeGrid, l0.Nn);
+    cudaMemsetAsync(s->tcErr, 0, sizeof(int), s->st);
+    s->l0k[1] = top_solver::L0Kernel{};      // kind 0 (dense), no mask
+    l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr, 1);
+    s->l0k[1] = cand; s->l0k[1].mask = saved.mask;
+    l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{s->z32, l0.g.cs}, none, nullptr, 1);
+    s->l0k[1] = saved;
+    cudaMemsetAsync(dev, 0, 2 * sizeof(double), s->st);
+    tc_probe_diff_kernel<<<256, 256, 0, s->st>>>(s->z32 - M, l0.t32 - M, n, dev);
+    double h[2] = {0, 0};
+    int err = 0;
+    if (cudaMemcpyAsync(h, dev, sizeof(h), cudaMemcpyDeviceToHost, s->st) != cudaSuccess ||
+        cudaMemcpyAsync(&err, s->tcErr, sizeof(int), cudaMemcpyDeviceToHost, s->st) != cudaSuccess ||
+        cudaStreamSynchronize(s->st) != cudaSuccess)
+        return TOP_ERR_CUDA;
+    cudaMemsetAsync(l0.x32 - M, 0, sizeof(float) * n, s->st);
+    if (!err && !(h[1] > 0)) {
+        set_error("level-0 kernel kind 5 is checked on the model: set the element densities first");
+        return TOP_ERR_STATE;
+    }
+    if (err || !(std::sqrt(h[0] / h[1]) < 1e-5)) {
+        set_error("level-0 tensor-core kernel failed its self-test (relative difference %.3e, wait error %d)",
+                  h[1] > 0 ? std::sqrt(h[0] / h[1]) : -1.0, err);
+        return TOP_ERR_CUDA;
+    }
+    return TOP_OK;
+}
+}  // namespace
+
 int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 {
     top_solver::L0Kernel &k = s->l0k[p];
     if (kind == 0) { k.kind = 0; ++s->opGen; return TOP_OK; }
-    if ((kind != 1 && kind != 3 && !((kind == 2 || kind == 4) && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0)
+    if (kind == 5) {                                   // tensor cores: FP32, 16 x 8, any Ke
+        if (p != 1 || ty != 16 || tx != 8 || ctas < 0 || s->super) return TOP_ERR_ARGS;
+        const int rc = tc_operand(s);
+        if (rc != TOP_OK) return rc;
+    } else if ((kind != 1 && kind != 3 && !((kind == 2 || kind == 4) && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0)
         return TOP_ERR_ARGS;
     DevLevel &l0 = s->L[0];
     const int tiles = tiles_of(l0.g, kind, ty, tx);
@@ -136,6 +251,12 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 #undef TOPGPU_MASK_SHAPE
     TOPGPU_COUNT_LAUNCH();
     if (cudaGetLastError() != cudaSuccess) return TOP_ERR_CUDA;
+    if (kind == 5) {
+        top_solver::L0Kernel cand = k;
+        cand.kind = kind; cand.ty = ty; cand.tx = tx; cand.ctas = ctas;
+        const int rc = tc_selftest(s, cand);
+        if (rc != TOP_OK) return rc;
+    }
     k.kind = kind; k.ty = ty; k.tx = tx; k.ctas = ctas;
     ++s->opGen;
     return TOP_OK;
@@ -182,8 +303,8 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
         double tBest = rc == TOP_OK ? time_l0(s, p, nrep, flush, (size_t)flushBytes, a, b) : -1.0;
         if (tBest < 0) { rc = TOP_ERR_CUDA; break; }
         if (s->walshOK) {
-            for (int kind = 1; kind <= 4 && rc == TOP_OK; ++kind) {
-                if ((kind == 2 || kind == 4) && p == 0) continue;
+            for (int kind = 1; kind <= 5 && rc == TOP_OK; ++kind) {
+                if ((kind == 2 || kind == 4 || kind == 5) && p == 0) continue;
                 for (const auto &sh : shapes)
                     for (int m : mults) {
                         const int ctas = m * s->numSMs;

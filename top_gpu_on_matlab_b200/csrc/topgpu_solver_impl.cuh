@@ -7,6 +7,7 @@
 #include <vector>
 #include "topgpu_grid.cuh"
 #include "topgpu_walsh.cuh"
+#include "topgpu_tc.cuh"
 
 namespace topgpu {
 
@@ -50,13 +51,16 @@ struct top_solver {
     topgpu::KeParam<double> Ke64{}; topgpu::KeParam<float> Ke32{};
     // level-0 product: kind 0 = node-centric dense Ke, 1 = Walsh-basis tiles
     // of ty x tx element columns (one per thread), 2 = the same with two
-    // element columns per thread (ty x tx threads), on ctas CTAs (0: as many
-    // as fit at once); per precision, set by top_solver_set_l0_kernel or the
-    // autotuner
+    // element columns per thread (ty x tx threads), 3 = Walsh with direct
+    // loads, 4 = paired direct loads, 5 = tensor cores (FP32, 16 x 8), on
+    // ctas CTAs (0: as many as fit at once); per precision, set by
+    // top_solver_set_l0_kernel or the autotuner
     struct L0Kernel { int kind = 0, ty = 16, tx = 16, ctas = 0; uint8_t *mask = nullptr; };
     int numSMs = 148;
     L0Kernel l0k[2];                 // [0] FP64, [1] FP32
     bool walshOK = false;            // Ke has the cube's reflection symmetry
+    topgpu::TcOperandB *tcB = nullptr;   // kind 5: Ke as TF32 hi/lo tensor-core operand (device)
+    int *tcErr = nullptr;            // kind 5: set by a kernel whose MMA wait gave up
     topgpu::WalshParam<double> W64{}; topgpu::WalshParam<float> W32{};
     topgpu::WalshPairParam<double> WP64{}; topgpu::WalshPairParam<float> WP32{};
     double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
