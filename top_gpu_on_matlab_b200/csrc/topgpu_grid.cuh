@@ -95,7 +95,9 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
 // PCG scalars of one right-hand side; batched solves keep one per vector
 struct PcgState {
     double normB, rho, rhoOld, pv, rr, resnorm, tol;
+    double lam;                      // step length of the last update (x += lam p is applied by the p kernel)
     int its, maxIT, done, status;
+    int xPend, pad_;                 // the last iteration's x update is still to be applied
 };
 constexpr int kStateInts = int(sizeof(PcgState) / sizeof(int));
 constexpr int kStateDoubles = int(sizeof(PcgState) / sizeof(double));

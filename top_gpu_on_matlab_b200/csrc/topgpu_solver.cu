@@ -301,24 +301,23 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__
 // ---- PCG vector kernels (FP64, level-0 grid arrays) ----
 // PCG vector kernels run over whole grid vectors, margins and guard slots
 // included (all zero), as one contiguous range of n = 3 CS values
-// x += lambda p, r -= lambda v, r.r; and the V-cycle's level-0 Jacobi
-// pre-smoothing iterate z1 = omega*invD.*r in the V-cycle's precision T
-// (stored in the level-0 x vector the V-cycle prolongs into)
+// r -= lambda v, r.r, and the V-cycle's level-0 Jacobi pre-smoothing iterate
+// z1 = omega*invD.*r in the V-cycle's precision T (stored in the level-0 x
+// vector the V-cycle prolongs into).  x += lambda p is left to the p kernel,
+// which reads p anyway (pcg_check records lambda and that it is pending).
 template <typename T>
-__global__ void pcg_update_kernel(double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                                  const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0,
+__global__ void pcg_update_kernel(double *__restrict__ r, const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0,
                                   T *__restrict__ z1, const T *__restrict__ invD, T omega)
 {
     const int vk = blockIdx.y;           // right-hand side; vectors at stride n
     st += vk;
     if (st->done) return;
-    x += vk * n; r += vk * n; p += vk * n; v += vk * n;
+    r += vk * n; v += vk * n;
     z1 += vk * n;
     const Reduce red = red0.at(vk);
     const double lambda = st->rho / st->pv;
     double rr = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += lambda * p[i];
         const double rv = r[i] - lambda * v[i];
         r[i] = rv;
         z1[i] = omega * invD[i] * T(rv);
@@ -343,7 +342,9 @@ __global__ void pcg_check_kernel(PcgState *st, int nv)
 {   // TOP_GPU.m:630-649, one thread per right-hand side
     if ((int)threadIdx.x >= nv) return;
     st += threadIdx.x;
-    if (st->done) return;
+    if (st->done) { st->xPend = 0; return; }
+    st->lam = st->rho / st->pv;          // the update kernel's lambda; x += lam p is pending
+    st->xPend = 1;
     st->its += 1;
     const double res = sqrt(st->rr) / st->normB;
     st->resnorm = res;
@@ -352,16 +353,25 @@ __global__ void pcg_check_kernel(PcgState *st, int nv)
     if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
     st->rhoOld = st->rho;
 }
+// p = z + beta p (first: p = z), and the pending x += lambda p of the last
+// update with the old p (also for a right-hand side that has just stopped)
 template <typename TZ>
-__global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, int64_t n, const PcgState *st, int first)
+__global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, int64_t n, const PcgState *st, int first,
+                             double *__restrict__ x)
 {
     const int vk = blockIdx.y;
     st += vk;
-    if (!first && st->done) return;
-    p += vk * n; z += vk * n;
+    const bool xp = !first && st->xPend;
+    const bool upd = first || !st->done;
+    if (!xp && !upd) return;
+    p += vk * n; z += vk * n; x += vk * n;
     const double beta = first ? 0.0 : st->rho / st->rhoOld;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = double(z[i]) + beta * p[i];
+    const double lam = st->lam;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double po = p[i];
+        if (xp) x[i] += lam * po;
+        if (upd) p[i] = double(z[i]) + beta * po;
+    }
 }
 __global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t n, Reduce red0)
 {
@@ -1287,10 +1297,10 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     auto precond_p = [&](cudaStream_t q, int first) {
         if (z32) {
             vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv, !first);
-            pcg_p_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first);
+            pcg_p_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first, xg - M);
         } else {
             vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv, !first);
-            pcg_p_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first);
+            pcg_p_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first, xg - M);
         }
         TOPGPU_COUNT_LAUNCH();
     };
@@ -1302,10 +1312,10 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     auto iteration = [&](cudaStream_t q) {
         outer_op(s, s->pv, s->v, &s->state->pv, done, nrhs, nv);                             // v = A p, p.v
         if (z32)
-            pcg_update_kernel<float><<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr),
+            pcg_update_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                 l0.x32 - M, l0.invD32 - M, float(s->p.omega));
         else
-            pcg_update_kernel<double><<<dim3(VB, K), 256, 0, q>>>(xg - M, s->r - M, s->pv - M, s->v - M, nv, s->state, red(&s->state->rr),
+            pcg_update_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                  l0.x64 - M, l0.invD64 - M, double(s->p.omega));
         TOPGPU_COUNT_LAUNCH();
         pcg_check_kernel<<<1, 32, 0, q>>>(s->state, nrhs);
