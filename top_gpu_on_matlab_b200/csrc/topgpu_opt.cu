@@ -65,7 +65,8 @@ struct OptState {
     double *xd = nullptr, *xPhys = nullptr, *xnew = nullptr, *dc = nullptr, *dv = nullptr, *ce = nullptr, *tmp = nullptr;
     double *U = nullptr;     // [nLoads][3 x cs] grid displacement fields (warm starts)
     OptScalars *sc = nullptr, *hsc = nullptr;
-    double *ocPartials = nullptr; int ocBlocks = 0;
+    double *ocPartials = nullptr; int ocBlocks = 0;   // 2 x ocBlocks block sums
+    double *ocR = nullptr;                              // -dc./dv of the bisection
     int64_t nv = 0;          // design variables (64 per super-element)
     SFilterState sf;         // super-element density filter
 };
@@ -426,20 +427,31 @@ __global__ void div_floor_kernel(const double *__restrict__ a, const double *__r
 // ---- OC update: bisection on the Lagrange multiplier (TOP_GPU.m:233-253) ----
 // One cooperative launch; every block reduces the same per-block partials in
 // the same order, so all blocks take identical branches without a broadcast.
-__device__ __forceinline__ double oc_new(double x, double dc, double dv, double lmid, double move)
+// OC update of one element (TOP_GPU.m:236-244) with r = -dc./dv precomputed:
+// x .* sqrt(r / lmid) is exactly x .* sqrt(-dc ./ dv / lmid) (same operations)
+__device__ __forceinline__ double oc_new(double x, double r, double lmid, double move)
 {
-    const double cand = x * sqrt(-dc / dv / lmid);
+    const double cand = x * sqrt(r / lmid);
     // MATLAB's max/min ignore NaN like fmax/fmin
     return fmax(0.0, fmax(x - move, fmin(1.0, fmin(x + move, cand))));
 }
+// Bisection on the Lagrange multiplier as one cooperative kernel.  r = -dc./dv
+// once per element (into rbuf), then per step: every element's x_new - x,
+// block sums, one grid-wide barrier, and warp 0 of every CTA adds the block
+// sums in the same fixed order (lane-strided, then a shuffle tree) so every
+// CTA takes the same branch; block sums alternate between two buffers, so
+// the next step cannot overwrite what a slower CTA still reads.
 __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc, const double *__restrict__ dv,
-                          int64_t n, double *__restrict__ partials, OptScalars *sc, double move, int maxSteps)
+                          double *__restrict__ rbuf, int64_t n, double *__restrict__ partials, OptScalars *sc,
+                          double move, int maxSteps)
 {
     cg::grid_group grid = cg::this_grid();
     __shared__ double red[8];
+    __shared__ double tot_s;
     const double fval = sc->fval;
     double l1 = 0.0, l2 = 1e9, lmid = 0.5 * (l1 + l2);
     const unsigned nb = gridDim.x;
+    const int64_t stride = (int64_t)nb * blockDim.x;
     auto block_reduce = [&](double v, bool isMax) -> double {
         for (int o = 16; o > 0; o >>= 1) {
             const double w = __shfl_down_sync(0xffffffffu, v, o);
@@ -447,7 +459,7 @@ __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc,
         }
         if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
         __syncthreads();
-        double t = isMax ? 0.0 : 0.0;
+        double t = 0.0;
         if (threadIdx.x == 0) {
             for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t = isMax ? fmax(t, red[i]) : t + red[i];
             red[0] = t;
@@ -457,35 +469,45 @@ __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc,
         __syncthreads();
         return t;
     };
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) rbuf[i] = -dc[i] / dv[i];
     int step = 0;
     while ((l2 - l1) / (l1 + l2) > 1e-6 && step < maxSteps) {
         lmid = 0.5 * (l2 + l1);
         double s = 0;
-        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)nb * blockDim.x)
-            s += oc_new(x[i], dc[i], dv[i], lmid, move) - x[i];
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+            const double xi = x[i];
+            s += oc_new(xi, rbuf[i], lmid, move) - xi;
+        }
         const double bs = block_reduce(s, false);
-        if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+        double *pp = partials + (step & 1) * nb;
+        if (threadIdx.x == 0) pp[blockIdx.x] = bs;
         grid.sync();
-        double tot = 0;
-        for (unsigned b = 0; b < nb; ++b) tot += partials[b];   // same order in every block
-        const double gt = fval + tot / (double)n;
+        if (threadIdx.x < 32) {
+            double t = 0;
+            for (unsigned b = threadIdx.x; b < nb; b += 32) t += pp[b];
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (threadIdx.x == 0) tot_s = t;
+        }
+        __syncthreads();
+        const double gt = fval + tot_s / (double)n;
         if (gt > 0) l1 = lmid; else l2 = lmid;
         ++step;
-        grid.sync();
+        __syncthreads();                 // tot_s is rewritten next step
     }
     // xnew from the last multiplier; change = max|xnew - x|; x = xnew
     double mx = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)nb * blockDim.x) {
-        const double xn = oc_new(x[i], dc[i], dv[i], lmid, move);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double xn = oc_new(x[i], rbuf[i], lmid, move);
         mx = fmax(mx, fabs(xn - x[i]));
         x[i] = xn;
     }
     const double bm = block_reduce(mx, true);
-    if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+    double *pp = partials + (step & 1) * nb;
+    if (threadIdx.x == 0) pp[blockIdx.x] = bm;
     grid.sync();
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         double c = 0;
-        for (unsigned b = 0; b < nb; ++b) c = fmax(c, partials[b]);
+        for (unsigned b = 0; b < nb; ++b) c = fmax(c, pp[b]);
         sc->change = c;
         sc->lmid = lmid;
         sc->pad = (double)step;
@@ -745,8 +767,9 @@ extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, do
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, oc_kernel, 256, 0);
         o.ocBlocks = std::max(1, std::min<int>(nsm * std::max(1, perSM), (int)((nv + 255) / 256)));
-        o.ocPartials = s->dalloc<double>(o.ocBlocks);
-        if (!o.xd || !o.xPhys || !o.xnew || !o.dc || !o.dv || !o.ce || !o.tmp || !o.U || !o.sc || !o.hsc || !o.ocPartials) {
+        o.ocPartials = s->dalloc<double>(2 * (size_t)o.ocBlocks);
+        o.ocR = s->dalloc<double>((size_t)nv);
+        if (!o.xd || !o.xPhys || !o.xnew || !o.dc || !o.dv || !o.ce || !o.tmp || !o.U || !o.sc || !o.hsc || !o.ocPartials || !o.ocR) {
             set_error("top_solver_opt_begin: out of memory"); return TOP_ERR_NOMEM;
         }
     }
@@ -840,8 +863,8 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
         double move = 0.2;
         int maxSteps = 256;
         int64_t n = Ne;
-        double *xa = o.xd; const double *dca = o.dc, *dva = o.dv; double *pa = o.ocPartials; OptScalars *sca = o.sc;
-        void *args[] = {&xa, &dca, &dva, &n, &pa, &sca, &move, &maxSteps};
+        double *xa = o.xd; const double *dca = o.dc, *dva = o.dv; double *ra = o.ocR, *pa = o.ocPartials; OptScalars *sca = o.sc;
+        void *args[] = {&xa, &dca, &dva, &ra, &n, &pa, &sca, &move, &maxSteps};
         CK(cudaLaunchCooperativeKernel((const void *)oc_kernel, dim3(o.ocBlocks), dim3(256), args, 0, st));
         TOPGPU_COUNT_LAUNCH();
     }
