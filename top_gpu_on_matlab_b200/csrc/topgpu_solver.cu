@@ -14,7 +14,9 @@
 #include <vector>
 #include "topgpu_kernels.cuh"
 #include "topgpu_solver_impl.cuh"
+#include "topgpu_dense.cuh"
 #include "topgpu_coarse.cuh"
+#include "topgpu_dense.cuh"
 
 namespace topgpu {
 int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const double *K0,
@@ -174,89 +176,6 @@ __global__ void coarsest_assemble_kernel(const double *__restrict__ KsC, const i
 }
 // ---- dense FP64 Cholesky (lower, col-major, in place), blocked 32 ----
 constexpr int kCb = 32;
-__global__ void chol_diag_kernel(double *A, int64_t n, int64_t k0, int kb, int *status)
-{
-    __shared__ double s[kCb][kCb + 1];
-    const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 32
-    if (tx < kb && ty < kb) s[ty][tx] = A[(k0 + ty) + n * (k0 + tx)];
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        if (tx == 0 && ty == 0) {
-            const double d = s[j][j];
-            if (!(d > 0.0)) { *status = 1; s[j][j] = 1.0; } else s[j][j] = sqrt(d);
-        }
-        __syncthreads();
-        if (tx == 0 && ty > j && ty < kb) s[ty][j] /= s[j][j];
-        __syncthreads();
-        if (ty > j && tx > j && tx <= ty && ty < kb) s[ty][tx] -= s[ty][j] * s[tx][j];
-        __syncthreads();
-    }
-    if (tx < kb && ty < kb && tx <= ty) A[(k0 + ty) + n * (k0 + tx)] = s[ty][tx];
-}
-__global__ void chol_trsm_kernel(double *A, int64_t n, int64_t k0, int kb)
-{   // rows i >= k0+kb: L[i, k0:k0+kb] = A[i, ...] L11^{-T}
-    __shared__ double L11[kCb][kCb + 1];
-    for (int t = threadIdx.x; t < kCb * kCb; t += blockDim.x) {
-        const int r = t % kCb, c = t / kCb;
-        L11[r][c] = (r < kb && c < kb) ? A[(k0 + r) + n * (k0 + c)] : 0.0;
-    }
-    __syncthreads();
-    const int64_t i = k0 + kb + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double x[kCb];
-    for (int j = 0; j < kb; ++j) {
-        double a = A[i + n * (k0 + j)];
-        for (int t = 0; t < j; ++t) a -= x[t] * L11[j][t];
-        x[j] = a / L11[j][j];
-    }
-    for (int j = 0; j < kb; ++j) A[i + n * (k0 + j)] = x[j];
-}
-__global__ void chol_syrk_kernel(double *A, int64_t n, int64_t k0, int kb)
-{   // trailing update of the lower triangle
-    const int64_t j = k0 + kb + (int64_t)blockIdx.y * 16 + threadIdx.y;
-    const int64_t i = k0 + kb + (int64_t)blockIdx.x * 16 + threadIdx.x;
-    if (i >= n || j >= n || j > i) return;
-    double s = 0;
-    for (int t = 0; t < kb; ++t) s += A[i + n * (k0 + t)] * A[j + n * (k0 + t)];
-    A[i + n * j] -= s;
-}
-// W = L^{-1}: one CTA per column j, forward substitution in axpy form on a
-// shared-memory copy of the column (each step: w_i /= L_ii, then the rows
-// below subtract L(:,i) w_i -- coalesced column reads of L).
-__global__ void tri_inv_kernel(const double *__restrict__ L, double *__restrict__ W, int64_t n)
-{
-    extern __shared__ double w[];
-    const int64_t j = blockIdx.x;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) w[i] = (i == j) ? 1.0 : 0.0;
-    __syncthreads();
-    for (int64_t i = j; i < n; ++i) {
-        const double wi = w[i] / L[i + n * i];
-        __syncthreads();
-        for (int64_t r = i + 1 + threadIdx.x; r < n; r += blockDim.x) w[r] -= L[r + n * i] * wi;
-        if (threadIdx.x == 0) w[i] = wi;
-        __syncthreads();
-    }
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) W[i + n * j] = w[i];
-}
-// A^{-1} = W^T W (W = L^{-1} lower), 16x16 output tiles, coalesced column reads
-__global__ void inv_gram_kernel(const double *__restrict__ W, double *__restrict__ Ainv, int64_t n)
-{
-    __shared__ double sA[16][17], sB[16][17];
-    const int tx = threadIdx.x, ty = threadIdx.y;
-    const int64_t i0 = (int64_t)blockIdx.x * 16, j0 = (int64_t)blockIdx.y * 16;
-    double acc = 0;
-    const int64_t k0 = i0 > j0 ? i0 : j0;          // W[k,i] = 0 for k < i
-    for (int64_t kb = k0; kb < n; kb += 16) {
-        const int64_t k = kb + tx;
-        sA[ty][tx] = (k < n && i0 + ty < n) ? W[k + n * (i0 + ty)] : 0.0;
-        sB[ty][tx] = (k < n && j0 + ty < n) ? W[k + n * (j0 + ty)] : 0.0;
-        __syncthreads();
-#pragma unroll
-        for (int t = 0; t < 16; ++t) acc += sA[tx][t] * sB[ty][t];
-        __syncthreads();
-    }
-    if (i0 + tx < n && j0 + ty < n) Ainv[(i0 + tx) + n * (j0 + ty)] = acc;
-}
 // coarsest solve: x_grid = Ainv * r (r gathered from the grid in compact order)
 template <typename T>
 __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const int32_t *__restrict__ nodeGrid,
@@ -911,8 +830,9 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         s->Ac = s->dalloc<double>((size_t)s->nC * s->nC);
         s->Ainv = s->dalloc<double>((size_t)s->nC * s->nC);
         s->Wc = s->dalloc<double>((size_t)s->nC * s->nC);
+        s->Dc = s->dalloc<double>((size_t)((s->nC + kDb - 1) / kDb) * kDb * kDb);
         s->cr = s->dalloc<double>((size_t)s->nC * s->kMax);
-        if (!s->eleCompactC || !s->nodeCompactC || !s->Ac || !s->Ainv || !s->Wc || !s->cr) return fail("out of device memory");
+        if (!s->eleCompactC || !s->nodeCompactC || !s->Ac || !s->Ainv || !s->Wc || !s->Dc || !s->cr) return fail("out of device memory");
         cudaMemcpy(s->eleCompactC, ec.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
         cudaMemcpy(s->nodeCompactC, nc.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
         s->eleCompactC += kMargin; s->nodeCompactC += kMargin;
@@ -1028,6 +948,56 @@ int topgpu::set_modulus_dev(top_solver *s, const double *src, int where, int sim
 extern "C" int top_solver_set_modulus(top_solver *s, const double *E, int where) { return set_modulus_dev(s, E, where, 0); }
 extern "C" int top_solver_set_density(top_solver *s, const double *x, int where) { return set_modulus_dev(s, x, where, 1); }
 
+// Cholesky factor and explicit inverse of the coarsest matrix s->Ac (n x n,
+// column-major): L over Ac's lower triangle, W = L^-1 in s->Wc, A^-1 in
+// s->Ainv (which also serves as the product scratch of the inversion);
+// a non-positive pivot sets s->zeroDone[1]
+namespace {
+void dgemm(cudaStream_t st, bool ta, bool tb, double *C, int64_t ldc, const double *A, int64_t lda, const double *B, int64_t ldb,
+           int64_t M, int64_t N, int64_t K, double alpha, double beta, bool lower, bool kFromTile)
+{
+    if (M <= 0 || N <= 0) return;
+    const dim3 g((unsigned)((M + 63) / 64), (unsigned)((N + 63) / 64));
+    const int lo = lower ? 1 : 0, kt = kFromTile ? 1 : 0;
+    if (!ta && !tb) dgemm_tile_kernel<false, false><<<g, 256, 0, st>>>(C, ldc, A, lda, B, ldb, (int)M, (int)N, (int)K, alpha, beta, lo, kt);
+    else if (!ta && tb) dgemm_tile_kernel<false, true><<<g, 256, 0, st>>>(C, ldc, A, lda, B, ldb, (int)M, (int)N, (int)K, alpha, beta, lo, kt);
+    else dgemm_tile_kernel<true, true><<<g, 256, 0, st>>>(C, ldc, A, lda, B, ldb, (int)M, (int)N, (int)K, alpha, beta, lo, kt);
+}
+}  // namespace
+
+int coarsest_inverse(top_solver *s, cudaStream_t st)
+{
+    const int64_t n = s->nC, nblk = (n + kDb - 1) / kDb;
+    double *A = s->Ac;
+    for (int64_t b = 0; b < nblk; ++b) {
+        const int64_t k0 = b * kDb;
+        const int kb = (int)std::min<int64_t>(kDb, n - k0);
+        double *D = s->Dc + b * kDb * kDb;
+        chol_block_kernel<<<1, 32, 0, st>>>(A, n, k0, kb, D, s->zeroDone + 1);
+        TOPGPU_COUNT_LAUNCH();
+        const int64_t rest = n - k0 - kb;
+        if (rest > 0) {
+            double *L21 = A + (k0 + kb) + n * k0;
+            dgemm(st, false, false, L21, n, L21, n, D, kDb, rest, kb, kb, 1.0, 0.0, false, false);       // A21 L11^-T
+            dgemm(st, false, false, A + (k0 + kb) * (1 + n), n, L21, n, L21, n, rest, rest, kb, -1.0, 1.0, true, false);
+            s->launches += 2;
+        }
+    }
+    CK(cudaMemsetAsync(s->Wc, 0, sizeof(double) * n * n, st));
+    place_dinv_kernel<<<(unsigned)nblk, kDb * kDb, 0, st>>>(s->Dc, s->Wc, n);
+    TOPGPU_COUNT_LAUNCH();
+    for (int64_t hs = kDb; hs < n; hs *= 2) {          // bottom-up levels of the block inversion
+        const int64_t nodes = (n + 2 * hs - 1) / (2 * hs), tiles = (hs + 63) / 64;
+        for (int step = 0; step < 2; ++step) {
+            inv_level_kernel<<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)nodes), 256, 0, st>>>(A, s->Wc, s->Ainv, n, (int)hs, step);
+            TOPGPU_COUNT_LAUNCH();
+        }
+    }
+    dgemm(st, true, true, s->Ainv, n, s->Wc, n, s->Wc, n, n, n, n, 1.0, 0.0, false, true);         // W^T W
+    TOPGPU_COUNT_LAUNCH();
+    return TOP_OK;
+}
+
 extern "C" int top_solver_assemble(top_solver *s)
 {
     if (!s) return TOP_ERR_ARGS;
@@ -1073,30 +1043,7 @@ extern "C" int top_solver_assemble(top_solver *s)
     coarsest_assemble_kernel<<<nb256(n), 256, 0, st>>>(lc.KsC, lc.nodeGrid, s->eleCompactC, s->nodeCompactC, lc.g, lc.Nn, s->Ac);
     TOPGPU_COUNT_LAUNCH();
     CK(cudaMemsetAsync(s->zeroDone, 0, sizeof(int) * 4, st));
-    for (int64_t k0 = 0; k0 < n; k0 += kCb) {
-        const int kb = (int)std::min<int64_t>(kCb, n - k0);
-        chol_diag_kernel<<<1, dim3(kCb, kCb), 0, st>>>(s->Ac, n, k0, kb, s->zeroDone + 1);
-        TOPGPU_COUNT_LAUNCH();
-        const int64_t rest = n - k0 - kb;
-        if (rest > 0) {
-            chol_trsm_kernel<<<(unsigned)((rest + 127) / 128), 128, 0, st>>>(s->Ac, n, k0, kb);
-            TOPGPU_COUNT_LAUNCH();
-            dim3 gs((unsigned)((rest + 15) / 16), (unsigned)((rest + 15) / 16));
-            chol_syrk_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Ac, n, k0, kb);
-            TOPGPU_COUNT_LAUNCH();
-        }
-    }
-    {
-        const size_t sm = sizeof(double) * (size_t)n;   // one column of W per CTA
-        if (sm > 48 * 1024) cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        tri_inv_kernel<<<(unsigned)n, 256, sm, st>>>(s->Ac, s->Wc, n);
-        TOPGPU_COUNT_LAUNCH();
-    }
-    {
-        dim3 gs((unsigned)((n + 15) / 16), (unsigned)((n + 15) / 16));
-        inv_gram_kernel<<<gs, dim3(16, 16), 0, st>>>(s->Wc, s->Ainv, n);
-        TOPGPU_COUNT_LAUNCH();
-    }
+    { const int rc = coarsest_inverse(s, st); if (rc) return rc; }
     CKL();
     int flag = 0;
     CK(cudaMemcpyAsync(&flag, s->zeroDone + 1, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -78,6 +78,7 @@ struct top_solver {
     double *scal = nullptr;          // device scalars for standalone reductions
     int *zeroDone = nullptr;
     int64_t nC = 0; double *Ac = nullptr, *Ainv = nullptr, *Wc = nullptr, *cr = nullptr;
+    double *Dc = nullptr;            // inverses of the coarsest factor's 32 x 32 diagonal blocks
     int32_t *eleCompactC = nullptr, *nodeCompactC = nullptr;
     bool assembled = false;
     // super-element mode (TOP_GPU.m:1101-1104, 721-741): level-0 elements are
