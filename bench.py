@@ -47,7 +47,7 @@ RMIN, FT = 3 ** 0.5, 1
 WORKLOAD = "cantilever_96x192x96_ft1_optimisation_iterations"
 # DRAM bytes (read + write) per launch of the level-0 stiffness products from
 # one ncu capture of this workload (profiles/l0d_kernel_cantilever_96x192x96.md)
-NCU_TRAFFIC = {"l0_f64": 75.2e6, "l0_f32": 31.7e6}
+NCU_TRAFFIC = {"l0_f64": 74.3e6, "l0_f32": 31.7e6}
 
 
 def _env_rank():
