@@ -351,6 +351,14 @@ coarse_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, c
 // threads of a warp read consecutive element slots (one coalesced run), and
 // the eight partial sums of a node are added in a fixed order.
 constexpr int kCoarseTileX = 32;
+// read-only global load kept in program order with the other such loads
+// (so a run of them is issued before the arithmetic that consumes them)
+__device__ __forceinline__ float ld_stream(const float *p)
+{
+    float v;
+    asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
 // packed-entry offsets (entry * CS) of Ks(r, k) of a level, in shared memory
 __device__ __forceinline__ void coarse_offsets(int *offs, const Geom &g, int tid, int nthreads)
 {
@@ -373,17 +381,37 @@ __device__ __forceinline__ double coarse_tile_unit(const In &in, const Out &out,
     if (valid) {
         const int slot = idx - cdy(i) - PY * cdx(i) - PL * cdz(i);
         const T *ke = Ks + slot;
+        // rows 3i+c, columns 3j+d of the packed symmetric Ks (i is warp-uniform:
+        // the offset loads are shared-memory broadcasts)
+        if constexpr (sizeof(T) == 4) {
+            // FP32: the level's grid is small and the product latency-bound, so
+            // all 72 matrix loads of the thread are issued, in order, before any
+            // arithmetic uses them (FP64 keeps the interleaved form: 144
+            // registers of loads in flight would cost it occupancy)
+            T kv[72];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int m = slot + cdy(j) + PY * cdx(j) + PL * cdz(j);
-            const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
-            // row 3i+c, column 3j+d of the packed symmetric Ks (i is warp-uniform:
-            // the offset loads are shared-memory broadcasts)
+            for (int e = 0; e < 72; ++e) kv[e] = ld_stream(ke + offs[(3 * i + e / 24) * 24 + e % 24]);
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+            for (int j = 0; j < 8; ++j) {
+                const int m = slot + cdy(j) + PY * cdx(j) + PL * cdz(j);
+                const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
 #pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    y[c] = fma(__ldg(ke + offs[(3 * i + c) * 24 + 3 * j + d]), u[d], y[c]);
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        y[c] = fma(kv[c * 24 + 3 * j + d], u[d], y[c]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int m = slot + cdy(j) + PY * cdx(j) + PL * cdz(j);
+                const T u[3] = {in(m, 0), in(m, 1), in(m, 2)};
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        y[c] = fma(__ldg(ke + offs[(3 * i + c) * 24 + 3 * j + d]), u[d], y[c]);
+            }
         }
     }
 #pragma unroll
