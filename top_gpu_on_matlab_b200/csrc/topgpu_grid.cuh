@@ -113,6 +113,16 @@ struct Reduce {             // where a fused dot product goes
         return Reduce{partials + k * pStride, counter + k, result ? result + k * rStride : nullptr, pStride, rStride};
     }
 };
+// Programmatic dependent launch: kernels the solver launches back to back
+// start with this.  The wait returns once the preceding kernel of the stream
+// has completed and its writes are visible (at once for an ordinary launch),
+// so nothing below it can read a predecessor's output early; the trigger lets
+// the next kernel's CTAs be scheduled as this kernel's CTAs finish.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 // per-vector done flag of a batched launch (flags in consecutive PcgState's)
 __device__ __forceinline__ const int *done_of(const int *done, int k) { return done ? done + k * kStateInts : nullptr; }
 
@@ -280,6 +290,7 @@ __global__ void __launch_bounds__(kNodeThreads)
 l0_kernel(const KeParam<T> K, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
           const uint8_t *__restrict__ tileFixed, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.z;          // right-hand side of a batched launch
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -308,6 +319,7 @@ template <typename T, class In, class Out>
 __global__ void __launch_bounds__(kNodeThreads)
 coarse_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -435,6 +447,7 @@ template <typename T, class In, class Out>
 __global__ void __launch_bounds__(kCoarseTileX * 8)
 coarse_tile_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.z;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -516,6 +529,7 @@ __global__ void __launch_bounds__(kNodeThreads)
 restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
                 const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsF = 0, int64_t vsC = 0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -539,6 +553,7 @@ __global__ void __launch_bounds__(256)
 restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc, const int *__restrict__ done0,
                   int64_t vsF = 0, int64_t vsT = 0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -566,6 +581,7 @@ __global__ void __launch_bounds__(256)
 restrict_x_kernel(const T *__restrict__ t, int NYc, int NXf, int NXc, int NZf, T *__restrict__ t2, const int *__restrict__ done0,
                   int64_t vsT = 0, int64_t vsT2 = 0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -593,6 +609,7 @@ __global__ void __launch_bounds__(256)
 restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc,
                   const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsT2 = 0, int64_t vsC = 0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -675,6 +692,7 @@ prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
                 const T *__restrict__ invD, T omega, const int *__restrict__ done0,
                 int64_t vsC = 0, int64_t vsF = 0, int64_t vsR = 0)
 {
+    pdl_enter();
     constexpr int S = 4;
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
@@ -806,6 +824,7 @@ prolong_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
                const T *__restrict__ invD, T omega, const int *__restrict__ done0,
                int64_t vsC = 0, int64_t vsF = 0, int64_t vsR = 0)
 {
+    pdl_enter();
     const int vk = blockIdx.z;
     const int *done = done_of(done0, vk);
     if (done && *done) return;

@@ -75,18 +75,18 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
         const T *Kp;
         if constexpr (sizeof(T) == 8) Kp = lv.KsP64; else Kp = lv.KsP32;
         dim3 gr = coarse_tile_grid(lv.g); gr.z = K;
-        coarse_tile_kernel<T, In, Out><<<gr, dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, Kp, lv.g, red, done);
+        launch_k(s, coarse_tile_kernel<T, In, Out>, gr, dim3(kCoarseTileX, 8), 0, s->st, in, out, Kp, lv.g, red, done);
     } else if (k.kind == 1) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
         if (k.ty == A && k.tx == B)                                                                           \
-            l0w_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 1>(s, k), K), A * B, 0, s->st>>>(  \
+            launch_k(s, l0w_kernel<T, A, B, In, Out>, dim3(l0w_ctas<T, A, B, In, Out, 1>(s, k), K), A * B, 0, s->st,   \
                 walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
         TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
     } else if (k.kind == 3) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
         if (k.ty == A && k.tx == B)                                                                           \
-            l0d_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 3>(s, k), K), A * B, 0, s->st>>>(  \
+            launch_k(s, l0d_kernel<T, A, B, In, Out>, dim3(l0w_ctas<T, A, B, In, Out, 3>(s, k), K), A * B, 0, s->st,   \
                 walshparam<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
         TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
@@ -95,14 +95,14 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
             static const bool attr = cudaFuncSetAttribute(l0t_kernel<16, 8, In, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                           tc::kSmemBytes) == cudaSuccess;
             (void)attr;
-            l0t_kernel<16, 8, In, Out><<<dim3(l0w_ctas<T, 16, 8, In, Out, 5>(s, k), K), 128, tc::kSmemBytes, s->st>>>(
+            launch_k(s, l0t_kernel<16, 8, In, Out>, dim3(l0w_ctas<T, 16, 8, In, Out, 5>(s, k), K), 128, tc::kSmemBytes, s->st, 
                 s->tcB, in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done, s->tcErr);
         }
     } else if (k.kind == 4) {        // FP32 only, as kind 2
         if constexpr (sizeof(T) == 4) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
             if (k.ty == A && k.tx == B)                                                                       \
-                l0q_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 4>(s, k), K), A * B, 0, s->st>>>( \
+                launch_k(s, l0q_kernel<T, A, B, In, Out>, dim3(l0w_ctas<T, A, B, In, Out, 4>(s, k), K), A * B, 0, s->st,  \
                     walshpair<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
             TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
@@ -111,13 +111,13 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
         if constexpr (sizeof(T) == 4) {
 #define TOPGPU_LAUNCH_SHAPE(A, B)                                                                             \
             if (k.ty == A && k.tx == B)                                                                       \
-                l0p_kernel<T, A, B, In, Out><<<dim3(l0w_ctas<T, A, B, In, Out, 2>(s, k), K), A * B, 0, s->st>>>( \
+                launch_k(s, l0p_kernel<T, A, B, In, Out>, dim3(l0w_ctas<T, A, B, In, Out, 2>(s, k), K), A * B, 0, s->st,  \
                     walshpair<T>(s), in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done);
             TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
 #undef TOPGPU_LAUNCH_SHAPE
         }
     } else {
-        l0_kernel<T, In, Out><<<dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ, K), kNodeThreads, 0, s->st>>>(
+        launch_k(s, l0_kernel<T, In, Out>, dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ, K), kNodeThreads, 0, s->st, 
             keparam<T>(s), in, out, egrid<T>(s), lv.flags, lv.tileFixed, lv.g, T(s->p.E0), red, done);
     }
     TOPGPU_COUNT_LAUNCH();

@@ -181,6 +181,7 @@ template <typename T>
 __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const int32_t *__restrict__ nodeGrid,
                                        int64_t Nn, double *__restrict__ cr, const int *__restrict__ done0, int64_t vs)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -196,6 +197,7 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__
                      T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
                      const int *__restrict__ done0, int64_t vs, int nv)
 {
+    pdl_enter();
     __shared__ double red[kCoarsestThreads / 32][4];
     const int64_t row = blockIdx.x;
     for (int v0 = 0; v0 < nv; v0 += 4) {
@@ -228,6 +230,7 @@ template <typename T>
 __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0,
                                   T *__restrict__ z1, const T *__restrict__ invD, T omega)
 {
+    pdl_enter();
     const int vk = blockIdx.y;           // right-hand side; vectors at stride n
     st += vk;
     if (st->done) return;
@@ -250,6 +253,7 @@ template <typename T, typename TR>
 __global__ void jacobi_base_kernel(const TR *__restrict__ r, const T *__restrict__ invD, T *__restrict__ z1, T omega,
                                    int64_t n, int64_t vsR, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -258,7 +262,8 @@ __global__ void jacobi_base_kernel(const TR *__restrict__ r, const T *__restrict
         z1[i] = omega * invD[i] * T(r[i]);
 }
 __global__ void pcg_check_kernel(PcgState *st, int nv)
-{   // TOP_GPU.m:630-649, one thread per right-hand side
+{
+    pdl_enter();   // TOP_GPU.m:630-649, one thread per right-hand side
     if ((int)threadIdx.x >= nv) return;
     st += threadIdx.x;
     if (st->done) { st->xPend = 0; return; }
@@ -278,6 +283,7 @@ template <typename TZ>
 __global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, int64_t n, const PcgState *st, int first,
                              double *__restrict__ x)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     st += vk;
     const bool xp = !first && st->xPend;
@@ -421,10 +427,10 @@ void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, c
 {
     DevLevel &lv = s->L[l];
     if (s->coarseLanes) {
-        coarse_kernel<T, In, Out><<<dim3(coarse_blocks(lv.g), (unsigned)nv), kNodeThreads, 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+        launch_k(s, coarse_kernel<T, In, Out>, dim3(coarse_blocks(lv.g), (unsigned)nv), kNodeThreads, 0, s->st, in, out, ks_packed<T>(lv), lv.g, red, done);
     } else {
         dim3 gr = coarse_tile_grid(lv.g); gr.z = (unsigned)nv;
-        coarse_tile_kernel<T, In, Out><<<gr, dim3(kCoarseTileX, 8), 0, s->st>>>(in, out, ks_packed<T>(lv), lv.g, red, done);
+        launch_k(s, coarse_tile_kernel<T, In, Out>, gr, dim3(kCoarseTileX, 8), 0, s->st, in, out, ks_packed<T>(lv), lv.g, red, done);
     }
     TOPGPU_COUNT_LAUNCH();
 }
@@ -445,13 +451,13 @@ void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int n
         const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf, nq = (int64_t)NYc * NXc * lc.g.NZ;
         const int64_t vsS = 3 * (nt + n2);          // scratch per right-hand side
         T *t1 = rscratch<T>(s), *t2 = t1 + 3 * nt;
-        restrict_y_kernel<T, 4><<<dim3((unsigned)((nt + 255) / 256), K), 256, 0, s->st>>>(d, lv.g, t1, NYc, done, lvs(lv), vsS);
+        launch_k(s, restrict_y_kernel<T, 4>, dim3((unsigned)((nt + 255) / 256), K), 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
         TOPGPU_COUNT_LAUNCH();
-        restrict_x_kernel<T, 4><<<dim3((unsigned)((n2 + 255) / 256), K), 256, 0, s->st>>>(t1, NYc, NXf, NXc, NZf, t2, done, vsS, vsS);
+        launch_k(s, restrict_x_kernel<T, 4>, dim3((unsigned)((n2 + 255) / 256), K), 256, 0, s->st, t1, NYc, NXf, NXc, NZf, t2, done, vsS, vsS);
         TOPGPU_COUNT_LAUNCH();
-        restrict_z_kernel<T, 4><<<dim3((unsigned)((nq + 255) / 256), K), 256, 0, s->st>>>(t2, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc));
+        launch_k(s, restrict_z_kernel<T, 4>, dim3((unsigned)((nq + 255) / 256), K), 256, 0, s->st, t2, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc));
     } else {
-        restrict_kernel<T, 2><<<dim3(restrict_blocks<2>(lc.g), K), kNodeThreads, 0, s->st>>>(d, lv.g, rc, lc.g, lc.flags, done,
+        launch_k(s, restrict_kernel<T, 2>, dim3(restrict_blocks<2>(lc.g), K), kNodeThreads, 0, s->st, d, lv.g, rc, lc.g, lc.flags, done,
                                                                                            lvs(lv), lvs(lc));
     }
     TOPGPU_COUNT_LAUNCH();
@@ -496,7 +502,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     if (!z1Ready) {
         DevLevel &l0 = s->L[0];
         const int64_t n0 = lvs(l0), M = kMargin;
-        jacobi_base_kernel<T, TR><<<dim3((unsigned)vec_blocks(n0), K), 256, 0, s->st>>>(r0 - M, invd<T>(l0) - M, vx<T>(l0) - M,
+        launch_k(s, jacobi_base_kernel<T, TR>, dim3((unsigned)vec_blocks(n0), K), 256, 0, s->st, r0 - M, invd<T>(l0) - M, vx<T>(l0) - M,
                                                                                       omega, n0, vs0, done);
         TOPGPU_COUNT_LAUNCH();
     }
@@ -534,9 +540,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     } else {
         // coarsest direct solve, FP64
-        coarsest_gather_kernel<T><<<dim3(nb256(n), K), 256, 0, s->st>>>(vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
+        launch_k(s, coarsest_gather_kernel<T>, dim3(nb256(n), K), 256, 0, s->st, vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
         TOPGPU_COUNT_LAUNCH();
-        coarsest_gemv_kernel<T><<<(unsigned)n, kCoarsestThreads, 0, s->st>>>(s->Ainv, s->cr, n, vt<T>(lc), lc.g,
+        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, 0, s->st, s->Ainv, s->cr, n, vt<T>(lc), lc.g,
                                                                            lc.nodeGrid, done, lvs(lc), nv);
         TOPGPU_COUNT_LAUNCH();
     }
@@ -550,18 +556,17 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         if (l == 0) {   // x = z1 + P t_c (x holds z1)
             const dim3 g4((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K);
             if (lcn.span == 4)
-                prolong4_kernel<T, TR, true><<<g4, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
+                launch_k(s, prolong4_kernel<T, TR, true>, g4, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
             else
-                prolong_kernel<T, 2, TR, true><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
+                launch_k(s, prolong_kernel<T, 2, TR, true>, gr, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
             TOPGPU_COUNT_LAUNCH();
             const Reduce rz = zr ? (nv > 1 ? s->redk(zr) : s->red(zr)) : none;
             l0_op<T>(s, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega, vs0}, rz, done, nv);
         } else {
             if (lcn.span == 4)
-                prolong4_kernel<T, T, false><<<dim3((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K),
-                                                kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
+                launch_k(s, prolong4_kernel<T, T, false>, dim3((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K), kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             else
-                prolong_kernel<T, 2, T><<<gr, kNodeThreads, 0, s->st>>>(xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
+                launch_k(s, prolong_kernel<T, 2, T>, gr, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             TOPGPU_COUNT_LAUNCH();
             coarse_op<T>(s, l, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, T, T>{x, vr<T>(lv), invd<T>(lv), vt<T>(lv), lv.g.cs, omega, vs},
                          none, done, nv);
@@ -1244,10 +1249,10 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     auto precond_p = [&](cudaStream_t q, int first) {
         if (z32) {
             vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv, !first);
-            pcg_p_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z32 - M, nv, s->state, first, xg - M);
+            launch_k(s, pcg_p_kernel<float>, dim3(VB, K), 256, 0, q, s->pv - M, s->z32 - M, nv, s->state, first, xg - M);
         } else {
             vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv, !first);
-            pcg_p_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->pv - M, s->z - M, nv, s->state, first, xg - M);
+            launch_k(s, pcg_p_kernel<double>, dim3(VB, K), 256, 0, q, s->pv - M, s->z - M, nv, s->state, first, xg - M);
         }
         TOPGPU_COUNT_LAUNCH();
     };
@@ -1259,13 +1264,13 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     auto iteration = [&](cudaStream_t q) {
         outer_op(s, s->pv, s->v, &s->state->pv, done, nrhs, nv);                             // v = A p, p.v
         if (z32)
-            pcg_update_kernel<float><<<dim3(VB, K), 256, 0, q>>>(s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
+            launch_k(s, pcg_update_kernel<float>, dim3(VB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                 l0.x32 - M, l0.invD32 - M, float(s->p.omega));
         else
-            pcg_update_kernel<double><<<dim3(VB, K), 256, 0, q>>>(s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
+            launch_k(s, pcg_update_kernel<double>, dim3(VB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                  l0.x64 - M, l0.invD64 - M, double(s->p.omega));
         TOPGPU_COUNT_LAUNCH();
-        pcg_check_kernel<<<1, 32, 0, q>>>(s->state, nrhs);
+        launch_k(s, pcg_check_kernel, 1, 32, 0, q, s->state, nrhs);
         TOPGPU_COUNT_LAUNCH();
         precond_p(q, 0);
     };

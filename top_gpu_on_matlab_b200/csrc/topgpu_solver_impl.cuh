@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdlib>
 #include <vector>
+#include <utility>
 #include "topgpu_grid.cuh"
 #include "topgpu_walsh.cuh"
 #include "topgpu_tc.cuh"
@@ -44,6 +45,7 @@ struct top_solver {
     bool useGraphs = true;
     bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
     bool coarsePersistent = false;   // levels below 0 of the V-cycle in one cooperative launch
+    bool pdl = std::getenv("TOPGPU_NO_PDL") == nullptr;   // programmatic dependent launch on the PCG path
     int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
     std::vector<DevLevel> L;
@@ -111,6 +113,23 @@ struct top_solver {
     Reduce redk(double *result) const { return Reduce{partials, counter, result, nPartials, topgpu::kStateDoubles}; }
     int kMax = 1;                    // right-hand sides the buffers hold (load cases)
 };
+
+namespace topgpu {
+// launch on the PCG path: with s->pdl, the kernel may be scheduled while its
+// predecessor in the stream finishes (it must begin with pdl_enter())
+template <typename... KArgs, typename... Args>
+inline void launch_k(const top_solver *s, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                     Args &&...args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = s->pdl ? 1 : 0;
+    cfg.attrs = at; cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+}  // namespace topgpu
 
 // every kernel launch of the solver is counted on the solver it serves
 #define TOPGPU_COUNT_LAUNCH() (++s->launches)

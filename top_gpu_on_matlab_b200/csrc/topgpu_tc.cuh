@@ -263,6 +263,7 @@ l0t_kernel(const TcOperandB *__restrict__ Bimg, In in0, Out out0, const float *_
            const uint8_t *__restrict__ flags, const uint8_t *__restrict__ tileMask, Geom g, float E0,
            Reduce red0, const int *__restrict__ done0, int *err)
 {
+    pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;

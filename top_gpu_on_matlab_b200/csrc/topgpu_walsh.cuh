@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(TY * TX, WalshOcc<T, TY * TX>::value)
 l0w_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
            const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;          // right-hand side of a batched launch
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -527,6 +528,7 @@ __global__ void __launch_bounds__(TYP * TX, WalshPairOcc<T, TYP * TX>::value)
 l0p_kernel(const WalshPairParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
            const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;          // right-hand side of a batched launch
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -697,6 +699,7 @@ __global__ void __launch_bounds__(TY * TX, (WalshOccD<T, TY * TX, Out>::value))
 l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
            const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;          // right-hand side of a batched launch
     const int *done = done_of(done0, vk);
     if (done && *done) return;
@@ -890,6 +893,7 @@ __global__ void __launch_bounds__(TYP * TX, WalshPairOcc<T, TYP * TX>::value)
 l0q_kernel(const WalshPairParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
            const uint8_t *__restrict__ tileMask, Geom g, T E0, Reduce red0, const int *__restrict__ done0)
 {
+    pdl_enter();
     const int vk = blockIdx.y;          // right-hand side of a batched launch
     const int *done = done_of(done0, vk);
     if (done && *done) return;
