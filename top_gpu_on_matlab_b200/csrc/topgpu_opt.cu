@@ -35,6 +35,8 @@ struct FilterState {
     double *invD = nullptr;  // Jacobi of the filter operator, node grid
     double *rhs = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *v = nullptr, *eg = nullptr;
     PcgState *st = nullptr;
+    cudaGraphExec_t chunk = nullptr;   // kChunk filter-PCG iterations as one graph (built on first use)
+    int64_t chunkNodes = 0;
 };
 
 struct AdjState {
@@ -537,6 +539,7 @@ int ensure_state(top_solver *s)
 
 void topgpu::free_opt_state(top_solver *s)
 {
+    if (s->filterState && filt(s).chunk) cudaGraphExecDestroy(filt(s).chunk);
     delete reinterpret_cast<FilterState *>(s->filterState);
     if (s->optState && opt(s).sf.h) cudaFree(opt(s).sf.h);
     delete reinterpret_cast<OptState *>(s->optState);
@@ -562,6 +565,7 @@ extern "C" int top_solver_filter_setup(top_solver *s, double rMin)
         }
     }
     filter_kernel_matrix(rMin, f.KEF.k);
+    if (f.chunk) { cudaGraphExecDestroy(f.chunk); f.chunk = nullptr; }   // the operator is a captured argument
     filter_activity_kernel<<<nb256(l0.Ne), 256, 0, s->st>>>(l0.eleGrid, l0.Ne, f.act);
     TOPGPU_COUNT_LAUNCH();
     filter_diag_kernel<<<dim3(l0.g.nbx, l0.g.NZ), kNodeThreads, 0, s->st>>>(f.KEF, f.act, l0.g, l0.flags, f.invD);
@@ -596,19 +600,50 @@ static int filter_apply(top_solver *s, const double *src, double *tar, int *itsO
     TOPGPU_COUNT_LAUNCH();
     const int *done = &f.st->done;
     const int chunk = 8;
+    // one filter-PCG iteration; every kernel returns at once after convergence
+    auto iteration = [&](cudaStream_t q) {
+        filter_apply_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, q>>>(f.KEF, f.act, f.p, f.v, g, s->red(&f.st->pv), done);
+        TOPGPU_COUNT_LAUNCH();
+        fpcg_update_kernel<<<VB, 256, 0, q>>>(f.x, f.r, f.z, f.p, f.v, f.invD, ng, f.st, s->red(&f.st->rr));
+        TOPGPU_COUNT_LAUNCH();
+        fpcg_check_kernel<<<1, 1, 0, q>>>(f.st);
+        TOPGPU_COUNT_LAUNCH();
+        fpcg_zr_kernel<<<VB, 256, 0, q>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
+        TOPGPU_COUNT_LAUNCH();
+        fpcg_p_kernel<<<VB, 256, 0, q>>>(f.p, f.z, ng, f.st);
+        TOPGPU_COUNT_LAUNCH();
+    };
+    // a chunk of iterations as one CUDA graph (its buffers and operator are
+    // fixed until the next filter setup), captured on the solver's capture
+    // stream and launched there after the caller's stream
+    if (s->useGraphs && !f.chunk) {
+        if (!s->capStream) {
+            CK(cudaStreamCreateWithFlags(&s->capStream, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&s->capIn, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&s->capOut, cudaEventDisableTiming));
+        }
+        const int64_t before = s->launches;
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(s->capStream, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < chunk; ++k) iteration(s->capStream);
+        cudaError_t e = cudaStreamEndCapture(s->capStream, &graph);
+        f.chunkNodes = s->launches - before;
+        s->launches = before;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&f.chunk, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        CK(e);
+    }
     PcgState h{};
     for (int it0 = 0; it0 < s->p.maxIT; it0 += chunk) {
-        for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) {
-            filter_apply_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, st>>>(f.KEF, f.act, f.p, f.v, g, s->red(&f.st->pv), done);
-            TOPGPU_COUNT_LAUNCH();
-            fpcg_update_kernel<<<VB, 256, 0, st>>>(f.x, f.r, f.z, f.p, f.v, f.invD, ng, f.st, s->red(&f.st->rr));
-            TOPGPU_COUNT_LAUNCH();
-            fpcg_check_kernel<<<1, 1, 0, st>>>(f.st);
-            TOPGPU_COUNT_LAUNCH();
-            fpcg_zr_kernel<<<VB, 256, 0, st>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
-            TOPGPU_COUNT_LAUNCH();
-            fpcg_p_kernel<<<VB, 256, 0, st>>>(f.p, f.z, ng, f.st);
-            TOPGPU_COUNT_LAUNCH();
+        if (f.chunk && s->useGraphs && it0 + chunk <= s->p.maxIT) {
+            CK(cudaEventRecord(s->capIn, st));
+            CK(cudaStreamWaitEvent(s->capStream, s->capIn, 0));
+            CK(cudaGraphLaunch(f.chunk, s->capStream));
+            CK(cudaEventRecord(s->capOut, s->capStream));
+            CK(cudaStreamWaitEvent(st, s->capOut, 0));
+            s->launches += f.chunkNodes;
+        } else {
+            for (int k = 0; k < chunk && it0 + k < s->p.maxIT; ++k) iteration(st);
         }
         CK(cudaMemcpyAsync(&h, f.st, sizeof(PcgState), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
