@@ -158,6 +158,40 @@ def test_persistent_coarse_vcycle_matches_per_level_launches(pair, mixed):
     assert torch.equal(za, zb)
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_dependent_launch_changes_no_result(pair, mixed, monkeypatch):
+    """programmatic dependent launch only lets a kernel be scheduled early; it
+    waits for its predecessor before reading anything: identical solutions"""
+    o, s, m, _ = pair
+    from top_gpu_on_matlab_b200.fea import Solver
+    x = torch.from_numpy(0.2 + 0.7 * np.random.default_rng(4).random(o.level(0).numElements)).cuda()
+    out = []
+    for off in (False, True):
+        if off:
+            monkeypatch.setenv("TOPGPU_NO_PDL", "1")
+        s2 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-8, maxIT=800, omega=0.6, mixed=mixed)
+        s2.set_density(x)
+        s2.assemble()
+        U, its, _ = s2.pcg(0)
+        r = torch.from_numpy(np.random.default_rng(8).standard_normal(o.level(0).numDOFs)).cuda()
+        out.append((U, its, s2.vcycle(r)))
+    assert out[0][1] == out[1][1] and torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][2], out[1][2])
+
+
+def test_filter_graph_matches_launches(pair):
+    """the PDE filter's PCG chunks as CUDA graphs give the launch-by-launch result bit for bit"""
+    o, s, m, _ = pair
+    from top_gpu_on_matlab_b200.fea import Solver
+    s2 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6)
+    s2.filter_setup(2.0)
+    src = torch.from_numpy(np.random.default_rng(6).random(o.level(0).numElements)).cuda()
+    ya, ia = s2.filter(src)
+    yb, ib = s2.filter(src)                   # the graph built by the first call, replayed
+    s2.set_graphs(False)
+    yc, ic = s2.filter(src)
+    assert ia == ib == ic and torch.equal(ya, yb) and torch.equal(ya, yc)
+
+
 def test_pcg_warm_start_and_unit_compliance(pair):
     _smooth_only(pair)
     o, s, _, _ = pair
