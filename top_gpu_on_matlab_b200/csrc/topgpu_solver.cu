@@ -1195,7 +1195,9 @@ static cudaError_t pcg_graph_prepare(top_solver *s, const double *b, double *x, 
     cudaGraph_t graph = nullptr;
     e = cudaStreamBeginCapture(s->capStream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
+        s->inCapture = true;
         body(s->capStream);
+        s->inCapture = false;
         e = cudaStreamEndCapture(s->capStream, &graph);
     }
     s->st = user;

@@ -46,6 +46,7 @@ struct top_solver {
     bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
     bool coarsePersistent = false;   // levels below 0 of the V-cycle in one cooperative launch
     bool pdl = std::getenv("TOPGPU_NO_PDL") == nullptr;   // programmatic dependent launch on the PCG path
+    bool inCapture = false;          // launches are being captured into a graph (no dependent launch there)
     int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
     std::vector<DevLevel> L;
@@ -115,8 +116,10 @@ struct top_solver {
 };
 
 namespace topgpu {
-// launch on the PCG path: with s->pdl, the kernel may be scheduled while its
-// predecessor in the stream finishes (it must begin with pdl_enter())
+// launch on the PCG path: with s->pdl, outside graph capture, the kernel may
+// be scheduled while its predecessor in the stream finishes (it must begin
+// with pdl_enter()); captured graphs keep plain dependencies (measured: the
+// dependent launch gains nothing inside them)
 template <typename... KArgs, typename... Args>
 inline void launch_k(const top_solver *s, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
                      Args &&...args)
@@ -125,7 +128,7 @@ inline void launch_k(const top_solver *s, void (*kernel)(KArgs...), dim3 grid, d
     cfg.gridDim = grid; cfg.blockDim = block; cfg.dynamicSmemBytes = smem; cfg.stream = st;
     cudaLaunchAttribute at[1];
     at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = s->pdl ? 1 : 0;
+    at[0].val.programmaticStreamSerializationAllowed = (s->pdl && !s->inCapture) ? 1 : 0;
     cfg.attrs = at; cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
