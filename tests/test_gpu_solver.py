@@ -178,6 +178,28 @@ def test_dependent_launch_changes_no_result(pair, mixed, monkeypatch):
     assert out[0][1] == out[1][1] and torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][2], out[1][2])
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_vector_transfers_change_no_result(pair, mixed, monkeypatch):
+    """span-4 restriction / prolongation with four fine y slots per aligned
+    vector access give the per-slot kernels' results bit for bit (every model
+    here coarsens by 4 first, with a ragged last y group)"""
+    o, s, m, _ = pair
+    from top_gpu_on_matlab_b200.fea import Solver
+    assert o.level(1).spanWidth == 4
+    x = torch.from_numpy(0.2 + 0.7 * np.random.default_rng(5).random(o.level(0).numElements)).cuda()
+    out = []
+    for off in (False, True):
+        if off:
+            monkeypatch.setenv("TOPGPU_NO_VEC4", "1")
+        s2 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-8, maxIT=800, omega=0.6, mixed=mixed)
+        s2.set_density(x)
+        s2.assemble()
+        U, its, _ = s2.pcg(0)
+        r = torch.from_numpy(np.random.default_rng(9).standard_normal(o.level(0).numDOFs)).cuda()
+        out.append((U, its, s2.vcycle(r)))
+    assert out[0][1] == out[1][1] and torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][2], out[1][2])
+
+
 def test_filter_graph_matches_launches(pair):
     """the PDE filter's PCG chunks as CUDA graphs give the launch-by-launch result bit for bit"""
     o, s, m, _ = pair

@@ -10,6 +10,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <initializer_list>
 #include "topgpu_internal.h"
 
 namespace topgpu {
@@ -371,6 +372,38 @@ __device__ __forceinline__ float ld_stream(const float *p)
     asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
     return v;
 }
+// four consecutive values at a 16-byte aligned address (one float4 or two
+// double2 accesses).  Grid vectors qualify at every slot Y = 4 m of a column:
+// the pitch, plane, origin and component stride are multiples of 4 and the
+// arrays start 16-byte aligned (vec4_ok checks it on the host).
+__device__ __forceinline__ void ld4(const float *p, float v[4])
+{
+    const float4 q = *reinterpret_cast<const float4 *>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double *p, double v[4])
+{
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void st4(float *p, const float v[4])
+{
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double *p, const double v[4])
+{
+    reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+inline bool vec4_ok(const Geom &g, std::initializer_list<const void *> ptrs, std::initializer_list<int64_t> strides)
+{
+    if ((g.PY | g.plane | g.origin | g.cs) & 3) return false;
+    for (const void *p : ptrs)
+        if (p && (reinterpret_cast<uintptr_t>(p) & 15)) return false;
+    for (int64_t v : strides)
+        if (v & 3) return false;
+    return true;
+}
 // packed-entry offsets (entry * CS) of Ks(r, k) of a level, in shared memory
 __device__ __forceinline__ void coarse_offsets(int *offs, const Geom &g, int tid, int nthreads)
 {
@@ -547,12 +580,16 @@ inline unsigned restrict_blocks(const Geom &gc)
 // pass: pass A folds the fine y taps, t[c][QY][X][Z] = sum_oy w(oy)
 // r_f[c][S QY + oy][X][Z] (dense NYc x NXf x NZf per component), passes B and
 // C fold x and z.  Same weights and clipping as restrict_kernel; every pass
-// reads runs of consecutive QY.
-template <typename T, int S>
+// reads runs of consecutive QY.  V4 (S = 4): the seven taps 4 QY - 3 ..
+// 4 QY + 3 come from two aligned four-value loads per component (slots
+// 4 QY - 4 .. 4 QY + 3 of the column; the first and any past NY are not used),
+// summed in the same order.
+template <typename T, int S, bool V4 = false>
 __global__ void __launch_bounds__(256)
 restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc, const int *__restrict__ done0,
                   int64_t vsF = 0, int64_t vsT = 0)
 {
+    static_assert(!V4 || S == 4, "vector taps need span 4");
     pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
@@ -564,13 +601,31 @@ restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc,
     const int QY = (int)(k % NYc), X = (int)((k / NYc) % gf.NX), Z = (int)(k / ((int64_t)NYc * gf.NX));
     const int64_t base = gf.origin + (int64_t)gf.PY * X + gf.plane * Z;
     T acc[3] = {T(0), T(0), T(0)};
+    if constexpr (V4) {
+        T lo[3][4], hi[3][4];
 #pragma unroll
-    for (int oy = -(S - 1); oy <= S - 1; ++oy) {
-        const int Y = S * QY + oy;
-        if (Y < 0 || Y >= gf.NY) continue;
-        const T w = T(S - (oy < 0 ? -oy : oy)) / T(S);
+        for (int c = 0; c < 3; ++c) {
+            const T *p = rf + c * gf.cs + base + S * QY;
+            ld4(p - 4, lo[c]);
+            ld4(p, hi[c]);
+        }
 #pragma unroll
-        for (int c = 0; c < 3; ++c) acc[c] = fma(w, rf[c * gf.cs + base + Y], acc[c]);
+        for (int oy = -(S - 1); oy <= S - 1; ++oy) {
+            const int Y = S * QY + oy;
+            if (Y < 0 || Y >= gf.NY) continue;
+            const T w = T(S - (oy < 0 ? -oy : oy)) / T(S);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[c] = fma(w, oy < 0 ? lo[c][4 + oy] : hi[c][oy], acc[c]);
+        }
+    } else {
+#pragma unroll
+        for (int oy = -(S - 1); oy <= S - 1; ++oy) {
+            const int Y = S * QY + oy;
+            if (Y < 0 || Y >= gf.NY) continue;
+            const T w = T(S - (oy < 0 ? -oy : oy)) / T(S);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[c] = fma(w, rf[c * gf.cs + base + Y], acc[c]);
+        }
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) t[c * nt + k] = acc[c];
@@ -684,8 +739,11 @@ __device__ __forceinline__ void coarsest_row(const double *__restrict__ a, const
 // corner values, which are loaded once.  Per node the weights, skipped
 // zero-weight corners and the order of the sum are those of prolong_node
 // (identical results).  XB: the base is the value xf holds; otherwise
-// omega*invD.*r (or 0 when r is null).
-template <typename T, typename TR, bool XB>
+// omega*invD.*r (or 0 when r is null).  V4: the four fine slots of a thread
+// are read as one aligned vector per array (slots past NY are y padding of
+// the same column, read but not used) and written as one where all four are
+// grid nodes (per node otherwise, so padding is never written).
+template <typename T, typename TR, bool XB, bool V4 = false>
 __global__ void __launch_bounds__(kNodeThreads)
 prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
                 const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
@@ -726,20 +784,36 @@ prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
     // add exactly as prolong_node does)
     uint8_t fl[S];
     T bs[S][3], br[S][3];
-#pragma unroll
-    for (int ry = 0; ry < S; ++ry) {
-        const bool on = S * qy + ry < gf.NY;
-        const int64_t i = i0 + ry;
-        fl[ry] = on ? flagsF[i] : uint8_t(0);
+    if constexpr (V4) {
+        static_assert(S == 4, "vector slots need span 4");
+        const uchar4 f4 = *reinterpret_cast<const uchar4 *>(flagsF + i0);
+        fl[0] = f4.x; fl[1] = f4.y; fl[2] = f4.z; fl[3] = f4.w;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            bs[ry][c] = !on ? T(0) : XB ? xf[c * gf.cs + i] : r ? invD[c * gf.cs + i] : T(0);
-            br[ry][c] = (!on || XB || !r) ? T(0) : T(r[c * gf.cs + i]);
+            T a[S] = {T(0), T(0), T(0), T(0)};
+            TR b[S] = {TR(0), TR(0), TR(0), TR(0)};
+            if constexpr (XB) ld4(xf + c * gf.cs + i0, a);
+            else if (r) { ld4(invD + c * gf.cs + i0, a); ld4(r + c * gf.cs + i0, b); }
+#pragma unroll
+            for (int ry = 0; ry < S; ++ry) { bs[ry][c] = a[ry]; br[ry][c] = T(b[ry]); }
+        }
+    } else {
+#pragma unroll
+        for (int ry = 0; ry < S; ++ry) {
+            const bool on = S * qy + ry < gf.NY;
+            const int64_t i = i0 + ry;
+            fl[ry] = on ? flagsF[i] : uint8_t(0);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                bs[ry][c] = !on ? T(0) : XB ? xf[c * gf.cs + i] : r ? invD[c * gf.cs + i] : T(0);
+                br[ry][c] = (!on || XB || !r) ? T(0) : T(r[c * gf.cs + i]);
+            }
         }
     }
+    T out[S][3];
 #pragma unroll
     for (int ry = 0; ry < S; ++ry) {
-        if (S * qy + ry >= gf.NY) break;
+        if constexpr (!V4) { if (S * qy + ry >= gf.NY) break; }
         const int64_t i = i0 + ry;
         const T wy[2] = {T(S - ry) / T(S), T(ry) / T(S)};
         T v[3] = {T(0), T(0), T(0)};
@@ -767,8 +841,28 @@ prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
                 for (int c = 0; c < 3; ++c) v[c] += omega * bs[ry][c] * br[ry][c];
             }
         }
+        if constexpr (V4) {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
+            for (int c = 0; c < 3; ++c) out[ry][c] = v[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
+        }
+    }
+    if constexpr (V4) {
+        if (S * qy + S <= gf.NY) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T w4[S] = {out[0][c], out[1][c], out[2][c], out[3][c]};
+                st4(xf + c * gf.cs + i0, w4);
+            }
+        } else {
+#pragma unroll
+            for (int ry = 0; ry < S; ++ry)
+                if (S * qy + ry < gf.NY)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) xf[c * gf.cs + i0 + ry] = out[ry][c];
+        }
     }
 }
 

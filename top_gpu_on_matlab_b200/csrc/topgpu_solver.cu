@@ -451,7 +451,11 @@ void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int n
         const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf, nq = (int64_t)NYc * NXc * lc.g.NZ;
         const int64_t vsS = 3 * (nt + n2);          // scratch per right-hand side
         T *t1 = rscratch<T>(s), *t2 = t1 + 3 * nt;
-        launch_k(s, restrict_y_kernel<T, 4>, dim3((unsigned)((nt + 255) / 256), K), 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
+        const dim3 gy((unsigned)((nt + 255) / 256), K);
+        if (s->vec4 && vec4_ok(lv.g, {d}, {lvs(lv)}))
+            launch_k(s, restrict_y_kernel<T, 4, true>, gy, 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
+        else
+            launch_k(s, restrict_y_kernel<T, 4>, gy, 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
         TOPGPU_COUNT_LAUNCH();
         launch_k(s, restrict_x_kernel<T, 4>, dim3((unsigned)((n2 + 255) / 256), K), 256, 0, s->st, t1, NYc, NXf, NXc, NZf, t2, done, vsS, vsS);
         TOPGPU_COUNT_LAUNCH();
@@ -555,7 +559,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         dim3 gr = node_grid(lv.g); gr.z = K;
         if (l == 0) {   // x = z1 + P t_c (x holds z1)
             const dim3 g4((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K);
-            if (lcn.span == 4)
+            if (lcn.span == 4 && s->vec4 && vec4_ok(lv.g, {x, lv.flags}, {vs}))
+                launch_k(s, prolong4_kernel<T, TR, true, true>, g4, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
+            else if (lcn.span == 4)
                 launch_k(s, prolong4_kernel<T, TR, true>, g4, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
             else
                 launch_k(s, prolong_kernel<T, 2, TR, true>, gr, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, nullptr, nullptr, omega, done, vsc, vs, 0);
@@ -563,8 +569,11 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
             const Reduce rz = zr ? (nv > 1 ? s->redk(zr) : s->red(zr)) : none;
             l0_op<T>(s, VecIn<T, T>{x, lv.g.cs, vs}, PostSmoothOut<T, TR, TZ>{x, r0, invd<T>(lv), z0, lv.g.cs, omega, vs0}, rz, done, nv);
         } else {
-            if (lcn.span == 4)
-                launch_k(s, prolong4_kernel<T, T, false>, dim3((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K), kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
+            const dim3 g4((unsigned)(((int64_t)((lv.g.NY + 3) / 4) * lv.g.NX * lv.g.NZ + kNodeThreads - 1) / kNodeThreads), K);
+            if (lcn.span == 4 && s->vec4 && vec4_ok(lv.g, {x, lv.flags, vr<T>(lv), invd<T>(lv)}, {vs}))
+                launch_k(s, prolong4_kernel<T, T, false, true>, g4, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
+            else if (lcn.span == 4)
+                launch_k(s, prolong4_kernel<T, T, false>, g4, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             else
                 launch_k(s, prolong_kernel<T, 2, T>, gr, kNodeThreads, 0, s->st, xc, lcn.g, x, lv.g, lv.flags, vr<T>(lv), invd<T>(lv), omega, done, vsc, vs, vs);
             TOPGPU_COUNT_LAUNCH();
@@ -1429,7 +1438,9 @@ extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_
         case 5: if (s->nL > 2) {   // level-1 -> level-0 prolongation with the Jacobi base, FP32
             DevLevel &f = s->L[0], &c = s->L[1];
             const dim3 g4((unsigned)(((int64_t)((f.g.NY + 3) / 4) * f.g.NX * f.g.NZ + kNodeThreads - 1) / kNodeThreads));
-            if (c.span == 4) prolong4_kernel<float, double, false><<<g4, kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
+            if (c.span == 4 && s->vec4 && vec4_ok(f.g, {f.x32, f.flags, s->r, f.invD32}, {}))
+                prolong4_kernel<float, double, false, true><<<g4, kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
+            else if (c.span == 4) prolong4_kernel<float, double, false><<<g4, kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
             else prolong_kernel<float, 2, double><<<node_grid(f.g), kNodeThreads, 0, s->st>>>(c.t32, c.g, f.x32, f.g, f.flags, s->r, f.invD32, 0.6f, nullptr);
             TOPGPU_COUNT_LAUNCH();
         } break;

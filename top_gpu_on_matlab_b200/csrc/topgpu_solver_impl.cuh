@@ -45,7 +45,10 @@ struct top_solver {
     bool useGraphs = true;
     bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
     bool coarsePersistent = false;   // levels below 0 of the V-cycle in one cooperative launch
-    bool pdl = std::getenv("TOPGPU_NO_PDL") == nullptr;   // programmatic dependent launch on the PCG path
+    bool pdl = std::getenv("TOPGPU_NO_PDL") == nullptr;
+    // span-4 transfers read and write four fine y slots as one aligned vector
+    // (identical results; TOPGPU_NO_VEC4 selects the per-slot kernels)
+    bool vec4 = std::getenv("TOPGPU_NO_VEC4") == nullptr;   // programmatic dependent launch on the PCG path
     bool inCapture = false;          // launches are being captured into a graph (no dependent launch there)
     int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
