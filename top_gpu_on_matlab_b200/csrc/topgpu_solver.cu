@@ -174,8 +174,7 @@ __global__ void coarsest_assemble_kernel(const double *__restrict__ KsC, const i
         }
     }
 }
-// ---- dense FP64 Cholesky (lower, col-major, in place), blocked 32 ----
-constexpr int kCb = 32;
+// ---- coarsest level ----
 // coarsest solve: x_grid = Ainv * r (r gathered from the grid in compact order)
 template <typename T>
 __global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const int32_t *__restrict__ nodeGrid,
@@ -413,12 +412,6 @@ template <> float *vx<float>(DevLevel &l) { return l.x32; }
 template <typename T> T *vt(DevLevel &l);
 template <> double *vt<double>(DevLevel &l) { return l.t64; }
 template <> float *vt<float>(DevLevel &l) { return l.t32; }
-template <typename T> const KeParam<T> &keparam(const top_solver *s);
-template <> const KeParam<double> &keparam<double>(const top_solver *s) { return s->Ke64; }
-template <> const KeParam<float> &keparam<float>(const top_solver *s) { return s->Ke32; }
-template <typename T> const T *egrid(const top_solver *s);
-template <> const double *egrid<double>(const top_solver *s) { return s->Eg64; }
-template <> const float *egrid<float>(const top_solver *s) { return s->Eg32; }
 
 // y-epilogue applied to (K_level in)(node) for every node of a coarse level;
 // nv right-hand sides in one launch (vectors at the functors' strides)
