@@ -25,6 +25,7 @@ runs the same iterations through the C ABI with the design held on the host
 the MATLAB driver cannot run here) on the host cores on a bounded sample.
 """
 import argparse
+import atexit
 import json
 import os
 import subprocess
@@ -55,41 +56,71 @@ def _env_rank():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons.  Started before
+    the solid solve and the warm-up steps so that the sampler is running when
+    the timed region begins; mark() at the start of the timed region, stop()
+    at its end reports the samples taken in between (the warm-up ones only if
+    the timed region was shorter than one sampling interval)."""
 
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=50, exe="nvidia-smi"):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.start_row = 0
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+            self.p = subprocess.Popen([exe, "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", str(interval_ms)], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        if self.p is not None:
+            atexit.register(self._end)                  # also when the bench fails before stop()
+
+    def _end(self):
+        if self.p is not None and self.p.poll() is None:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def _rows(self):
+        rows = []
+        try:
+            text = Path(self.f.name).read_text()
+        except OSError:
+            return rows
+        for line in text.splitlines(keepends=True):
+            if not line.endswith("\n"):
+                break                                   # a line still being written
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        return rows
+
+    def mark(self):
+        if self.p is not None:
+            self.start_row = len(self._rows())
 
     def stop(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
         if self.p is None:
             return out
-        self.p.terminate()
-        try:
-            self.p.wait(5)
-        except Exception:
-            self.p.kill()
+        self._end()
         self.f.flush()
-        rows = []
-        for line in Path(self.f.name).read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        if rows:
-            sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-            mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        rows = self._rows()
+        timed = rows[self.start_row:]
+        use = timed if timed else rows
+        if use:
+            sm = [float(r[1]) for r in use if r[1].replace(".", "").isdigit()]
+            mx = [float(r[2]) for r in use if r[2].replace(".", "").isdigit()]
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-            reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+            reasons = sorted({names[i] for r in use for i in range(4) if r[5 + i] == "Active"})
             out = {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                   "reasons": reasons, "samples": len(rows)}
+                   "reasons": reasons, "samples": len(use),
+                   "window": ("warm-up and timed (no sample visible at the start of the timed region)"
+                              if self.start_row == 0 else
+                              "timed" if timed else "warm-up (timed region shorter than the sampling interval)")}
         try:
             os.unlink(self.f.name)
         except OSError:
@@ -194,10 +225,14 @@ def run_ours(args):
 
     results = {}
     for name, mixed in (("fp64", False), ("mixed", True)):
+        # the sampler starts ahead of the solid solve and the warm-up steps, so
+        # that it is sampling when the timed region begins
+        clk = Clocks(local) if name == "mixed" else None
         s, c_solid = make(mixed)
         recs = [s.opt_step() for _ in range(args.warmup)]
         barrier()
-        clk = Clocks(local) if name == "mixed" else None
+        if clk:
+            clk.mark()
         n0 = s.launches
         t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
