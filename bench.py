@@ -162,6 +162,18 @@ def cpu_sample(iters=2, gpu_its=None):
     return {"ms_per_pcg_iter": 1e3 * t_it, "assemble_ms": 1e3 * t_asm, "cores": cores, "iters": its}
 
 
+def max_over_ranks(values, device, world):
+    """Per-rank timings -> the job's: the maximum over ranks of each value (one
+    all-reduce; every rank calls it at the same point).  One rank: unchanged."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def run_reference(args):
     rank, world, _ = _env_rank()
     if rank != 0:
@@ -242,10 +254,8 @@ def run_ours(args):
         launches = s.launches - n0
         clocks = clk.stop() if clk else None
         total = t0.elapsed_time(t1)
-        vals = torch.tensor([float(np.mean([r["msSolve"] for r in timed])), total / args.steps,
-                             float(np.mean([r["msAssemble"] for r in timed]))], device=dev)
-        if world > 1:
-            dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+        vals = max_over_ranks([float(np.mean([r["msSolve"] for r in timed])), total / args.steps,
+                               float(np.mean([r["msAssemble"] for r in timed]))], dev, world)
         xp, _ = s.design()
         results[name] = dict(solver=s, pcg_ms=float(vals[0]), step_ms=float(vals[1]), asm_ms=float(vals[2]),
                              its=[r["pcgIts"] for r in timed], c=[r["c"] for r in recs + timed],
@@ -273,7 +283,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         if k >= args.warmup:
             e2e.append(e0.elapsed_time(e1))
-    e2e_ms = float(np.mean(e2e))
+    e2e_ms = max_over_ranks([float(np.mean(e2e))], dev, world)[0]
     del s
 
     # ---- kernel roofline: level-0 stiffness products, L2 flushed ----
