@@ -136,6 +136,19 @@ int top_mesh_apply_bc(top_mesh *m, int64_t nFix, const double *fixRows,
                       int nLoads, const int64_t *nLoadRows,
                       const double *const *loadRows, const double *weights);
 
+/* A .TopVoxel model file, format version 1.0 (replaces the file branch of
+ * CreateVoxelFEAmodel, TOP_GPU.m:416-496): solid voxels, optional per-voxel
+ * densities, passive elements, fixations and load cases.  Builds the mesh
+ * (cellSize 1, as for file models) and applies the BCs after moving their
+ * nodes to the padded grid and the compact numbering (AdaptBCExternalMdl,
+ * TOP_GPU.m:1743-1793; one row per node, the first one), load cases weighted
+ * equally.  Passive elements (AdaptPassiveElementsExternalMdl, 1795-1813):
+ * top_mesh_get(m, 0, "passiveElements", ...) (compact, ascending); the file's
+ * densities: "densityLayout".  Errors: TOP_ERR_ARGS with "Incompatible Mesh
+ * Data Format!" (a token out of place), "Unsupported Data!" (another
+ * version), or a BC node / passive element that touches no solid voxel. */
+int top_mesh_create_from_topvoxel(const char *path, int control, double nu, top_mesh **out);
+
 /* Sizes: out[0] numLevels, then per level l (8 values each, from index
  * 1 + 8*l): resX, resY, resZ, spanWidth, numElements, numNodes,
  * intermediateNumNodes, nUnique (level 0 only).  Fills min(n, total). */
@@ -146,7 +159,9 @@ int top_mesh_info(const top_mesh *m, int64_t *out, int n);
  *   nodesOnBoundary elementsOnBoundary elementUpwardMap transferMat
  *   transferMatCoeffi solidNodeMapCoarser2Finer RI Ke mapUniqueKes
  *   eleWithFixedDOFs uniqueKesFree uniqueKesFixed fixingCond F objWeights
- *   I_mat.  *count receives the element count; dst may be NULL to query. */
+ *   I_mat passiveElements densityLayout, and resolution (int32 nely, nelx,
+ *   nelz of the model before padding).  *count receives the element count;
+ *   dst may be NULL to query. */
 int top_mesh_get(const top_mesh *m, int level, const char *name, void *dst,
                  int64_t capacity, int64_t *count);
 

@@ -82,6 +82,7 @@ SIGNATURES = {
     "top_mesh_destroy": (_int, [_vp]),
     "top_mesh_apply_optcase": (_int, [_vp, _int]),
     "top_mesh_apply_bc": (_int, [_vp, _i64, _vp, _int, _vp, _vp, _vp]),
+    "top_mesh_create_from_topvoxel": (_int, [C.c_char_p, _int, _dbl, _vp]),
     "top_mesh_info": (_int, [_vp, _vp, _int]),
     "top_mesh_get": (_int, [_vp, _int, C.c_char_p, _vp, _i64, _vp]),
     "top_solver_create": (_int, [_vp, _vp, _vp]),

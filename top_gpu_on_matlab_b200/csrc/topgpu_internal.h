@@ -47,6 +47,10 @@ struct top_mesh {
     std::vector<double> uniqueKesFree, uniqueKesFixed;
     std::vector<uint8_t> nodeFixed;      // level-0 compact nodes: bit c = component c fixed
     std::vector<double> I_mat;           // super-element sub-voxel stiffnesses [576 x 64]
+    // .TopVoxel models: passive elements (compact, ascending) and the file's
+    // per-voxel densities (file order; empty when the file has none)
+    std::vector<int32_t> passiveElements;
+    std::vector<double> densityLayout;
 };
 
 namespace topgpu {

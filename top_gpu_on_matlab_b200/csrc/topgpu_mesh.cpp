@@ -495,6 +495,7 @@ extern "C" int top_mesh_get(const top_mesh *m, int level, const char *name, void
     int64_t n = 0;
     size_t es = 4;
     std::string k(name);
+    const std::vector<int32_t> resolution{m->nely, m->nelx, m->nelz};
     auto I = [&](const std::vector<int32_t> &v) { src = v.data(); n = (int64_t)v.size(); es = 4; };
     auto D = [&](const std::vector<double> &v) { src = v.data(); n = (int64_t)v.size(); es = 8; };
     if (k == "eleMapBack") I(L.eleMapBack);
@@ -518,6 +519,9 @@ extern "C" int top_mesh_get(const top_mesh *m, int level, const char *name, void
     else if (k == "F") D(m->F);
     else if (k == "objWeights") D(m->weights);
     else if (k == "I_mat") D(m->I_mat);
+    else if (k == "passiveElements") I(m->passiveElements);
+    else if (k == "resolution") I(resolution);
+    else if (k == "densityLayout") D(m->densityLayout);
     else { set_error("top_mesh_get: unknown array '%s'", name); return TOP_ERR_ARGS; }
     if (count) *count = n;
     if (dst) {

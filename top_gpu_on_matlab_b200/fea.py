@@ -8,6 +8,7 @@ GPU and provides Solving_AssembleFEAstencil, Solving_KbyU_MatrixFree,
 Solving_Vcycle and Solving_PCG (TOP_GPU.m:602-878, 1033-1267).
 """
 import ctypes as C
+import os
 
 import numpy as np
 import torch
@@ -15,7 +16,7 @@ import torch
 from ._lib import (OptParams, OptRecord, SolverParams, TOP_ERR_NOT_CONVERGED, TOP_OK, TOP_PREC_FP64,
                    TOP_PREC_MIXED, TopGpuError, check, last_error, lib)
 
-_INT_ARRAYS = {"eleMapBack", "eleMapForward", "eNodMat", "nodMapBack", "nodMapForward", "nodesOnBoundary",
+_INT_ARRAYS = {"passiveElements", "resolution", "eleMapBack", "eleMapForward", "eNodMat", "nodMapBack", "nodMapForward", "nodesOnBoundary",
                "elementsOnBoundary", "elementUpwardMap", "transferMat", "solidNodeMapCoarser2Finer",
                "mapUniqueKes", "eleWithFixedDOFs", "fixingCond"}
 
@@ -41,6 +42,23 @@ class Mesh:
               "top_mesh_create")
         self._h = h
         self.super_element = super_element
+
+    @classmethod
+    def from_topvoxel(cls, path, control=20000, nu=0.3):
+        """A .TopVoxel model file (CreateVoxelFEAmodel, TOP_GPU.m:416-496), its
+        fixations and load cases applied; cellSize 1 as for file models.
+        .passive_elements (compact, 1-based) and .density_layout (the file's
+        per-voxel densities, may be empty) come with it."""
+        self = cls.__new__(cls)
+        h = C.c_void_p()
+        check(lib().top_mesh_create_from_topvoxel(os.fsencode(str(path)), control, nu, C.byref(h)),
+              "top_mesh_create_from_topvoxel")
+        self._h = h
+        self.super_element = 0
+        self.shape = tuple(int(v) for v in self.get(0, "resolution"))
+        self.passive_elements = self.get(0, "passiveElements")
+        self.density_layout = self.get(0, "densityLayout")
+        return self
 
     def close(self):
         if getattr(self, "_h", None):
