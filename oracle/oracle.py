@@ -55,6 +55,7 @@ class OModel(C.Structure):
         ("filterENod", i32p), ("nFilterEles", C.c_int64),
         ("fincPtr", i64p), ("fincIdx", i32p),
         ("lastPcgIts", C.c_int),
+        ("passive", C.POINTER(C.c_uint8)),
     ]
 
 
@@ -105,6 +106,7 @@ def lib():
         L.orc_pde_filter.argtypes = [C.POINTER(OModel), C.c_void_p, C.c_void_p]
         L.orc_top_opt.argtypes = [C.POINTER(OModel), C.c_double, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_solve_state.argtypes = [C.POINTER(OModel), C.c_void_p, C.c_int]
+        L.orc_set_passive.argtypes = [C.POINTER(OModel), C.c_void_p, C.c_int64]
         _LIB = L
     return _LIB
 
@@ -345,6 +347,13 @@ class Model:
         out = np.zeros(self.m.L[0].numElements)
         lib().orc_pde_filter(self._m, _p(src), _p(out))
         return out
+
+    def set_passive(self, ids):
+        """passive elements (1-based compact ids; empty clears): design 1 inside
+        the OC bisection and after the filter (TOP_GPU.m:239/247, 270/273)"""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        if lib().orc_set_passive(self._m, _p(ids), ids.size):
+            raise ValueError("oracle: passive element id out of range")
 
     def top_opt(self, V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1):
         ne = self.m.L[0].numElements * (64 if self.super_element else 1)

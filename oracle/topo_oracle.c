@@ -544,6 +544,7 @@ void orc_destroy(OModel *m)
         free(L->transferMat); free(L->transferMatCoeffi); free(L->solidNodeMapCoarser2Finer);
         free(L->RI); free(L->Ks); free(L->diagK); free(L->incPtr); free(L->incIdx);
     }
+    free(m->passive);
     free(m->L); free(m->fixingCond); free(m->F); free(m->objWeights);
     free(m->mapUniqueKes); free(m->eleWithFixedDOFs); free(m->uniqueKesFree);
     free(m->uniqueKesFixed); free(m->eleModulus); free(m->I_mat); free(m->K_mat);
@@ -1344,6 +1345,33 @@ static void sfilt_apply(const OModel *m, const SFilt *f, const double *in, doubl
 }
 
 /* ------------------------------------------------------------------------ */
+/* Passive elements (passiveElements_, TOP_GPU.m:125)                         */
+int orc_set_passive(OModel *m, const int32_t *ids, int64_t n)
+{
+    const int64_t Ne = m->L[0].numElements;
+    free(m->passive);
+    m->passive = NULL;
+    if (n <= 0) return 0;
+    m->passive = xc(Ne, 1);
+    for (int64_t k = 0; k < n; ++k) {
+        if (ids[k] < 1 || ids[k] > Ne) { free(m->passive); m->passive = NULL; return -1; }
+        m->passive[ids[k] - 1] = 1;
+    }
+    return 0;
+}
+
+/* the design entries a passive element pins to 1: the element (standard
+ * voxels) or, as the reference indexes xnew(Num_, passiveElements) and
+ * xPhys(Num_, passiveElements) (TOP_GPU.m:247, 273), its sub-voxel row Num_ = 4
+ * alone (super elements) */
+static void pin_passive(const OModel *m, double *v, int64_t Ne, int sup)
+{
+    if (!m->passive) return;
+    for (int64_t e = 0; e < Ne; ++e)
+        if (m->passive[e]) v[sup ? 3 + 64 * e : e] = 1.0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Optimisation loop (TOP_GPU.m:122-292)                                      */
 int orc_top_opt(OModel *m, double V0, double rMin, int nLoop, int ft,
                 double *xPhysOut, double *hist, double *cSolidOut)
@@ -1412,9 +1440,10 @@ int orc_top_opt(OModel *m, double V0, double rMin, int nLoop, int ft,
             double lmid = 0.5 * (l2 + l1), sum = 0;
             for (int64_t i = 0; i < nv; ++i) {
                 double cand = x[i] * sqrt(-dc[i] / dv[i] / lmid);
-                double v = fmax(0.0, fmax(x[i] - move, fmin(1.0, fmin(x[i] + move, cand))));
-                xnew[i] = v; sum += v - x[i];
+                xnew[i] = fmax(0.0, fmax(x[i] - move, fmin(1.0, fmin(x[i] + move, cand))));
             }
+            pin_passive(m, xnew, Ne, sup);                        /* 239 / 247 */
+            for (int64_t i = 0; i < nv; ++i) sum += xnew[i] - x[i];
             double gt = fval + sum / (double)nv;
             if (gt > 0) l1 = lmid; else l2 = lmid;
         }
@@ -1423,6 +1452,7 @@ int orc_top_opt(OModel *m, double V0, double rMin, int nLoop, int ft,
         memcpy(x, xnew, sizeof(double) * nv);
         if (ft == 1) memcpy(xPhys, xnew, sizeof(double) * nv);
         else if (ft == 2) { if (!sup) orc_pde_filter(m, xnew, xPhys); else sfilt_apply(m, &sf, xnew, xPhys, 1); }
+        pin_passive(m, xPhys, Ne, sup);                           /* 270 / 273 */
         sharp = 0;
         for (int64_t i = 0; i < nv; ++i) sharp += xPhys[i] * (1.0 - xPhys[i]);
         sharp = 4 * sharp / (double)nv;

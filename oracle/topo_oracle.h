@@ -95,7 +95,13 @@ typedef struct {
     int64_t *fincPtr; int32_t *fincIdx;
     /* statistics */
     int lastPcgIts;
+    /* passive elements (TOP_GPU.m:125, 239/247, 270/273): [Ne] 0 / 1, or NULL */
+    uint8_t *passive;
 } OModel;
+
+/* passive elements, 1-based compact ids (n = 0 clears): in the optimisation
+ * loop their design is 1 inside the OC bisection and after the filter */
+int orc_set_passive(OModel *m, const int32_t *ids, int64_t n);
 
 /* ---- model construction ------------------------------------------------ */
 /* mask: logical [nely x nelx x nelz] col-major (uint8).  Builds level 1,
