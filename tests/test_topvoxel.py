@@ -144,3 +144,33 @@ def test_bc_on_void_is_rejected(tmp_path):
         OT.create_model(path, control=500)
     write_topvoxel(path, mask, fix[:1], loads, passive=[voxel_index(3, 3, 3, shape)])
     _expect_error(path, "is not a solid voxel")
+
+
+def test_corrupted_files_fail_cleanly(tmp_path):
+    """seeded token corruption (dropped, duplicated, replaced, huge or negative
+    numbers): every file either loads or fails with a status, never crashes"""
+    path, text = _base_file(tmp_path)
+    toks = text.split()
+    rng = np.random.default_rng(7)
+    bad = tmp_path / "fuzz.TopVoxel"
+    outcomes = {"ok": 0, "error": 0}
+    for _ in range(200):
+        t = list(toks)
+        for _ in range(int(rng.integers(1, 4))):
+            k = int(rng.integers(0, len(t)))
+            op = int(rng.integers(0, 4))
+            if op == 0:
+                del t[k]
+            elif op == 1:
+                t.insert(k, t[k])
+            elif op == 2:
+                t[k] = str(int(rng.choice([-1, 0, 2 ** 31, 2 ** 62, 10 ** 30])))
+            else:
+                t[k] = rng.choice(["x", "1e400", "nan", "-0", "Loads:"])
+        bad.write_text(" ".join(t))
+        try:
+            Mesh.from_topvoxel(bad, control=500).close()
+            outcomes["ok"] += 1
+        except TopGpuError:
+            outcomes["error"] += 1
+    assert outcomes["error"] > 0 and sum(outcomes.values()) == 200
