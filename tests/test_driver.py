@@ -73,8 +73,8 @@ def test_run_writes_the_reference_files(tmp_path):
     assert s.prm == (0.12, math.sqrt(3), 8, 1) and len(out["history"]) == 8 and out["cSolid"] == 123.5
     assert os.path.basename(out["path"]) == "case1_12x6x6_V0.12_r1.732_ft1_n8_mp1_se0"
     names = sorted(os.listdir(out["path"]))
-    assert names == ["DesignVolume.nii", "RunLog.log", "c_Target.dat", "iters_Target.dat", "sharp_Target.dat",
-                     "solvetiming_Target.dat", "timing_Target.dat"]
+    assert names == ["DesignVolume.nii", "RunLog.log", "c_Target.dat", "history.json", "iters_Target.dat",
+                     "sharp_Target.dat", "solvetiming_Target.dat", "timing_Target.dat"]
     log = open(os.path.join(out["path"], "RunLog.log")).read().splitlines()
     assert log[1] == "Compliance of Fully Solid Domain:     1.235000e+02"
     assert sum(l.startswith(" It.:") for l in log) == 2 * 8

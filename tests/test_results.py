@@ -37,6 +37,11 @@ def test_history_files(tmp_path):
     assert read("solvetiming_Target.dat") == ["%16.6e" % (r["msSolve"] / 1e3) for r in recs]
     assert read("iters_Target.dat") == [str(r["pcgIts"]) for r in recs]
     assert all(len(l) == 30 for l in read("c_Target.dat"))
+    import json
+    h = json.loads((tmp_path / "history.json").read_text())
+    assert [r["iteration"] for r in h] == list(range(1, 8))
+    assert all(r["c"] == q["c"] and r["total_s"] == q["msTotal"] / 1e3 and r["cg_s"] == q["msSolve"] / 1e3
+               for r, q in zip(h, recs))
     R.write_history(tmp_path, recs, iters=[3, 4, 5])          # per-solve counts (several load cases)
     assert read("iters_Target.dat") == ["3", "4", "5"]
 
@@ -101,7 +106,7 @@ def test_write_results_files(tmp_path):
     recs = _records(3, np.random.default_rng(5))
     R.write_results(tmp_path, m, x, recs)
     names = sorted(p.name for p in tmp_path.iterdir())
-    assert names == ["DesignVolume.nii", "c_Target.dat", "iters_Target.dat", "sharp_Target.dat",
+    assert names == ["DesignVolume.nii", "c_Target.dat", "history.json", "iters_Target.dat", "sharp_Target.dat",
                      "solvetiming_Target.dat", "timing_Target.dat"]
     _, V = _read_nifti(tmp_path / "DesignVolume.nii")
     assert np.array_equal(V.ravel(order="F")[m.get(0, "eleMapBack") - 1], x)

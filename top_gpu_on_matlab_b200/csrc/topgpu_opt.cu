@@ -845,20 +845,33 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
     const int64_t Ne = o.nv;           // design variables (64 per super-element)
     cudaStream_t st = s->st;
     const int VB = vb(Ne);
-    cudaEvent_t ev[7];
-    for (auto &e : ev) CK(cudaEventCreate(&e));
+    struct PhaseEvents {             // destroyed on every return
+        cudaEvent_t e[7] = {};
+        ~PhaseEvents() { for (cudaEvent_t x : e) if (x) cudaEventDestroy(x); }
+    } pe;
+    cudaEvent_t *ev = pe.e;
+    for (int k = 0; k < 7; ++k) CK(cudaEventCreate(&ev[k]));
+    NvtxRange whole("opt_step");
     CK(cudaEventRecord(ev[0], st));
     // 5.1 SIMP moduli and stencil assembly
-    int rc = set_modulus_dev(s, o.xPhys, 1, 1);
-    if (!rc) rc = top_solver_assemble(s);
+    int rc;
+    {
+        NvtxRange r("opt_step: SIMP + assembly");
+        rc = set_modulus_dev(s, o.xPhys, 1, 1);
+        if (!rc) rc = top_solver_assemble(s);
+    }
     if (rc) return rc;
     CK(cudaEventRecord(ev[1], st));
     // 5.2 state solves, warm-started
     int its = 0;
-    rc = solve_all(s, 1, &its);
+    {
+        NvtxRange r("opt_step: PCG");
+        rc = solve_all(s, 1, &its);
+    }
     if (rc) return rc;
     CK(cudaEventRecord(ev[2], st));
     // objective and sensitivities, volume
+    NvtxRange rest("opt_step: sensitivities, filter, OC");
     rc = sensitivities(s, 1);
     if (rc) return rc;
     sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 0, s->red(&o.sc->sumE));
@@ -933,7 +946,6 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
         cudaEventElapsedTime(&tot, ev[0], ev[6]);
         rec->msTotal = tot;
     }
-    for (auto &e : ev) cudaEventDestroy(e);
     return TOP_OK;
 }
 

@@ -3,6 +3,7 @@
 // (filters, sensitivities, OC loop).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdlib>
 #include <vector>
 #include <utility>
@@ -119,6 +120,13 @@ struct top_solver {
 };
 
 namespace topgpu {
+// named host range for profilers (NVTX; nothing happens without one attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 // launch on the PCG path: with s->pdl, outside graph capture, the kernel may
 // be scheduled while its predecessor in the stream finishes (it must begin
 // with pdl_enter()); captured graphs keep plain dependencies (measured: the

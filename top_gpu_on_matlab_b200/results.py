@@ -8,6 +8,9 @@
     iters_Target.dat        PCG iterations per solve         %d
     xPhys_sorted.dat        super-element designs in spatial order   %30.16e
     DesignVolume.nii        the design on the padded voxel grid (NIfTI-1)
+    history.json            one object per iteration: objective, volume,
+                            sharpness, constraint, change, PCG iterations and
+                            the tHist columns (TOP_GPU.m:283) in seconds
 
 Histories come from the solver's per-iteration records (keys c, sharp,
 msSolve, msTotal, pcgIts as returned by Solver.opt_step / Solver.optimize);
@@ -17,6 +20,7 @@ and iteration; a record holds their sum over the load cases, so
 iters_Target.dat takes per-solve counts when given (`iters`) and the
 record's count otherwise (the same for one load case).
 """
+import json
 import math
 import os
 import struct
@@ -51,6 +55,19 @@ def write_history(out_dir, records, iters=None):
     _write_column(j("sharp_Target.dat"), [r["sharp"] for r in records], lambda v: _fmt_e(v, 30, 16))
     _write_column(j("timing_Target.dat"), [r["msTotal"] / 1e3 for r in records], lambda v: _fmt_e(v, 16, 6))
     _write_column(j("solvetiming_Target.dat"), [r["msSolve"] / 1e3 for r in records], lambda v: _fmt_e(v, 16, 6))
+    rows = []
+    for k, r in enumerate(records, start=1):
+        row = {"iteration": k}
+        for key in ("c", "vol", "sharp", "cons", "change", "pcgIts"):
+            if key in r:
+                row[key] = r[key]
+        for name, key in (("assembling_s", "msAssemble"), ("cg_s", "msSolve"), ("optimisation_s", "msOpt"),
+                          ("filtering_s", "msFilter"), ("total_s", "msTotal")):
+            if key in r:
+                row[name] = r[key] / 1e3
+        rows.append(row)
+    with open(j("history.json"), "w") as f:
+        json.dump(rows, f, indent=1)
 
 
 def super_spatial_order(nelx, nely, nelz, n=4):
