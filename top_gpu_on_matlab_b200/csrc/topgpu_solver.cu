@@ -1404,19 +1404,26 @@ extern "C" int top_solver_unit_compliance(top_solver *s, const double *U, double
 
 // ---- kernel timing (CUDA events on the solver's stream) -------------------
 // which: 0 = level-0 K*u FP64 (the outer PCG operator), 1 = level-0 K*u FP32
-// (the V-cycle smoother operator), 2 = one V-cycle, 3 = level-1 K*u FP32.
+// (the V-cycle smoother operator), 2 = one V-cycle, 3 = level-1 K*u FP32,
+// 4 = level 0 -> 1 restriction FP32, 5 = level 1 -> 0 prolongation FP32.
 // Each launch is preceded by a write of flushBytes to evict L2 (0 = none);
 // *msPerLaunch receives the mean event time of the launches alone.
 extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_t flushBytes, double *msPerLaunch)
 {
     if (!s || nrep < 1 || !msPerLaunch) return TOP_ERR_ARGS;
+    if (which < 0 || which > 5) { set_error("top_solver_time_kernel: unknown kernel %d", which); return TOP_ERR_ARGS; }
     if (which != 0 && !s->assembled) { set_error("top_solver_time_kernel: assemble first"); return TOP_ERR_STATE; }
     DevLevel &l0 = s->L[0];
     const Reduce none{nullptr, nullptr, nullptr};
-    void *flush = nullptr;
-    if (flushBytes > 0) CK(cudaMalloc(&flush, (size_t)flushBytes));
-    cudaEvent_t a, b;
-    CK(cudaEventCreate(&a)); CK(cudaEventCreate(&b));
+    struct Held {                    // released on every return
+        void *flush = nullptr;
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~Held() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); if (flush) cudaFree(flush); }
+    } h;
+    if (flushBytes > 0) CK(cudaMalloc(&h.flush, (size_t)flushBytes));
+    CK(cudaEventCreate(&h.a)); CK(cudaEventCreate(&h.b));
+    void *flush = h.flush;
+    cudaEvent_t a = h.a, b = h.b;
     double total = 0;
     for (int k = 0; k < nrep; ++k) {
         if (flush) CK(cudaMemsetAsync(flush, k & 0xff, (size_t)flushBytes, s->st));
@@ -1446,8 +1453,6 @@ extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_
         CK(cudaEventElapsedTime(&ms, a, b));
         total += ms;
     }
-    cudaEventDestroy(a); cudaEventDestroy(b);
-    if (flush) cudaFree(flush);
     CKL();
     *msPerLaunch = total / nrep;
     return TOP_OK;
