@@ -243,15 +243,20 @@ extern "C" int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void
     const int hasFixed = (nUnique > 0 && mapUnique && uniqueFree && uniqueFixed) ? 1 : 0;
     cudaStream_t st = S(stream);
     if (dtype == TOP_F64) {
-        double *Q = nullptr; int32_t *one = nullptr;
+        struct Scratch {             // stream-ordered frees on every exit of this block
+            void *p = nullptr; cudaStream_t st;
+            explicit Scratch(cudaStream_t q) : st(q) {}
+            ~Scratch() { if (p) cudaFreeAsync(p, st); }
+        } q(st), o(st);
         const size_t qn = (size_t)576 * (nCh > 64 ? nCh : 64);
-        TOP_CUDA_CHECK(cudaMallocAsync(&Q, sizeof(double) * qn, st), N);
-        TOP_CUDA_CHECK(cudaMemsetAsync(Q, 0, sizeof(double) * qn, st), N);
-        TOP_CUDA_CHECK(cudaMallocAsync(&one, sizeof(int32_t) * (size_t)nCh * nCh + 4, st), N);
+        TOP_CUDA_CHECK(cudaMallocAsync(&q.p, sizeof(double) * qn, st), N);
+        TOP_CUDA_CHECK(cudaMemsetAsync(q.p, 0, sizeof(double) * qn, st), N);
+        TOP_CUDA_CHECK(cudaMallocAsync(&o.p, sizeof(int32_t) * (size_t)nCh * nCh + 4, st), N);
+        double *Q = static_cast<double *>(q.p);
+        int32_t *one = static_cast<int32_t *>(o.p);
         int rc = assemble_level2_f64((double *)Ks, upMap, (const double *)eleModulus, (const double *)K0,
                                      (const double *)Pch, mapUnique, (const double *)uniqueFree,
                                      (const double *)uniqueFixed, nElem, nCh, hasFixed ? nUnique : 0, Q, one, st, nullptr, -1);
-        cudaFreeAsync(Q, st); cudaFreeAsync(one, st);
         if (rc) { set_error("%s:CUDA launch failed: %s", N, cudaGetErrorString(cudaGetLastError())); return rc; }
     } else {
         ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
