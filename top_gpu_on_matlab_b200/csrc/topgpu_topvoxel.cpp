@@ -26,7 +26,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <fstream>
 #include <new>
 #include <string>
 #include <vector>
@@ -40,46 +39,55 @@ namespace {
 
 constexpr const char *kFormatError = "Incompatible Mesh Data Format!";   // TOP_GPU.m:423 & co.
 
+// whitespace-separated tokens scanned in place in the file's bytes (the
+// buffer is NUL-terminated, so strtoll / strtod stop at a token's end)
 struct Tokens {
-    std::vector<std::string> t;
+    std::string buf;
     size_t i = 0;
-    bool word(std::string &w)
+    static bool ws(char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t' || c == '\v' || c == '\f'; }
+    bool next(const char *&b, const char *&e)
     {
-        if (i >= t.size()) return false;
-        w = t[i++];
+        while (i < buf.size() && ws(buf[i])) ++i;
+        if (i >= buf.size()) return false;
+        size_t j = i;
+        while (j < buf.size() && !ws(buf[j])) ++j;
+        b = buf.data() + i;
+        e = buf.data() + j;
+        i = j;
         return true;
     }
     bool skip(int n)
     {
-        std::string w;
+        const char *b, *e;
         for (int k = 0; k < n; ++k)
-            if (!word(w)) return false;
+            if (!next(b, e)) return false;
         return true;
     }
-    size_t left() const { return t.size() - i; }
+    // an upper bound on the tokens left (each takes a byte and a separator)
+    size_t left() const { return (buf.size() - i + 1) / 2; }
     bool expect(const char *w)
     {
-        std::string s;
-        return word(s) && s == w;
+        const char *b, *e;
+        return next(b, e) && size_t(e - b) == std::strlen(w) && std::memcmp(b, w, size_t(e - b)) == 0;
     }
     bool integer(int64_t &v)
     {
-        std::string s;
-        if (!word(s)) return false;
+        const char *b, *e;
+        if (!next(b, e)) return false;
         char *end = nullptr;
         errno = 0;
-        const long long r = std::strtoll(s.c_str(), &end, 10);
-        if (errno || end == s.c_str() || *end) return false;
+        const long long r = std::strtoll(b, &end, 10);
+        if (errno || end != e) return false;
         v = r;
         return true;
     }
     bool real(double &v)
     {
-        std::string s;
-        if (!word(s)) return false;
+        const char *b, *e;
+        if (!next(b, e)) return false;
         char *end = nullptr;
-        v = std::strtod(s.c_str(), &end);
-        return end != s.c_str() && !*end;
+        v = std::strtod(b, &end);
+        return end == e;
     }
 };
 
@@ -125,15 +133,17 @@ static int create_from_topvoxel(const char *path, int control, double nu, top_me
 {
     if (!path || !out || control < 1) return fail("bad arguments");
     *out = nullptr;
-    std::ifstream f(path);
-    if (!f) {
-        set_error("top_mesh_create_from_topvoxel: cannot open '%s'", path);
-        return TOP_ERR_ARGS;
-    }
     Tokens tk;
     {
-        std::string w;
-        while (f >> w) tk.t.push_back(w);
+        std::FILE *f = std::fopen(path, "rb");
+        if (!f) {
+            set_error("top_mesh_create_from_topvoxel: cannot open '%s'", path);
+            return TOP_ERR_ARGS;
+        }
+        char chunk[1 << 16];
+        size_t n;
+        while ((n = std::fread(chunk, 1, sizeof chunk, f)) > 0) tk.buf.append(chunk, n);
+        std::fclose(f);
     }
     double version = 0;
     if (!tk.skip(4) || !tk.skip(1) || !tk.real(version)) return fail(kFormatError);
