@@ -260,6 +260,12 @@ int top_solver_super_filter(top_solver *s, const double *src, double *tar, int m
  * sensitivities, filter, OC bisection, xPhys); optimize loops until
  * nLoop / change <= 1e-4 / sharpness <= 0.01.  Designs are device arrays. */
 int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, double *cSolid);
+/* Passive elements (passiveElements_, e.g. from a .TopVoxel file): host array
+ * of n compact 1-based element ids (n = 0 clears).  In the loop their design
+ * is 1 inside the OC bisection and after the filter (TOP_GPU.m:239, 270); for
+ * super elements only sub-voxel row Num_ = 4 of each, as the reference
+ * indexes it (247, 273). */
+int top_solver_set_passive(top_solver *s, const int32_t *ids, int64_t n);
 int top_solver_opt_step(top_solver *s, top_opt_record *rec);
 int top_solver_opt_state(top_solver *s, int *loop, double *change, double *sharpness);
 /* get/set copy the physical and raw designs (either may be NULL) to/from

@@ -23,6 +23,9 @@ class ScriptedSolver:
         self.ne = mesh.info()[0]["numElements"] * (64 if mesh.super_element else 1)
         ScriptedSolver.made.append(self)
 
+    def set_passive(self, ids):
+        self.passive = np.asarray(ids)
+
     def opt_begin(self, V0, rMin, nLoop, ft):
         self.prm = (V0, rMin, nLoop, ft)
         return 123.5
@@ -104,8 +107,8 @@ def test_argument_errors(tmp_path):
     load = np.array([[node_index(3, 8, 0, shape), 0.0, 0.0, -1.0]])
     path = tmp_path / "p.TopVoxel"
     write_topvoxel(path, np.ones(shape, bool), fix, [load], passive=[1, 2])
-    with pytest.raises(NotImplementedError, match="passive"):
-        D.TOP_GPU(str(path), out_root=str(tmp_path), solver_class=ScriptedSolver)
+    D.TOP_GPU(str(path), nLoop=1, out_root=str(tmp_path), solver_class=ScriptedSolver, log=lambda s: None)
+    assert list(ScriptedSolver.made[-1].passive) == [1, 2]        # the file's passive list reaches the solver
     write_topvoxel(path, np.ones(shape, bool), fix, [load])
     out = D.TOP_GPU(str(path), nLoop=3, out_root=str(tmp_path), solver_class=ScriptedSolver, log=lambda s: None)
     assert os.path.basename(out["path"]) == "p_V0.12_r1.732_ft1_n3_mp0_se0" and len(out["history"]) == 3

@@ -108,6 +108,7 @@ SIGNATURES = {
     "top_solver_super_filter_setup": (_int, [_vp, _dbl]),
     "top_solver_super_filter": (_int, [_vp, _vp, _vp, _int]),
     "top_solver_opt_begin": (_int, [_vp, _vp, _vp]),
+    "top_solver_set_passive": (_int, [_vp, _vp, _i64]),
     "top_solver_opt_step": (_int, [_vp, _vp]),
     "top_solver_opt_state": (_int, [_vp, _vp, _vp, _vp]),
     "top_solver_get_design": (_int, [_vp, _vp, _vp]),

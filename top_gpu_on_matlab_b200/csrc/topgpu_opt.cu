@@ -71,6 +71,9 @@ struct OptState {
     double *ocR = nullptr;                              // -dc./dv of the bisection
     int64_t nv = 0;          // design variables (64 per super-element)
     SFilterState sf;         // super-element density filter
+    // passive elements: 1 on the design variables held at 1 (TOP_GPU.m:239, 270;
+    // super elements: sub-voxel row Num_ = 4, 247, 273); used when nPassive > 0
+    uint8_t *passive = nullptr; int64_t passiveLen = 0, nPassive = 0;
 };
 
 }  // namespace topgpu
@@ -443,9 +446,11 @@ __device__ __forceinline__ double oc_new(double x, double r, double lmid, double
 // sums in the same fixed order (lane-strided, then a shuffle tree) so every
 // CTA takes the same branch; block sums alternate between two buffers, so
 // the next step cannot overwrite what a slower CTA still reads.
+// pin (may be null): design variables held at 1 whatever the multiplier
+// (passive elements, TOP_GPU.m:239 / 247)
 __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc, const double *__restrict__ dv,
                           double *__restrict__ rbuf, int64_t n, double *__restrict__ partials, OptScalars *sc,
-                          double move, int maxSteps)
+                          double move, int maxSteps, const uint8_t *__restrict__ pin)
 {
     cg::grid_group grid = cg::this_grid();
     __shared__ double red[8];
@@ -478,7 +483,7 @@ __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc,
         double s = 0;
         for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
             const double xi = x[i];
-            s += oc_new(xi, rbuf[i], lmid, move) - xi;
+            s += ((pin && pin[i]) ? 1.0 : oc_new(xi, rbuf[i], lmid, move)) - xi;
         }
         const double bs = block_reduce(s, false);
         double *pp = partials + (step & 1) * nb;
@@ -499,7 +504,7 @@ __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc,
     // xnew from the last multiplier; change = max|xnew - x|; x = xnew
     double mx = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const double xn = oc_new(x[i], rbuf[i], lmid, move);
+        const double xn = (pin && pin[i]) ? 1.0 : oc_new(x[i], rbuf[i], lmid, move);
         mx = fmax(mx, fabs(xn - x[i]));
         x[i] = xn;
     }
@@ -518,6 +523,9 @@ __global__ void oc_kernel(double *__restrict__ x, const double *__restrict__ dc,
 
 __global__ void copy_kernel(const double *__restrict__ a, double *__restrict__ b, int64_t n)
 { for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) b[i] = a[i]; }
+// xPhys(passive) = 1 after the filter (TOP_GPU.m:270 / 273)
+__global__ void pin_kernel(double *__restrict__ x, const uint8_t *__restrict__ pin, int64_t n)
+{ for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) if (pin[i]) x[i] = 1.0; }
 __global__ void fill_kernel(double *__restrict__ a, double v, int64_t n)
 { for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) a[i] = v; }
 
@@ -777,6 +785,30 @@ static int sensitivities(top_solver *s, int withGrad)
     return TOP_OK;
 }
 
+extern "C" int top_solver_set_passive(top_solver *s, const int32_t *ids, int64_t n)
+{
+    if (!s || n < 0 || (n > 0 && !ids)) { set_error("top_solver_set_passive: bad arguments"); return TOP_ERR_ARGS; }
+    ensure_state(s);
+    OptState &o = opt(s);
+    const int64_t Ne = s->L[0].Ne, nv = Ne * (s->super ? 64 : 1);
+    std::vector<uint8_t> mask((size_t)nv, 0);
+    for (int64_t k = 0; k < n; ++k) {
+        if (ids[k] < 1 || ids[k] > Ne) { set_error("top_solver_set_passive: element %d out of range", (int)ids[k]); return TOP_ERR_ARGS; }
+        mask[(size_t)(s->super ? 3 + 64 * (int64_t)(ids[k] - 1) : ids[k] - 1)] = 1;
+    }
+    if (n > 0 && (!o.passive || o.passiveLen != nv)) {
+        o.passive = s->dalloc<uint8_t>((size_t)nv);
+        if (!o.passive) { set_error("top_solver_set_passive: out of device memory"); return TOP_ERR_NOMEM; }
+        o.passiveLen = nv;
+    }
+    if (n > 0) {
+        CK(cudaMemcpyAsync(o.passive, mask.data(), (size_t)nv, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    o.nPassive = n;
+    return TOP_OK;
+}
+
 extern "C" int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, double *cSolidOut)
 {
     if (!s || !prm || prm->nLoop < 0 || !(prm->V0 > 0) || (prm->ft != 0 && prm->ft != 1 && prm->ft != 2)) {
@@ -912,7 +944,8 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
         int maxSteps = 256;
         int64_t n = Ne;
         double *xa = o.xd; const double *dca = o.dc, *dva = o.dv; double *ra = o.ocR, *pa = o.ocPartials; OptScalars *sca = o.sc;
-        void *args[] = {&xa, &dca, &dva, &ra, &n, &pa, &sca, &move, &maxSteps};
+        const uint8_t *pin = o.nPassive > 0 ? o.passive : nullptr;
+        void *args[] = {&xa, &dca, &dva, &ra, &n, &pa, &sca, &move, &maxSteps, &pin};
         CK(cudaLaunchCooperativeKernel((const void *)oc_kernel, dim3(o.ocBlocks), dim3(256), args, 0, st));
         TOPGPU_COUNT_LAUNCH();
     }
@@ -921,6 +954,7 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
     if (o.prm.ft == 2 && s->super) { rc = sfilter_apply(s, o.xd, o.xPhys, 1); if (rc) return rc; }   // 262-265
     else if (o.prm.ft == 2) { rc = filter_apply(s, o.xd, o.xPhys, &fits); if (rc) return rc; }
     else { copy_kernel<<<VB, 256, 0, st>>>(o.xd, o.xPhys, Ne); TOPGPU_COUNT_LAUNCH(); }
+    if (o.nPassive > 0) { pin_kernel<<<VB, 256, 0, st>>>(o.xPhys, o.passive, Ne); TOPGPU_COUNT_LAUNCH(); }
     sum_kernel<<<VB, 256, 0, st>>>(o.xPhys, Ne, 1, s->red(&o.sc->sharp));
     TOPGPU_COUNT_LAUNCH();
     CK(cudaEventRecord(ev[6], st));

@@ -67,11 +67,7 @@ def _model(input_model, optCase, super_element):
         return m
     if super_element:
         raise ValueError("super_element = 1 needs a box domain given as a logical array")
-    m = Mesh.from_topvoxel(input_model, control=SETTINGS["control"], nu=SETTINGS["nu"])
-    if m.passive_elements.size:
-        raise NotImplementedError("%d passive elements in %s: the device optimisation loop does not apply "
-                                  "passive elements yet" % (m.passive_elements.size, input_model))
-    return m
+    return Mesh.from_topvoxel(input_model, control=SETTINGS["control"], nu=SETTINGS["nu"])
 
 
 def TOP_GPU(input_model, optCase=1, V0=0.12, rMin=math.sqrt(3), nLoop=50, ft=1, mixed_Precision=0,
@@ -99,6 +95,9 @@ def TOP_GPU(input_model, optCase=1, V0=0.12, rMin=math.sqrt(3), nLoop=50, ft=1, 
     s = solver_class(mesh, E0=SETTINGS["E0"], Emin=SETTINGS["Emin"], penal=SETTINGS["penal"], tol=SETTINGS["tol"],
                      maxIT=SETTINGS["maxIT"], omega=SETTINGS["omega"], mixed=bool(mixed_Precision),
                      outer_fp32=bool(outer_fp32))
+    passive = getattr(mesh, "passive_elements", None)
+    if passive is not None and passive.size:
+        s.set_passive(passive)                                     # TOP_GPU.m:123-125
     t_start = time.perf_counter()
     c_solid = s.opt_begin(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
     say("Compliance of Fully Solid Domain: %16.6e" % c_solid)

@@ -260,6 +260,12 @@ class Solver:
         check(lib().top_solver_filter(self._h, src.data_ptr(), out.data_ptr(), C.byref(its)), "top_solver_filter")
         return out, its.value
 
+    def set_passive(self, ids):
+        """Passive elements (compact 1-based ids, e.g. Mesh.passive_elements):
+        design 1 in the OC update and after the filter (TOP_GPU.m:239, 270)."""
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        check(lib().top_solver_set_passive(self._h, _p(ids) if ids.size else None, ids.size), "top_solver_set_passive")
+
     def opt_begin(self, V0=0.12, rMin=np.sqrt(3), nLoop=50, ft=1):
         self._opt = OptParams(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
         cs = C.c_double(0)
