@@ -1070,11 +1070,22 @@ void orc_vcycle(OModel *m, const double *r, double *x)
 /* ------------------------------------------------------------------------ */
 /* PCG (Solving_PCG, TOP_GPU.m:602-667)                                       */
 typedef void (*op_fn)(OModel *, const double *, double *);
+/* 64 fixed index ranges summed in order: the same value on every run and for
+ * any number of threads (an OpenMP reduction combines its partials in no
+ * fixed order) */
 static double dotp(const double *a, const double *b, int64_t n)
 {
+    enum { NC = 64 };
+    double part[NC];
+    #pragma omp parallel for schedule(static)
+    for (int c = 0; c < NC; ++c) {
+        const int64_t lo = n * c / NC, hi = n * (c + 1) / NC;
+        double t = 0;
+        for (int64_t i = lo; i < hi; ++i) t += a[i] * b[i];
+        part[c] = t;
+    }
     double s = 0;
-    #pragma omp parallel for reduction(+:s) schedule(static)
-    for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+    for (int c = 0; c < NC; ++c) s += part[c];
     return s;
 }
 static int pcg_generic(OModel *m, op_fn A, op_fn M, int64_t n, const double *b, double *y,
