@@ -268,6 +268,10 @@ int top_solver_opt_begin(top_solver *s, const top_opt_params *prm, double *cSoli
 int top_solver_set_passive(top_solver *s, const int32_t *ids, int64_t n);
 int top_solver_opt_step(top_solver *s, top_opt_record *rec);
 int top_solver_opt_state(top_solver *s, int *loop, double *change, double *sharpness);
+/* PCG iterations of each load case in the last state solves (the record's
+ * pcgIts is their sum; the reference lists them per case, lssIts,
+ * TOP_GPU.m:186): copies min(capacity, nLoads) counts, *count = nLoads. */
+int top_solver_opt_case_its(top_solver *s, int *its, int capacity, int *count);
 /* get/set copy the physical and raw designs (either may be NULL) to/from
  * device or host memory (any pointer CUDA's unified addressing accepts);
  * set_design replaces the state the next opt_step starts from. */

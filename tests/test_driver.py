@@ -39,6 +39,9 @@ class ScriptedSolver:
     def opt_state(self):
         return self.k, 0.2 / self.k, 0.5 / self.k
 
+    def opt_case_its(self):                      # two load cases splitting the record's count
+        return [5, 5 + self.k]
+
     def design(self):
         x = np.linspace(0.0, 1.0, self.ne)
         return x, x
@@ -81,7 +84,8 @@ def test_run_writes_the_reference_files(tmp_path):
     log = open(os.path.join(out["path"], "RunLog.log")).read().splitlines()
     assert log[1] == "Compliance of Fully Solid Domain:     1.235000e+02"
     assert sum(l.startswith(" It.:") for l in log) == 2 * 8
-    assert open(os.path.join(out["path"], "iters_Target.dat")).read().split() == [str(10 + k) for k in range(1, 9)]
+    iters = open(os.path.join(out["path"], "iters_Target.dat")).read().split()
+    assert iters == [str(v) for k in range(1, 9) for v in (5, 5 + k)]      # per load case, per iteration
 
 
 def test_loop_stops_on_sharpness(tmp_path):

@@ -111,6 +111,7 @@ SIGNATURES = {
     "top_solver_set_passive": (_int, [_vp, _vp, _i64]),
     "top_solver_opt_step": (_int, [_vp, _vp]),
     "top_solver_opt_state": (_int, [_vp, _vp, _vp, _vp]),
+    "top_solver_opt_case_its": (_int, [_vp, _vp, _int, _vp]),
     "top_solver_get_design": (_int, [_vp, _vp, _vp]),
     "top_solver_set_design": (_int, [_vp, _vp, _vp]),
     "top_solver_launch_count": (_int, [_vp, _vp]),

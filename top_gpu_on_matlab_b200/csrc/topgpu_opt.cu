@@ -74,6 +74,7 @@ struct OptState {
     // passive elements: 1 on the design variables held at 1 (TOP_GPU.m:239, 270;
     // super elements: sub-voxel row Num_ = 4, 247, 273); used when nPassive > 0
     uint8_t *passive = nullptr; int64_t passiveLen = 0, nPassive = 0;
+    std::vector<int> caseIts;   // PCG iterations per load case of the last state solves
 };
 
 }  // namespace topgpu
@@ -757,6 +758,7 @@ static int solve_all(top_solver *s, int warm, int *itsTotal)
     int tot = 0;
     for (int k = 0; k < s->nLoads; ++k) tot += its[k];
     if (itsTotal) *itsTotal = tot;
+    o.caseIts.assign(its.begin(), its.begin() + s->nLoads);
     return TOP_OK;
 }
 
@@ -980,6 +982,16 @@ extern "C" int top_solver_opt_step(top_solver *s, top_opt_record *rec)
         cudaEventElapsedTime(&tot, ev[0], ev[6]);
         rec->msTotal = tot;
     }
+    return TOP_OK;
+}
+
+extern "C" int top_solver_opt_case_its(top_solver *s, int *its, int capacity, int *count)
+{
+    if (!s || capacity < 0 || (capacity > 0 && !its)) { set_error("top_solver_opt_case_its: bad arguments"); return TOP_ERR_ARGS; }
+    if (!s->optState) { set_error("top_solver_opt_case_its: no state solves yet"); return TOP_ERR_STATE; }
+    const std::vector<int> &v = opt(s).caseIts;
+    if (count) *count = (int)v.size();
+    for (int k = 0; k < capacity && k < (int)v.size(); ++k) its[k] = v[k];
     return TOP_OK;
 }
 

@@ -101,12 +101,13 @@ def TOP_GPU(input_model, optCase=1, V0=0.12, rMin=math.sqrt(3), nLoop=50, ft=1, 
     t_start = time.perf_counter()
     c_solid = s.opt_begin(V0=V0, rMin=rMin, nLoop=nLoop, ft=ft)
     say("Compliance of Fully Solid Domain: %16.6e" % c_solid)
-    history = []
+    history, iters = [], []
     loop, change, sharp = 0, 1.0, 1.0
     while loop < nLoop and change > 0.0001 and sharp > 0.01:       # TOP_GPU.m:177
         rec = s.opt_step()
         loop, change, sharp = s.opt_state()
         history.append(rec)
+        iters.extend(s.opt_case_its())                             # lssIts, one per load case
         for text in iteration_lines(loop, rec):
             say(text)
     xphys, _ = s.design()          # [Ne], or [64 x Ne] column-major for super elements
@@ -115,7 +116,7 @@ def TOP_GPU(input_model, optCase=1, V0=0.12, rMin=math.sqrt(3), nLoop=50, ft=1, 
     say("..........Optimization (inc. sentivity analysis, update) Costs: %10.4es." % t("msOpt"))
     say("..........Performing PDE Filtering Costs: %10.4es." % t("msFilter"))
     say("..........Performing Topology Optimization Costs (in total): %10.4es." % (time.perf_counter() - t_start))
-    results.write_results(path, mesh, xphys, history)
+    results.write_results(path, mesh, xphys, history, iters)
     with open(os.path.join(path, "RunLog.log"), "w") as f:
         f.write("\n".join(lines) + "\n")
     return dict(xPhys=xphys, history=history, cSolid=c_solid, path=path)

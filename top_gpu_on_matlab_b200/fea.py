@@ -277,6 +277,13 @@ class Solver:
         check(lib().top_solver_opt_step(self._h, C.byref(rec)), "top_solver_opt_step")
         return {k: getattr(rec, k) for k, _ in OptRecord._fields_}
 
+    def opt_case_its(self):
+        """PCG iterations per load case in the last opt_step's state solves."""
+        its = (C.c_int * max(1, self.nLoads))()
+        n = C.c_int(0)
+        check(lib().top_solver_opt_case_its(self._h, its, len(its), C.byref(n)), "top_solver_opt_case_its")
+        return [its[k] for k in range(n.value)]
+
     def opt_state(self):
         loop, ch, sh = C.c_int(0), C.c_double(0), C.c_double(0)
         check(lib().top_solver_opt_state(self._h, C.byref(loop), C.byref(ch), C.byref(sh)), "top_solver_opt_state")

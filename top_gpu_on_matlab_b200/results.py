@@ -17,8 +17,9 @@ msSolve, msTotal, pcgIts as returned by Solver.opt_step / Solver.optimize);
 times there are milliseconds and are written in seconds, like the
 reference's tic/toc.  The reference lists PCG iterations once per load case
 and iteration; a record holds their sum over the load cases, so
-iters_Target.dat takes per-solve counts when given (`iters`) and the
-record's count otherwise (the same for one load case).
+iters_Target.dat takes the per-case counts when given (`iters`, from
+Solver.opt_case_its, as the driver passes them) and the record's count
+otherwise (the same for one load case).
 """
 import json
 import math
