@@ -36,8 +36,13 @@ def node_index(y, x, z, shape):
 
 
 def _rows(f, rows, fmt):
-    for r in rows:
-        f.write(fmt % tuple(r) + "\n")
+    if len(rows):
+        f.write("\n".join(fmt % tuple(r) for r in rows) + "\n")
+
+
+def _load_rows(f, rows):
+    if len(rows):
+        f.write("\n".join("%d %.17g %.17g %.17g" % (int(r[0]), r[1], r[2], r[3]) for r in rows) + "\n")
 
 
 def write_topvoxel(path, mask, fixations, loads, passive=(), density=None):
@@ -71,10 +76,10 @@ def write_topvoxel(path, mask, fixations, loads, passive=(), density=None):
         f.write("Density values: %d\n" % (density is not None))
         f.write("Solid voxels: %d\n" % solid.size)
         if density is None:
-            _rows(f, solid[:, None], "%d")
-        else:
-            for v, d in zip(solid, density):
-                f.write("%d %.17g\n" % (v, d))
+            if solid.size:
+                f.write("\n".join(map(str, solid.tolist())) + "\n")
+        elif solid.size:
+            f.write("\n".join("%d %.17g" % vd for vd in zip(solid.tolist(), density.tolist())) + "\n")
         passive = np.asarray(passive, dtype=np.int64).ravel()
         f.write("Passive elements: %d\n" % passive.size)
         if passive.size:
@@ -82,10 +87,8 @@ def write_topvoxel(path, mask, fixations, loads, passive=(), density=None):
         f.write("Fixations: %d\n" % len(fixations))
         _rows(f, fixations, "%d %d %d %d")
         f.write("Loads: %d\n" % len(loads[0]))
-        for r in loads[0]:
-            f.write("%d %.17g %.17g %.17g\n" % (int(r[0]), r[1], r[2], r[3]))
+        _load_rows(f, loads[0])
         f.write("Additional loads: %d\n" % len(more))
         for case, l in more:
             f.write("Loads: %d %d\n" % (len(l), case))
-            for r in l:
-                f.write("%d %.17g %.17g %.17g\n" % (int(r[0]), r[1], r[2], r[3]))
+            _load_rows(f, l)
