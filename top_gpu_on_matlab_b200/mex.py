@@ -81,6 +81,13 @@ def _need(name, t, what):
     return t
 
 
+def _need_all(name, **tensors):
+    """_need on every given tensor (None: an optional argument left out)."""
+    for what, t in tensors.items():
+        if t is not None:
+            _need(name, t, what)
+
+
 def _dtype_code(name, t, what):
     if t.dtype == torch.float64:
         return TOP_F64
@@ -172,6 +179,8 @@ def _opt(t):
 
 def assembleKs_level2_inplace(d_Ks, d_upMap, d_eleModulus, d_K_0, d_Pch, d_mapUnique, d_uniqueFree, d_uniqueFixed):
     n = "assembleKs_level2_inplace"
+    _need_all(n, d_Ks=d_Ks, d_upMap=d_upMap, d_eleModulus=d_eleModulus, d_K_0=d_K_0, d_Pch=d_Pch,
+              d_mapUnique=d_mapUnique, d_uniqueFree=d_uniqueFree, d_uniqueFixed=d_uniqueFixed)
     cls = _dtype_code(n, d_Ks, "d_Ks")
     if d_upMap.dtype != torch.int32 or d_mapUnique.dtype != torch.int32:
         _err(n, TOP_ERR_TYPE, "d_upMap and d_mapUnique must be int32 gpuArray.")
@@ -214,6 +223,7 @@ def assembleKs_level2_inplace(d_Ks, d_upMap, d_eleModulus, d_K_0, d_Pch, d_mapUn
 
 def assembleKs_higherLevel_inplace(d_Ks, d_upMap, d_KsPrev, d_Psub):
     n = "assembleKs_higherLevel_inplace"
+    _need_all(n, d_Ks=d_Ks, d_upMap=d_upMap, d_KsPrev=d_KsPrev, d_Psub=d_Psub)
     cls = _dtype_code(n, d_Ks, "d_Ks")
     if d_upMap.dtype != torch.int32:
         _err(n, TOP_ERR_TYPE, "d_upMap must be int32 gpuArray.")
@@ -240,6 +250,8 @@ def assembleKs_higherLevel_inplace(d_Ks, d_upMap, d_KsPrev, d_Psub):
 
 def assembleKs_level2_superEle_inplace(d_Ks, d_upMap, d_Ks0, d_Psub, d_mapUnique, d_eleModulus, d_uniqueFree, d_uniqueFixed):
     n = "assembleKs_level2_superEle_inplace"
+    _need_all(n, d_Ks=d_Ks, d_upMap=d_upMap, d_Ks0=d_Ks0, d_Psub=d_Psub, d_mapUnique=d_mapUnique,
+              d_eleModulus=d_eleModulus, d_uniqueFree=d_uniqueFree, d_uniqueFixed=d_uniqueFixed)
     cls = _dtype_code(n, d_Ks, "d_Ks")
     if d_upMap.dtype != torch.int32 or d_mapUnique.dtype != torch.int32:
         _err(n, TOP_ERR_TYPE, "d_upMap and d_mapUnique must be int32 gpuArray.")
