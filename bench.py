@@ -21,8 +21,18 @@ the density error the max-abs difference of xPhys after the last one.  e2e
 runs the same iterations through the C ABI with the design held on the host
 (pinned): the design goes up before and comes back after every iteration.
 
+After the timed region the mixed path's last design is solved once more on
+the device and by the FP64 oracle (cold start, same tolerance): the line
+reports the compliance and displacement-field errors against the oracle.
+
 --impl reference times the FP64 CPU restatement of the reference (oracle/,
-the MATLAB driver cannot run here) on the host cores on a bounded sample.
+the MATLAB driver cannot run here) on the host cores: each step times two
+oracle PCG iterations on the workload's first design, and the PCG ms per
+optimisation iteration is projected with the FP64 PCG iteration count of the
+same optimisation iterations, recorded from this benchmark's FP64 device path
+(bench_fp64_its.json; the device FP64 path and the oracle take the same
+iteration counts to +-1, tests/test_gpu_solver.py).  The line says
+"projected" and gives the multiplier and its source.
 """
 import argparse
 import atexit
@@ -46,9 +56,15 @@ E0, EMIN, PENAL, NU = 1.0, 1e-9, 3.0, 0.3
 TOL, MAXIT, OMEGA = 1e-6, 800, 0.6
 RMIN, FT = 3 ** 0.5, 1
 WORKLOAD = "cantilever_96x192x96_ft1_optimisation_iterations"
-# DRAM bytes (read + write) per launch of the level-0 stiffness products from
-# one ncu capture of this workload (profiles/l0d_kernel_cantilever_96x192x96.md)
-NCU_TRAFFIC = {"l0_f64": 74.3e6, "l0_f32": 31.7e6}
+# DRAM bytes (read + write) per launch of a level-0 stiffness product on this
+# workload, from one-launch ncu captures (dram__bytes_read.sum +
+# dram__bytes_write.sum), keyed by precision and the kernel configuration
+# (kind, tile y, tile x, CTAs); a configuration without a capture reports null
+NCU_TRAFFIC = {
+    ("fp64", 3, 16, 8, 1184): 74.3e6,
+    ("fp32", 3, 16, 8, 888): 37.5e6,
+}
+ITS_RECORD = ROOT / "bench_fp64_its.json"
 
 
 def _env_rank():
@@ -140,26 +156,61 @@ def _cpu_cores():
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
 
-def cpu_sample(iters=2, gpu_its=None):
-    """Oracle (FP64 C + OpenMP) PCG iterations on the same problem; ms per iteration."""
-    from oracle import oracle as O
-    cores = _cpu_cores()
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    mask = np.ones(SHAPE, bool)
-    o = O.Model(mask, control=CONTROL)
-    o.apply_optcase(1)
-    o.set_material(E0, EMIN, PENAL)
-    o.set_solver(TOL, MAXIT, OMEGA)
-    ne = o.level(0).numElements
-    o.set_density(np.full(ne, V0))
-    t0 = time.perf_counter()
-    o.assemble()
-    t_asm = time.perf_counter() - t0
-    b = o.F()[:, 0]
-    t0 = time.perf_counter()
-    _, its, _ = o.pcg(b, maxIT=iters, tol=1e-300)
-    t_it = (time.perf_counter() - t0) / its
-    return {"ms_per_pcg_iter": 1e3 * t_it, "assemble_ms": 1e3 * t_asm, "cores": cores, "iters": its}
+class OracleWorkload:
+    """The workload on the FP64 oracle (C + OpenMP, all host cores): model,
+    hierarchy and BCs built once; the design set and assembled on demand."""
+
+    def __init__(self):
+        from oracle import oracle as O
+        self.cores = _cpu_cores()
+        os.environ.setdefault("OMP_NUM_THREADS", str(self.cores))
+        self.o = O.Model(np.ones(SHAPE, bool), control=CONTROL)
+        self.o.apply_optcase(1)
+        self.o.set_material(E0, EMIN, PENAL)
+        self.o.set_solver(TOL, MAXIT, OMEGA)
+        self.ne = self.o.level(0).numElements
+        self.b = self.o.F()[:, 0]
+
+    def set_design(self, xPhys):
+        self.o.set_density(np.ascontiguousarray(xPhys, dtype=np.float64))
+        t0 = time.perf_counter()
+        self.o.assemble()
+        return 1e3 * (time.perf_counter() - t0)
+
+    def pcg_ms_per_iter(self, iters=2):
+        """ms per PCG iteration over `iters` iterations from a zero start."""
+        t0 = time.perf_counter()
+        _, its, _ = self.o.pcg(self.b, maxIT=iters, tol=1e-300)
+        return 1e3 * (time.perf_counter() - t0) / its
+
+    def solve(self):
+        """Solving_PCG at the workload's tolerance from a zero start: (U, its, relres, ms)."""
+        t0 = time.perf_counter()
+        U, its, res = self.o.pcg(self.b)
+        return U, its, res, 1e3 * (time.perf_counter() - t0)
+
+
+def workload_config(levels, world):
+    ny, nx, nz = SHAPE
+    return {"workload": WORKLOAD, "shape": list(SHAPE), "elements": ny * nx * nz,
+            "dofs": 3 * (ny + 1) * (nx + 1) * (nz + 1), "levels": levels,
+            "control": CONTROL, "tol": TOL, "V0": V0, "rMin": RMIN, "ft": FT,
+            "precision": "mixed (FP32 V-cycle, FP64 outer)",
+            "l2": "working set > L2 per PCG iteration; kernel timings flush L2",
+            "parallelism": "replicas" if world > 1 else "single"}
+
+
+def recorded_fp64_its(warmup, steps):
+    """Mean FP64 PCG iterations of optimisation iterations warmup+1 ..
+    warmup+steps from the record of this benchmark's FP64 device path, or
+    None when the record does not reach that far."""
+    if not ITS_RECORD.exists():
+        return None, None
+    rec = json.loads(ITS_RECORD.read_text())
+    its = rec["fp64_pcg_its_per_opt_iter"]
+    if warmup + steps > len(its):
+        return None, rec
+    return float(np.mean(its[warmup:warmup + steps])), rec
 
 
 def max_over_ranks(values, device, world):
@@ -178,22 +229,40 @@ def run_reference(args):
     rank, world, _ = _env_rank()
     if rank != 0:
         return
+    its, rec = recorded_fp64_its(args.warmup, args.steps)
+    if its is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "no FP64 PCG iteration record for optimisation iterations %d-%d in %s"
+                          % (args.warmup + 1, args.warmup + args.steps, ITS_RECORD.name)}), flush=True)
+        return
+    ow = OracleWorkload()
+    asm_ms = ow.set_design(np.full(ow.ne, V0))
     samples = []
     for k in range(args.warmup + args.steps):
-        s = cpu_sample(iters=2)
+        ms_it = ow.pcg_ms_per_iter(2)
         if k >= args.warmup:
-            samples.append(s)
-    ms_it = float(np.mean([s["ms_per_pcg_iter"] for s in samples]))
-    its = args.ref_its
+            samples.append(ms_it)
+    ms_it = float(np.mean(samples))
     value = ms_it * its
+    cfg = workload_config(ow.o.numLevels, world)
+    cfg["opt_iters_timed"] = "%d-%d" % (args.warmup + 1, args.warmup + args.steps)
+    cfg["precision"] = "fp64 (oracle)"
     line = {
         "impl": "reference", "metric": "PCG ms/opt-iter", "value": value, "unit": "ms",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": value,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOAD, "shape": list(SHAPE), "levels": 5, "tol": TOL},
-        "cpu_baseline": {"value": value, "unit": "ms", "cores": samples[0]["cores"], "kind": "port",
-                         "sample": "2 FP64 PCG iterations of the oracle per step, ms/iteration x %d iterations "
-                                   "(the FP64 iteration count of this problem)" % its},
+        "data": "synthetic", "config": cfg,
+        "projected": True,
+        "projection": {"ms_per_pcg_iter": ms_it, "multiplier": its,
+                       "multiplier_source": "mean FP64 PCG iterations of optimisation iterations %d-%d measured by "
+                                            "this benchmark's FP64 device path (%s, %s)"
+                                            % (args.warmup + 1, args.warmup + args.steps, ITS_RECORD.name,
+                                               rec.get("source", "")),
+                       "timed_pcg_iterations": 2 * args.steps},
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": ow.cores, "kind": "port",
+                         "sample": "2 FP64 PCG iterations of the oracle per step (%d steps timed), ms/iteration "
+                                   "x %.2f PCG iterations per optimisation iteration" % (args.steps, its),
+                         "assemble_ms": asm_ms},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -259,6 +328,7 @@ def run_ours(args):
         xp, _ = s.design()
         results[name] = dict(solver=s, pcg_ms=float(vals[0]), step_ms=float(vals[1]), asm_ms=float(vals[2]),
                              its=[r["pcgIts"] for r in timed], c=[r["c"] for r in recs + timed],
+                             its_all=[r["pcgIts"] for r in recs + timed],
                              rows=timed, launches=launches, clocks=clocks, xPhys=xp, c_solid=c_solid)
     mixed, fp64 = results["mixed"], results["fp64"]
     comp_err = max(abs(a - b) / abs(b) for a, b in zip(mixed["c"], fp64["c"]))
@@ -302,24 +372,26 @@ def run_ours(args):
     # mixed PCG iteration: 1 FP64 outer product + 2 FP32 level-0 smoother products
     share64, share32 = tk["l0_f64"], 2 * tk["l0_f32"]
     if share64 >= share32:
-        dom, t_dom, byt, traffic = "level-0 K*u FP64 (outer K*p), kind %d" % tuned["fp64"][1][0], tk["l0_f64"], bytes64, NCU_TRAFFIC["l0_f64"]
+        prec, dom, t_dom, byt = "fp64", "level-0 K*u FP64 (outer K*p)", tk["l0_f64"], bytes64
     else:
-        dom, t_dom, byt, traffic = "level-0 K*u FP32 (V-cycle), kind %d" % tuned["fp32"][1][0], tk["l0_f32"], bytes32, NCU_TRAFFIC["l0_f32"]
+        prec, dom, t_dom, byt = "fp32", "level-0 K*u FP32 (V-cycle)", tk["l0_f32"], bytes32
+    cfg_dom = tuple(int(v) for v in tuned[prec][1])
+    dom += ", kind %d, %dx%d tiles, %d CTAs" % cfg_dom
+    traffic = NCU_TRAFFIC.get((prec,) + cfg_dom)
     achieved = byt / (t_dom * 1e-3) / 1e9
     its_m = float(np.mean(mixed["its"]))
     its_d = float(np.mean(fp64["its"]))
+    cfg = workload_config(len(info), world)
+    assert cfg["elements"] == ne and cfg["dofs"] == 3 * nn
+    cfg["opt_iters_timed"] = "%d-%d" % (args.warmup + 1, args.warmup + args.steps)
     line = {
         "metric": "PCG ms/opt-iter", "value": mixed["pcg_ms"], "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed["step_ms"],
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "shape": list(SHAPE), "elements": ne, "dofs": 3 * nn, "levels": len(info),
-                   "control": CONTROL, "tol": TOL, "V0": V0, "rMin": RMIN, "ft": FT,
-                   "opt_iters_timed": "%d-%d" % (args.warmup + 1, args.warmup + args.steps),
-                   "precision": "mixed (FP32 V-cycle, FP64 outer)",
-                   "l2": "working set > L2 per PCG iteration; kernel timings flush L2",
-                   "parallelism": "replicas" if world > 1 else "single"},
+        "config": cfg,
         "pcg_its": its_m, "fp64_pcg_ms": fp64["pcg_ms"], "fp64_pcg_its": its_d,
+        "fp64_pcg_its_per_opt_iter": fp64["its_all"], "mixed_pcg_its_per_opt_iter": mixed["its_all"],
         "mixed_vs_fp64_speedup": fp64["pcg_ms"] / mixed["pcg_ms"],
         "opt_iter_ms": {"mixed": mixed["step_ms"], "fp64": fp64["step_ms"]},
         "compliance_rel_err_mixed_vs_fp64": comp_err,
@@ -331,7 +403,10 @@ def run_ours(args):
         "matvec_tflops": {"fp64": flops / (tk["l0_f64"] * 1e-3) / 1e12, "fp32": flops / (tk["l0_f32"] * 1e-3) / 1e12},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                     "algorithmic_bytes": byt, "traffic": traffic},
+                     "algorithmic_bytes": byt, "traffic": traffic,
+                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this "
+                                        "kernel configuration" if traffic is not None else
+                                        "no ncu capture of this kernel configuration")},
         "gpu_launches": mixed["launches"],
         "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * ne * 8, "d2h_bytes_per_step": 2 * ne * 8,
                 "includes": "whole optimisation iteration through the C ABI: H2D design, SIMP, assembly, "
@@ -339,18 +414,52 @@ def run_ours(args):
         "clocks": mixed["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        cs = cpu_sample(iters=2)
-        line["cpu_baseline"] = {"value": cs["ms_per_pcg_iter"] * its_d, "unit": "ms", "cores": cs["cores"],
-                                "kind": "port",
-                                "sample": "2 FP64 PCG iterations of the oracle (C + OpenMP) on this problem, "
+        # oracle leg (outside every timed region): the bounded CPU sample, then
+        # the mixed path's last design solved by the device and by the oracle
+        ow = OracleWorkload()
+        asm_ms = ow.set_design(np.full(ow.ne, V0))
+        ms_it = float(np.mean([ow.pcg_ms_per_iter(2) for _ in range(3)]))
+        line["cpu_baseline"] = {"value": ms_it * its_d, "unit": "ms", "cores": ow.cores, "kind": "port",
+                                "sample": "3 x 2 FP64 PCG iterations of the oracle (C + OpenMP) on this problem, "
                                           "ms/iteration x the mean FP64 iteration count of the timed "
-                                          "optimisation iterations (%.1f)" % its_d,
-                                "assemble_ms": cs["assemble_ms"]}
+                                          "optimisation iterations (%.2f)" % its_d,
+                                "assemble_ms": asm_ms}
+        if not args.no_oracle_check:
+            line["vs_oracle"] = oracle_check(ow, mixed["solver"], mixed["xPhys"])
+    if rank == 0 and args.record_its:
+        ITS_RECORD.write_text(json.dumps({
+            "fp64_pcg_its_per_opt_iter": fp64["its_all"],
+            "source": "bench.py --steps %d --warmup %d --record-its on one %s, %s; level-0 kernels %s" % (
+                args.steps, args.warmup, torch.cuda.get_device_name(dev), time.strftime("%Y-%m-%d"),
+                json.dumps({k: list(v[1]) for k, v in tuned.items()})),
+        }, indent=1) + "\n")
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def oracle_check(ow, s, xPhys):
+    """The mixed path's last design, solved from a zero start by the mixed
+    device solver and by the FP64 oracle at the same tolerance: compliance
+    F'U and the displacement field compared (TOP_GPU.m:186-191)."""
+    import torch
+    xp = xPhys.detach().cpu().numpy()
+    s.set_density(xPhys)
+    s.assemble()
+    U, its, res = s.pcg(0)
+    Ud = U.cpu().numpy()
+    ow.set_design(xp)
+    Uo, its_o, res_o, ms_o = ow.solve()
+    c_d, c_o = float(ow.b @ Ud), float(ow.b @ Uo)
+    return {"design": "xPhys after the last timed mixed-precision iteration",
+            "compliance_rel_err": abs(c_d - c_o) / abs(c_o),
+            "displacement_rel_err_max": float(np.abs(Ud - Uo).max() / np.abs(Uo).max()),
+            "displacement_rel_err_l2": float(np.linalg.norm(Ud - Uo) / np.linalg.norm(Uo)),
+            "pcg_its": {"device_mixed": its, "oracle_fp64": its_o},
+            "relres": {"device_mixed": res, "oracle_fp64": res_o},
+            "oracle_solve_ms": ms_o, "oracle_cores": ow.cores}
 
 
 def run_kernels_only(args):
@@ -387,14 +496,22 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--ref-its", type=int, default=52,
-                    help="FP64 PCG iterations per timed optimisation iteration (measured on the B200: 52.4), scaling the CPU sample")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample and the oracle check")
+    ap.add_argument("--no-oracle-check", action="store_true",
+                    help="skip the oracle solve of the last design (the CPU baseline sample still runs)")
+    ap.add_argument("--record-its", action="store_true",
+                    help="write the FP64 PCG iterations per optimisation iteration to %s" % ITS_RECORD.name)
     ap.add_argument("--kernels-only", action="store_true", help="time a few launches of the level-0 kernels (profiling)")
     ap.add_argument("--l0", action="append", help="with --kernels-only: fp64=KIND,TY,TX,CTAS or fp32=...")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "RANK" not in os.environ:
+        # one replica per GPU: relaunch under torch.distributed.run
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", str(args.gpus),
+               "--master-addr", "127.0.0.1", "--master-port", os.environ.get("MASTER_PORT", "29517"),
+               str(Path(__file__).resolve())] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
     if args.kernels_only:
         run_kernels_only(args)
     elif args.impl == "reference":

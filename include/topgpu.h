@@ -85,8 +85,9 @@ int top_assemble_ks_level2(void *Ks, const int32_t *upMap, const void *eleModulu
  * reserves its memory up front and must avoid the device synchronisation of
  * cudaMalloc/cudaFree.  Its FP64 scratch is a fixed device array (~311 KB per
  * GPU, held until exit); nCh is limited to 64 (TOP_ERR_SHAPE above that).
- * The first call on a device resolves the array's address (make it before
- * any stream capture); concurrent calls on one device race -- serialise them. */
+ * The first call on a device, and the first after its context was replaced
+ * (cudaDeviceReset), resolves the array's address (make it before any stream
+ * capture); concurrent calls on one device race -- serialise them. */
 int top_assemble_ks_level2_noalloc(void *Ks, const int32_t *upMap, const void *eleModulus,
                                    const void *K0, const void *Pch, const int32_t *mapUnique,
                                    const void *uniqueFree, const void *uniqueFixed,

@@ -99,11 +99,39 @@ def test_vcycle_fp64(pair):
     assert _rel(s.vcycle(torch.from_numpy(r).cuda()), o.vcycle(r)) < 1e-11
 
 
+_SMOOTHED = set()
+
+
 def _smooth_only(pair):
-    # i.i.d. random moduli (contrast 8000) make the reference's damped-Jacobi
-    # V-cycle (omega 0.6) indefinite; PCG parity runs on smooth designs
-    if pair[3] != "smooth":
-        pytest.skip("PCG parity on the smooth design")
+    """PCG parity runs on a smooth design on every model: i.i.d. random moduli
+    (contrast 8000) make the reference's damped-Jacobi V-cycle (omega 0.6)
+    indefinite, in the oracle as on the device.  A model set up with the
+    i.i.d. design is switched (oracle and device alike) to the smooth one."""
+    o, s, _, kind = pair
+    if kind == "smooth" or id(s) in _SMOOTHED:
+        return
+    L0 = o.level(0)
+    x = smooth_design(L0, L0.resY, L0.resX)
+    o.set_density(x)
+    o.assemble()
+    s.set_density(torch.from_numpy(x).cuda())
+    s.assemble()
+    _SMOOTHED.add(id(s))
+
+
+def _oracle_spread(o, b, seeds=(1, 2, 3), eps=1e-15):
+    """The oracle's own sensitivity to rounding: PCG on b perturbed by eps
+    (relative, seeded) -- (min, max) iterations and the compliance spread.
+    On slowly converging models (the irregular mask needs ~630 iterations)
+    a 1e-15 perturbation already moves the oracle's iteration count by
+    tens and its compliance by ~1e-9; parity is asked for within that band."""
+    its, cs = [], []
+    for sd in seeds:
+        bb = b * (1 + eps * np.random.default_rng(sd).standard_normal(b.size))
+        xo, it, _ = o.pcg(bb)
+        its.append(it)
+        cs.append(b @ xo)
+    return min(its), max(its), max(cs) - min(cs)
 
 
 def test_pcg_fp64_matches_oracle(pair):
@@ -112,11 +140,16 @@ def test_pcg_fp64_matches_oracle(pair):
     b = o.F()[:, 0]
     xo, its_o, res_o = o.pcg(b)
     U, its, res = s.pcg(0)
-    assert abs(its - its_o) <= 1, (its, its_o)
-    assert res < 1e-6
-    # compliance F'U
-    c_o, c = b @ xo, float(torch.from_numpy(b).cuda() @ U)
-    assert abs(c - c_o) <= 1e-9 * abs(c_o)
+    assert res < 1e-6 and res_o < 1e-6
+    c_o, c = b @ xo, float(torch.from_numpy(b).cuda() @ U)      # compliance F'U
+    lo, hi, dc = _oracle_spread(o, b)
+    print("PCG its device %d, oracle %d (oracle under 1e-15 perturbations: %d..%d); compliance rel diff %.2e "
+          "(oracle spread %.2e)" % (its, its_o, lo, hi, abs(c - c_o) / abs(c_o), dc / abs(c_o)))
+    # iterations within +-1 of the oracle, or within the oracle's own rounding band
+    band = max(1, 2 * (hi - lo))
+    assert min(its_o, lo) - band <= its <= max(its_o, hi) + band, (its, its_o, lo, hi)
+    # compliance within 1e-9, or within twice the oracle's own spread
+    assert abs(c - c_o) <= max(1e-9 * abs(c_o), 2 * dc)
 
 
 def test_pcg_graphs_match_launches(pair):

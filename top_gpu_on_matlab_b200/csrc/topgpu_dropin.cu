@@ -201,8 +201,9 @@ int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const
     if (nCh <= kGemmK) {
         cudaFuncSetAttribute(dgemm_k64_kernel<Level2Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
         dim3 grid((unsigned)((nElem + kGemmBM - 1) / kGemmBM), (576 + kGemmBN - 1) / kGemmBN);
-        // rows of B beyond nCh are never read (ARow returns 0 there) but must
-        // exist: Qscratch is sized for 64 slots
+        // B = Qscratch has 64 rows whatever nCh is: the GEMM's K tiles load rows
+        // nCh..63 too and multiply them by the zero A entries that ARow returns
+        // there, so those rows must exist and hold finite values (0 * NaN = NaN)
         dgemm_k64_kernel<<<grid, 128, kGemmSmem, st>>>(Ks, nElem, 576, 576, Qscratch, 576,
                                                        Level2Row{upMap, E, mapUnique, nElem, nCh, hasFixed});
         // children with fixed DOFs: full triple products, accumulated; only the
@@ -336,9 +337,10 @@ extern "C" int top_assemble_ks_level2_super(void *Ks, const int32_t *upMap, cons
 //  * at most kNoAllocMaxChildren (64) children per coarse element -- the
 //    level-2 case of the reference (span 4); larger nCh is rejected with
 //    TOP_ERR_SHAPE before anything runs;
-//  * the first call on a device resolves the arrays' device addresses with
-//    cudaGetSymbolAddress (with that device current); make that first call
-//    before any stream capture on that device;
+//  * the first call on a device (and the first call after that device's
+//    context was replaced, e.g. by cudaDeviceReset) resolves the arrays'
+//    device addresses with cudaGetSymbolAddress, with that device current;
+//    make that call before any stream capture on that device;
 //  * all calls share the arrays and each call clears the part it reads, so
 //    calls that run concurrently on the GPU (different streams or threads)
 //    race -- serialise them.
@@ -348,21 +350,47 @@ constexpr int kNoAllocMaxDevices = 64;
 static __device__ __align__(256) double g_noalloc_Q[576 * kNoAllocMaxChildren];
 static __device__ __align__(256) int32_t g_noalloc_eye[kNoAllocMaxChildren * kNoAllocMaxChildren];
 
-struct NoAllocScratch { double *Q = nullptr; int32_t *eye = nullptr; };
+// The resolved addresses are valid for one context of one device: a device
+// reset unloads the module and the next context may place the arrays
+// elsewhere, so the cache is keyed on (device, current context).  The context
+// handle comes from the driver's cuCtxGetCurrent, looked up through the
+// runtime (no link against libcuda).
+struct NoAllocScratch { double *Q = nullptr; int32_t *eye = nullptr; void *ctx = nullptr; };
 std::mutex g_noalloc_mu;
 NoAllocScratch g_noalloc_dev[kNoAllocMaxDevices];
 bool g_noalloc_ready[kNoAllocMaxDevices] = {};
+typedef int (*CtxGetCurrentFn)(void **);
+
+int current_context(void **ctx, const char *N)
+{
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        TOP_CUDA_CHECK(cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q), N);
+        if (q != cudaDriverEntryPointSuccess || !p) { set_error("%s:CUDA cuCtxGetCurrent not available", N); return TOP_ERR_CUDA; }
+        fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    }
+    *ctx = nullptr;
+    if (fn(ctx) != 0 || !*ctx) { set_error("%s:CUDA no current context", N); return TOP_ERR_CUDA; }
+    return TOP_OK;
+}
 
 int noalloc_scratch(NoAllocScratch *out, const char *N)
 {
     int dev = 0;
     TOP_CUDA_CHECK(cudaGetDevice(&dev), N);
     if (dev < 0 || dev >= kNoAllocMaxDevices) { set_error("%s:CUDA device %d out of range", N, dev); return TOP_ERR_CUDA; }
+    TOP_CUDA_CHECK(cudaSetDevice(dev), N);         // binds the device's primary context to this thread
+    void *ctx = nullptr;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ready[dev]) {
+    int rc = current_context(&ctx, N);
+    if (rc) return rc;
+    if (!g_noalloc_ready[dev] || g_noalloc_dev[dev].ctx != ctx) {
         NoAllocScratch s;
         TOP_CUDA_CHECK(cudaGetSymbolAddress((void **)&s.Q, g_noalloc_Q), N);
         TOP_CUDA_CHECK(cudaGetSymbolAddress((void **)&s.eye, g_noalloc_eye), N);
+        s.ctx = ctx;
         g_noalloc_dev[dev] = s;
         g_noalloc_ready[dev] = true;
     }
@@ -392,7 +420,9 @@ extern "C" int top_assemble_ks_level2_noalloc(void *Ks, const int32_t *upMap, co
         NoAllocScratch sc;
         int rc = noalloc_scratch(&sc, N);
         if (rc) return rc;
-        // rows of Q beyond nCh are read by the GEMM (times zero weights): clear all 64
+        // the GEMM loads all 64 rows of Q and multiplies rows nCh..63 by zero:
+        // clear them all, so that no value left by an earlier call (NaN or Inf
+        // included) reaches this call's result
         TOP_CUDA_CHECK(cudaMemsetAsync(sc.Q, 0, sizeof(double) * 576 * kNoAllocMaxChildren, st), N);
         rc = assemble_level2_f64((double *)Ks, upMap, (const double *)eleModulus, (const double *)K0,
                                  (const double *)Pch, mapUnique, (const double *)uniqueFree,
