@@ -336,6 +336,15 @@ int top_solver_get_l0_kernel(const top_solver *s, int fp32, int *out4);
  * on a solver-owned stream ordered after the caller's); on = 0 launches the
  * kernels one by one instead.  Default on.  No counterpart in the reference. */
 int top_solver_set_graphs(top_solver *s, int on);
+/* PCG direction update.  flexible = 0 (default): the reference's
+ * beta = rho / rhoOld (TOP_GPU.m:650-653).  flexible = 1: the flexible
+ * (Polak-Ribiere) beta = z.(r - r_old) / rhoOld, computed as
+ * -z.(A p_old) / (p_old . A p_old) with one extra dot product per iteration;
+ * it keeps consecutive directions A-orthogonal when the preconditioner is not
+ * exactly symmetric (an FP32 V-cycle on high-contrast designs).  Changes the
+ * iterates; compliance and the stopping test are unchanged.  No counterpart
+ * in the reference. */
+int top_solver_set_pcg_beta(top_solver *s, int flexible);
 /* The V-cycle below level 0 (coarse products, span-2 transfers, coarsest
  * solve) as one persistent cooperative launch with grid-wide barriers
  * (on = 1) or one launch per step (0, default: inside the captured PCG

@@ -83,7 +83,7 @@ def test_walsh_matvec_matches_oracle(model, shape, ctas):
     u = np.random.default_rng(ctas).standard_normal(o.level(0).numDOFs)
     ref = o.matvec(0, u)
     ud = torch.from_numpy(u).cuda()
-    for fp32, kind in ((False, 1), (True, 1), (True, 2), (False, 3), (True, 3), (True, 4), (True, 5)):
+    for fp32, kind in ((False, 1), (True, 1), (True, 2), (False, 3), (True, 3), (True, 4), (True, 5), (True, 6)):
         if kind == 5 and shape != (16, 8):    # the tensor-core kind: 16 x 8 element columns only
             continue
         s.set_l0_kernel(fp32, kind, shape[0], shape[1], ctas)
@@ -120,6 +120,8 @@ def test_walsh_rejects_bad_shape(model):
         s.set_l0_kernel(False, 5, 16, 8, 0)
     with pytest.raises(TopGpuError):
         s.set_l0_kernel(True, 5, 16, 16, 0)
+    with pytest.raises(TopGpuError):          # TMA-staged kind: FP32 only
+        s.set_l0_kernel(False, 6, 16, 8, 0)
     assert s.l0_kernel(False) == keep        # a rejected configuration changes nothing
 
 
@@ -131,7 +133,7 @@ def test_vcycle_and_pcg_with_walsh_match_oracle():
     assert _rel(s.vcycle(torch.from_numpy(r).cuda()), o.vcycle(r)) < 1e-11
 
 
-@pytest.mark.parametrize("kind", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("kind", [1, 2, 3, 4, 5, 6])
 def test_mixed_vcycle_kinds_agree(kind):
     """The FP32 V-cycle with either Walsh kernel stays within FP32 rounding
     of the FP64 V-cycle."""

@@ -97,6 +97,7 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
 struct PcgState {
     double normB, rho, rhoOld, pv, rr, resnorm, tol;
     double lam;                      // step length of the last update (x += lam p is applied by the p kernel)
+    double sigma;                    // z . A p_old (flexible beta: beta = -sigma / pv)
     int its, maxIT, done, status;
     int xPend, pad_;                 // the last iteration's x update is still to be applied
 };
@@ -139,6 +140,22 @@ __device__ __forceinline__ const int *done_of(const int *done, int k) { return d
 // rather than occupying registers through the whole kernel (the solver
 // checks that kMax vs fits).  Vectors shared by all right-hand sides (invD)
 // take no offset.
+// two adjacent node slots (i, i+1) of a component array, i even and the
+// array 16-byte aligned: one 8-byte (float) or 16-byte (double) access
+template <typename T> struct Vec2Of;
+template <> struct Vec2Of<float> { using type = float2; };
+template <> struct Vec2Of<double> { using type = double2; };
+template <typename T> __device__ __forceinline__ void ld2(const T *p, T &a, T &b)
+{
+    const typename Vec2Of<T>::type v = *reinterpret_cast<const typename Vec2Of<T>::type *>(p);
+    a = v.x; b = v.y;
+}
+template <typename T> __device__ __forceinline__ void st2(T *p, T a, T b)
+{
+    typename Vec2Of<T>::type v; v.x = a; v.y = b;
+    *reinterpret_cast<typename Vec2Of<T>::type *>(p) = v;
+}
+
 template <typename P> struct Comp3 {
     P p0, p1, p2;
     Comp3() = default;
@@ -177,6 +194,16 @@ struct StoreOut {   // y
     __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &, double &) const
     { for (int c = 0; c < 3; ++c) y[c][i + o] = TY(yv[c]); }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
+    // node pair (i, i+1), i even: vector stores; only node i when !both
+    struct Pre2 {};
+    __device__ __forceinline__ Pre2 pre2(int) const { return Pre2{}; }
+    __device__ __forceinline__ void apply2(int i, const T ya[3], const T yb[3], bool both, const Pre2 &, double &) const
+    {
+        for (int c = 0; c < 3; ++c) {
+            if (both) st2(y[c] + i + o, TY(ya[c]), TY(yb[c]));
+            else y[c][i + o] = TY(ya[c]);
+        }
+    }
 };
 template <typename T, typename TU, typename TY>
 struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
@@ -188,6 +215,18 @@ struct DotStoreOut { // y, and dot += u . y  (PCG: p . Ap)
     __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &p, double &dot) const
     { for (int c = 0; c < 3; ++c) { y[c][i + o] = TY(yv[c]); dot += double(p.u[c]) * double(yv[c]); } }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
+    struct Pre2 { TU a[3], b[3]; };
+    __device__ __forceinline__ Pre2 pre2(int i) const
+    { Pre2 p; for (int c = 0; c < 3; ++c) ld2(u[c] + i + o, p.a[c], p.b[c]); return p; }
+    __device__ __forceinline__ void apply2(int i, const T ya[3], const T yb[3], bool both, const Pre2 &p, double &dot) const
+    {
+        for (int c = 0; c < 3; ++c) {
+            if (both) st2(y[c] + i + o, TY(ya[c]), TY(yb[c]));
+            else y[c][i + o] = TY(ya[c]);
+            dot += double(p.a[c]) * double(ya[c]);
+            if (both) dot += double(p.b[c]) * double(yb[c]);
+        }
+    }
 };
 template <typename T, typename TR, typename TD>
 struct ResidOut {   // d = r - y
@@ -200,6 +239,17 @@ struct ResidOut {   // d = r - y
     __device__ __forceinline__ void apply(int i, const T yv[3], const Pre &p, double &) const
     { for (int c = 0; c < 3; ++c) d[c][i + oD] = TD(T(p.r[c]) - yv[c]); }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
+    struct Pre2 { TR a[3], b[3]; };
+    __device__ __forceinline__ Pre2 pre2(int i) const
+    { Pre2 p; for (int c = 0; c < 3; ++c) ld2(r[c] + i + oR, p.a[c], p.b[c]); return p; }
+    __device__ __forceinline__ void apply2(int i, const T ya[3], const T yb[3], bool both, const Pre2 &p, double &) const
+    {
+        for (int c = 0; c < 3; ++c) {
+            const TD da = TD(T(p.a[c]) - ya[c]), db = TD(T(p.b[c]) - yb[c]);
+            if (both) st2(d[c] + i + oD, da, db);
+            else d[c][i + oD] = da;
+        }
+    }
 };
 // z = x + omega*invD.*(r - y), optionally dot += z . r  (post-smoothing)
 template <typename T, typename TR, typename TZ>
@@ -224,6 +274,28 @@ struct PostSmoothOut {
         }
     }
     __device__ __forceinline__ void operator()(int i, const T yv[3], double &dot) const { apply(i, yv, pre(i), dot); }
+    struct Pre2 { T xa[3], xb[3], da[3], db[3]; TR ra[3], rb[3]; };
+    __device__ __forceinline__ Pre2 pre2(int i) const
+    {
+        Pre2 p;
+        for (int c = 0; c < 3; ++c) {
+            ld2(x[c] + i + o, p.xa[c], p.xb[c]);
+            ld2(invD[c] + i, p.da[c], p.db[c]);
+            ld2(r[c] + i + o, p.ra[c], p.rb[c]);
+        }
+        return p;
+    }
+    __device__ __forceinline__ void apply2(int i, const T ya[3], const T yb[3], bool both, const Pre2 &p, double &dot) const
+    {
+        for (int c = 0; c < 3; ++c) {
+            const T za = p.xa[c] + omega * p.da[c] * (T(p.ra[c]) - ya[c]);
+            const T zb = p.xb[c] + omega * p.db[c] * (T(p.rb[c]) - yb[c]);
+            if (both) st2(z[c] + i + o, TZ(za), TZ(zb));
+            else z[c][i + o] = TZ(za);
+            dot += double(za) * double(p.ra[c]);
+            if (both) dot += double(zb) * double(p.rb[c]);
+        }
+    }
 };
 
 // ---------------------------------------------------------------------------

@@ -3,10 +3,13 @@
 // Walsh-basis tile kernel (topgpu_walsh.cuh), per precision, with the
 // operand/epilogue combinations the solver uses instantiated here.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include "topgpu_solver_impl.cuh"
+#include "topgpu_stage.cuh"
 
 namespace topgpu {
 namespace {
@@ -37,7 +40,84 @@ bool walsh_shape_ok(int ty, int tx)
 }
 int tiles_of(const Geom &g, int kind, int ty, int tx)
 {
+    if (kind == 6) return stg::tiles(g, ty, tx);
     return (kind == 2 || kind == 4) ? walsh_pair_tiles(g, ty, tx) : walsh_tiles(g, ty, tx);
+}
+
+// ---- kind 6: tensor maps of the staged level-0 product -------------------
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda)
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+// node vector: (y, x', z', component, right-hand side) over a level-0 grid
+// vector (base = slot 0 of component 0 = node (0, -1, -1)); box = one staged
+// node layer of a tile
+bool encode_nodes(CUtensorMap *m, const float *base, const Geom &g, int64_t vs, int nv, int boxY, int boxX)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const int64_t PX = g.NX + 2, PZ = g.NZ + 2;
+    const cuuint64_t dims[5] = {(cuuint64_t)g.PY, (cuuint64_t)PX, (cuuint64_t)PZ, 3, (cuuint64_t)(nv > 0 ? nv : 1)};
+    const cuuint64_t strides[4] = {(cuuint64_t)g.PY * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.cs * 4,
+                                   (cuuint64_t)(vs > 0 ? vs : 3 * g.cs) * 4};
+    const cuuint32_t box[5] = {(cuuint32_t)boxY, (cuuint32_t)boxX, 1, 3, 1};
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, const_cast<float *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+// element moduli on the node grid (element at its base node's slot)
+bool encode_moduli(CUtensorMap *m, const float *base, const Geom &g, int boxY, int boxX)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const int64_t PX = g.NX + 2, PZ = g.NZ + 2;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.PY, (cuuint64_t)PX, (cuuint64_t)PZ};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.PY * 4, (cuuint64_t)g.plane * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)boxY, (cuuint32_t)boxX, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+// the staged kernel needs 16-byte aligned vectors and multiple-of-four
+// pitches (TMA strides and the paired epilogue accesses)
+bool stage_geom_ok(const Geom &g) { return ((g.PY | g.plane | g.origin | g.cs) & 3) == 0; }
+
+template <int A, int B, class Out>
+void launch_stage(top_solver *s, const top_solver::L0Kernel &k, const VecIn<float, float> &in, const Out &out,
+                  Reduce red, const int *done, int nv)
+{
+    using Tl = stg::Tile<A, B>;
+    DevLevel &lv = s->L[0];
+    static const int occ = [] {
+        int n = 0;
+        if (cudaFuncSetAttribute(l0s_kernel<A, B, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tl::SMEM) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, l0s_kernel<A, B, Out>, Tl::NTHREADS, Tl::SMEM) != cudaSuccess)
+            n = 1;
+        return n > 0 ? n : 1;
+    }();
+    const int64_t work = (int64_t)stg::tiles(lv.g, A, B) * lv.g.NZ;
+    int64_t n = k.ctas > 0 ? k.ctas : (int64_t)s->numSMs * occ;
+    n = std::max<int64_t>(std::min<int64_t>(std::min<int64_t>(n, work), s->nPartials), 1);
+    CUtensorMap mu, me;
+    const float *ub = in.u.p0;
+    const int64_t vs = in.vs;
+    const bool ok = encode_nodes(&mu, ub, lv.g, vs, vs > 0 ? nv : 1, Tl::BY, Tl::BXU) &&
+                    encode_moduli(&me, s->Eg32, lv.g, Tl::BY, B);
+    if (!ok) { s->stageErr = true; return; }
+    launch_k(s, l0s_kernel<A, B, Out>, dim3((unsigned)n, (unsigned)nv), Tl::NTHREADS, (size_t)Tl::SMEM, s->st,
+             mu, me, s->WP32, in, out, lv.flags, k.mask, lv.g, float(s->p.E0), red, done, s->tcErr);
 }
 
 // grid of the Walsh kernel: the configured CTA count (0: the CTAs that fit
@@ -97,6 +177,15 @@ void l0_op(top_solver *s, const In &in, const Out &out, Reduce red, const int *d
             (void)attr;
             launch_k(s, l0t_kernel<16, 8, In, Out>, dim3(l0w_ctas<T, 16, 8, In, Out, 5>(s, k), K), 128, tc::kSmemBytes, s->st, 
                 s->tcB, in, out, egrid<T>(s), lv.flags, k.mask, lv.g, T(s->p.E0), red, done, s->tcErr);
+        }
+    } else if (k.kind == 6) {        // FP32 only: TMA-staged layers, plain FP32 operand vectors
+        if constexpr (sizeof(T) == 4 && std::is_same<In, VecIn<float, float>>::value) {
+#define TOPGPU_LAUNCH_SHAPE(A, B) if (k.ty == A && k.tx == B) launch_stage<A, B, Out>(s, k, in, out, red, done, nv);
+            TOPGPU_WALSH_SHAPES(TOPGPU_LAUNCH_SHAPE)
+#undef TOPGPU_LAUNCH_SHAPE
+        } else if constexpr (sizeof(T) == 4) {   // another operand type: the direct-load kind, same tile shape
+            launch_k(s, l0d_kernel<T, 16, 8, In, Out>, dim3(l0w_ctas<T, 16, 8, In, Out, 3>(s, s->l0kFallback), K), 128, 0, s->st,
+                walshparam<T>(s), in, out, egrid<T>(s), lv.flags, s->l0kFallback.mask, lv.g, T(s->p.E0), red, done);
         }
     } else if (k.kind == 4) {        // FP32 only, as kind 2
         if constexpr (sizeof(T) == 4) {
@@ -182,9 +271,9 @@ __global__ void tc_probe_diff_kernel(const float *a, const float *b, int64_t n, 
     }
     atomicAdd(out, dd); atomicAdd(out + 1, nn);
 }
-// the tensor-core kind against the dense kernel on one pseudo-random vector,
-// with the model's current moduli: relative 2-norm difference below 1e-5 and
-// no MMA wait gave up
+// the tensor-core or staged kind against the dense kernel on one
+// pseudo-random vector, with the model's current moduli: relative 2-norm
+// difference below 1e-5 and no mbarrier wait gave up
 int tc_selftest(top_solver *s, const top_solver::L0Kernel &cand)
 {
     DevLevel &l0 = s->L[0];
@@ -211,12 +300,12 @@ int tc_selftest(top_solver *s, const top_solver::L0Kernel &cand)
         return TOP_ERR_CUDA;
     cudaMemsetAsync(l0.x32 - M, 0, sizeof(float) * n, s->st);
     if (!err && !(h[1] > 0)) {
-        set_error("level-0 kernel kind 5 is checked on the model: set the element densities first");
+        set_error("level-0 kernel kind %d is checked on the model: set the element densities first", cand.kind);
         return TOP_ERR_STATE;
     }
     if (err || !(std::sqrt(h[0] / h[1]) < 1e-5)) {
-        set_error("level-0 tensor-core kernel failed its self-test (relative difference %.3e, wait error %d)",
-                  h[1] > 0 ? std::sqrt(h[0] / h[1]) : -1.0, err);
+        set_error("level-0 kernel kind %d failed its self-test (relative difference %.3e, wait error %d)",
+                  cand.kind, h[1] > 0 ? std::sqrt(h[0] / h[1]) : -1.0, err);
         return TOP_ERR_CUDA;
     }
     return TOP_OK;
@@ -227,13 +316,24 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 {
     top_solver::L0Kernel &k = s->l0k[p];
     if (kind == 0) { k.kind = 0; ++s->opGen; return TOP_OK; }
+    DevLevel &l0 = s->L[0];
     if (kind == 5) {                                   // tensor cores: FP32, 16 x 8, any Ke
         if (p != 1 || ty != 16 || tx != 8 || ctas < 0 || s->super) return TOP_ERR_ARGS;
         const int rc = tc_operand(s);
         if (rc != TOP_OK) return rc;
+    } else if (kind == 6) {                            // TMA-staged: FP32, Walsh-symmetric Ke
+        if (p != 1 || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0 || s->super || !stage_geom_ok(l0.g) || !encode_fn())
+            return TOP_ERR_ARGS;
+        if (!s->tcErr && !(s->tcErr = s->dalloc<int>(1))) return TOP_ERR_NOMEM;
+        if (!s->l0kFallback.mask) {                    // direct-load kind for other operand types
+            const int t3 = walsh_tiles(l0.g, 16, 8);
+            if (cudaMalloc(&s->l0kFallback.mask, (size_t)t3) != cudaSuccess) { s->l0kFallback.mask = nullptr; return TOP_ERR_NOMEM; }
+            walsh_mask_kernel<16, 8><<<t3, 256, 0, s->st>>>(l0.flags, l0.g, s->l0kFallback.mask);
+            TOPGPU_COUNT_LAUNCH();
+            s->l0kFallback.kind = 3; s->l0kFallback.ty = 16; s->l0kFallback.tx = 8; s->l0kFallback.ctas = 0;
+        }
     } else if ((kind != 1 && kind != 3 && !((kind == 2 || kind == 4) && p == 1)) || !s->walshOK || !walsh_shape_ok(ty, tx) || ctas < 0)
         return TOP_ERR_ARGS;
-    DevLevel &l0 = s->L[0];
     const int tiles = tiles_of(l0.g, kind, ty, tx);
     if (ctas > s->nPartials) {                         // one reduction partial per CTA and right-hand side
         double *pp = s->dalloc<double>((size_t)ctas * s->kMax);
@@ -245,17 +345,20 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 #define TOPGPU_MASK_SHAPE(A, B)                                                                    \
     if (ty == A && tx == B) {                                                                      \
         if (kind == 2 || kind == 4) walsh_pair_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask); \
+        else if (kind == 6) stage_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask); \
         else walsh_mask_kernel<A, B><<<tiles, 256, 0, s->st>>>(l0.flags, l0.g, k.mask);            \
     }
     TOPGPU_WALSH_SHAPES(TOPGPU_MASK_SHAPE)
 #undef TOPGPU_MASK_SHAPE
     TOPGPU_COUNT_LAUNCH();
     if (cudaGetLastError() != cudaSuccess) return TOP_ERR_CUDA;
-    if (kind == 5) {
+    if (kind == 5 || kind == 6) {
         top_solver::L0Kernel cand = k;
         cand.kind = kind; cand.ty = ty; cand.tx = tx; cand.ctas = ctas;
+        s->stageErr = false;
         const int rc = tc_selftest(s, cand);
         if (rc != TOP_OK) return rc;
+        if (s->stageErr) { set_error("level-0 kernel kind 6: tensor map encoding failed"); return TOP_ERR_CUDA; }
     }
     k.kind = kind; k.ty = ty; k.tx = tx; k.ctas = ctas;
     ++s->opGen;
@@ -295,7 +398,8 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
     cudaEvent_t a, b;
     cudaEventCreate(&a); cudaEventCreate(&b);
     static const int shapes[][2] = {{16, 16}, {16, 8}};
-    static const int mults[] = {4, 6, 8, 12, 16};
+    static const std::vector<int> mults = {4, 6, 8, 12, 16};
+    static const std::vector<int> stageMults = {1, 2, 3, 4};     // kind 6 CTAs are large (a producer warp + a stage ring)
     int rc = TOP_OK;
     for (int p = 0; p < 2 && rc == TOP_OK; ++p) {
         int best[4] = {0, 16, 16, 0};
@@ -303,10 +407,10 @@ int autotune_l0(top_solver *s, int nrep, int64_t flushBytes, double *msBest, int
         double tBest = rc == TOP_OK ? time_l0(s, p, nrep, flush, (size_t)flushBytes, a, b) : -1.0;
         if (tBest < 0) { rc = TOP_ERR_CUDA; break; }
         if (s->walshOK) {
-            for (int kind = 1; kind <= 5 && rc == TOP_OK; ++kind) {
-                if ((kind == 2 || kind == 4 || kind == 5) && p == 0) continue;
+            for (int kind = 1; kind <= 6 && rc == TOP_OK; ++kind) {
+                if ((kind == 2 || kind == 4 || kind == 5 || kind == 6) && p == 0) continue;
                 for (const auto &sh : shapes)
-                    for (int m : mults) {
+                    for (int m : (kind == 6 ? stageMults : mults)) {
                         const int ctas = m * s->numSMs;
                         if (set_l0_kernel(s, p, kind, sh[0], sh[1], ctas) != TOP_OK) continue;
                         const double t = time_l0(s, p, nrep, flush, (size_t)flushBytes, a, b);
@@ -337,4 +441,5 @@ template void l0_op<float, VIfd, DotStoreOut<float, double, double>>(top_solver 
 template void l0_op<float, VIfd, StoreOut<float, double>>(top_solver *, const VIfd &, const StoreOut<float, double> &, Reduce, const int *, int);
 template void l0_op<float, VIfd, ResidOut<float, double, double>>(top_solver *, const VIfd &, const ResidOut<float, double, double> &, Reduce, const int *, int);
 template void l0_op<float, VIff, StoreOut<float, float>>(top_solver *, const VIff &, const StoreOut<float, float> &, Reduce, const int *, int);
+template void l0_op<float, VIff, StoreOut<float, double>>(top_solver *, const VIff &, const StoreOut<float, double> &, Reduce, const int *, int);
 }  // namespace topgpu

@@ -277,10 +277,12 @@ __global__ void pcg_check_kernel(PcgState *st, int nv)
     st->rhoOld = st->rho;
 }
 // p = z + beta p (first: p = z), and the pending x += lambda p of the last
-// update with the old p (also for a right-hand side that has just stopped)
+// update with the old p (also for a right-hand side that has just stopped).
+// beta = rho / rhoOld (the reference's), or with flex the flexible
+// (Polak-Ribiere) beta = -sigma / pv, sigma = z . A p_old, pv = p_old . A p_old
 template <typename TZ>
 __global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, int64_t n, const PcgState *st, int first,
-                             double *__restrict__ x)
+                             double *__restrict__ x, int flex)
 {
     pdl_enter();
     const int vk = blockIdx.y;
@@ -289,13 +291,29 @@ __global__ void pcg_p_kernel(double *__restrict__ p, const TZ *__restrict__ z, i
     const bool upd = first || !st->done;
     if (!xp && !upd) return;
     p += vk * n; z += vk * n; x += vk * n;
-    const double beta = first ? 0.0 : st->rho / st->rhoOld;
+    const double beta = first ? 0.0 : (flex ? -st->sigma / st->pv : st->rho / st->rhoOld);
     const double lam = st->lam;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double po = p[i];
         if (xp) x[i] += lam * po;
         if (upd) p[i] = double(z[i]) + beta * po;
     }
+}
+// sigma = z . v of every right-hand side that is still iterating (flexible beta)
+template <typename TZ>
+__global__ void zv_dot_kernel(const TZ *__restrict__ z, const double *__restrict__ v, int64_t n, Reduce red0,
+                              const int *__restrict__ done0)
+{
+    pdl_enter();
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    z += vk * n; v += vk * n;
+    const Reduce red = red0.at(vk);
+    double s = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += double(z[i]) * v[i];
+    block_sum_to<256>(s, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
 __global__ void dot_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t n, Reduce red0)
 {
@@ -869,6 +887,7 @@ extern "C" int top_solver_destroy(top_solver *s)
     if (s->capIn) cudaEventDestroy(s->capIn);
     if (s->capOut) cudaEventDestroy(s->capOut);
     for (auto &k : s->l0k) if (k.mask) cudaFree(k.mask);
+    if (s->l0kFallback.mask) cudaFree(s->l0kFallback.mask);
     for (void *p : s->allocs) cudaFree(p);
     if (s->hstate) cudaFreeHost(s->hstate);
     delete s;
@@ -893,6 +912,14 @@ extern "C" int top_solver_set_coarse_persistent(top_solver *s, int on)
 {
     if (!s) return TOP_ERR_ARGS;
     s->coarsePersistent = on != 0;
+    ++s->opGen;                      // captured PCG graphs change
+    return TOP_OK;
+}
+
+extern "C" int top_solver_set_pcg_beta(top_solver *s, int flexible)
+{
+    if (!s) return TOP_ERR_ARGS;
+    s->flexible = flexible != 0;
     ++s->opGen;                      // captured PCG graphs change
     return TOP_OK;
 }
@@ -1071,8 +1098,11 @@ extern "C" int top_solver_matvec(top_solver *s, int level, const double *u, doub
     CK(cudaMemsetAsync(d.x64 - kMargin, 0, sizeof(double) * 3 * d.g.cs, s->st));
     compact_to_grid_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(u, d.x64, d.nodeGrid, d.Nn, d.g.cs);
     TOPGPU_COUNT_LAUNCH();
-    if (fp32) {
-        level_op<float>(s, level, VecIn<float, double>{d.x64, d.g.cs}, StoreOut<float, double>{d.t64, d.g.cs}, none, nullptr);
+    if (fp32) {                      // the operand rounded to FP32 once (as the V-cycle holds it)
+        CK(cudaMemsetAsync(d.x32 - kMargin, 0, sizeof(float) * 3 * d.g.cs, s->st));
+        compact_to_grid_kernel<double, float><<<nb256(d.Nn), 256, 0, s->st>>>(u, d.x32, d.nodeGrid, d.Nn, d.g.cs);
+        TOPGPU_COUNT_LAUNCH();
+        level_op<float>(s, level, VecIn<float, float>{d.x32, d.g.cs}, StoreOut<float, double>{d.t64, d.g.cs}, none, nullptr);
     } else {
         level_op<double>(s, level, VecIn<double, double>{d.x64, d.g.cs}, StoreOut<double, double>{d.t64, d.g.cs}, none, nullptr);
     }
@@ -1250,13 +1280,22 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
                       Reduce{nullptr, nullptr, nullptr}, done, nrhs);
     // z = M r ; rho = z . r ; p = z
     // z = M r, z.r; p = z + beta p (z1Ready: the update kernel stored the V-cycle's Jacobi iterate)
+    const int flex = s->flexible ? 1 : 0;
     auto precond_p = [&](cudaStream_t q, int first) {
         if (z32) {
             vcycle<float, double, float>(s, s->r, s->z32, &s->state->rho, done, nrhs, nv, !first);
-            launch_k(s, pcg_p_kernel<float>, dim3(VB, K), 256, 0, q, s->pv - M, s->z32 - M, nv, s->state, first, xg - M);
+            if (flex && !first) {
+                launch_k(s, zv_dot_kernel<float>, dim3(VB, K), 256, 0, q, s->z32 - M, s->v - M, nv, red(&s->state->sigma), done);
+                TOPGPU_COUNT_LAUNCH();
+            }
+            launch_k(s, pcg_p_kernel<float>, dim3(VB, K), 256, 0, q, s->pv - M, s->z32 - M, nv, s->state, first, xg - M, flex);
         } else {
             vcycle<double, double, double>(s, s->r, s->z, &s->state->rho, done, nrhs, nv, !first);
-            launch_k(s, pcg_p_kernel<double>, dim3(VB, K), 256, 0, q, s->pv - M, s->z - M, nv, s->state, first, xg - M);
+            if (flex && !first) {
+                launch_k(s, zv_dot_kernel<double>, dim3(VB, K), 256, 0, q, s->z - M, s->v - M, nv, red(&s->state->sigma), done);
+                TOPGPU_COUNT_LAUNCH();
+            }
+            launch_k(s, pcg_p_kernel<double>, dim3(VB, K), 256, 0, q, s->pv - M, s->z - M, nv, s->state, first, xg - M, flex);
         }
         TOPGPU_COUNT_LAUNCH();
     };

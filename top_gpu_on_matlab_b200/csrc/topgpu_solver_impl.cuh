@@ -51,6 +51,9 @@ struct top_solver {
     // (identical results; TOPGPU_NO_VEC4 selects the per-slot kernels)
     bool vec4 = std::getenv("TOPGPU_NO_VEC4") == nullptr;   // programmatic dependent launch on the PCG path
     bool inCapture = false;          // launches are being captured into a graph (no dependent launch there)
+    // PCG direction update: false = the reference's beta = rho / rhoOld (TOP_GPU.m:650-653);
+    // true = flexible (Polak-Ribiere) beta = z.(r - r_old) / rhoOld = -z.(A p_old) / (p_old.A p_old)
+    bool flexible = false;
     int opGen = 0;                   // bumped whenever captured launches would change
     int nL = 0, nLoads = 0;
     std::vector<DevLevel> L;
@@ -59,12 +62,15 @@ struct top_solver {
     // level-0 product: kind 0 = node-centric dense Ke, 1 = Walsh-basis tiles
     // of ty x tx element columns (one per thread), 2 = the same with two
     // element columns per thread (ty x tx threads), 3 = Walsh with direct
-    // loads, 4 = paired direct loads, 5 = tensor cores (FP32, 16 x 8), on
+    // loads, 4 = paired direct loads, 5 = tensor cores (FP32, 16 x 8), 6 =
+    // paired with TMA-staged node layers (FP32; tiles of 2 ty x tx), on
     // ctas CTAs (0: as many as fit at once); per precision, set by
     // top_solver_set_l0_kernel or the autotuner
     struct L0Kernel { int kind = 0, ty = 16, tx = 16, ctas = 0; uint8_t *mask = nullptr; };
     int numSMs = 148;
     L0Kernel l0k[2];                 // [0] FP64, [1] FP32
+    L0Kernel l0kFallback;            // kind 6 with a converting operand: the direct-load kind, 16 x 8
+    bool stageErr = false;           // kind 6: a tensor map could not be encoded
     bool walshOK = false;            // Ke has the cube's reflection symmetry
     topgpu::TcOperandB *tcB = nullptr;   // kind 5: Ke as TF32 hi/lo tensor-core operand (device)
     int *tcErr = nullptr;            // kind 5: set by a kernel whose MMA wait gave up

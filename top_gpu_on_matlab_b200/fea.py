@@ -358,6 +358,10 @@ class Solver:
         """V-cycle levels below 0 in one cooperative launch (default) or one launch per step."""
         check(lib().top_solver_set_coarse_persistent(self._h, int(bool(on))), "top_solver_set_coarse_persistent")
 
+    def set_pcg_beta(self, flexible):
+        """False: the reference's beta = rho/rhoOld; True: flexible (Polak-Ribiere) beta."""
+        check(lib().top_solver_set_pcg_beta(self._h, int(bool(flexible))), "top_solver_set_pcg_beta")
+
     def set_graphs(self, on):
         """Run PCG iterations as captured CUDA graphs (default) or launch by launch."""
         check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
