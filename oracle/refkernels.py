@@ -31,17 +31,20 @@ class RefError(RuntimeError):
 _LIBS = {}
 
 
-def available():
-    return all((_DIR / ("lib%s.so" % n)).exists() for n in NAMES)
+def available(libdir=None):
+    d = Path(libdir) if libdir is not None else _DIR
+    return all((d / ("lib%s.so" % n)).exists() for n in NAMES)
 
 
-def _lib(name):
-    if name not in _LIBS:
-        so = C.CDLL(str(_DIR / ("lib%s.so" % name)))
+def _lib(name, libdir=None):
+    d = Path(libdir) if libdir is not None else _DIR
+    key = (str(d), name)
+    if key not in _LIBS:
+        so = C.CDLL(str(d / ("lib%s.so" % name)))
         so.shim_call.restype = C.c_int
         so.shim_call.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_char_p, C.c_int]
-        _LIBS[name] = so
-    return _LIBS[name]
+        _LIBS[key] = so
+    return _LIBS[key]
 
 
 def _mx(t, dims=None):
@@ -65,8 +68,11 @@ def _mx(t, dims=None):
     return a
 
 
-def call(name, *args, nlhs=0):
-    """args: CUDA tensors (column-major) or (tensor, dims) pairs."""
+def call(name, *args, nlhs=0, libdir=None, sync=True):
+    """args: CUDA tensors (column-major) or (tensor, dims) pairs.  libdir: a
+    directory of other gateway libraries built against the same stand-in
+    (default: the reference's, oracle/_ref).  sync=False skips the device
+    synchronisation (for calls that fail their argument checks on the host)."""
     arrs = []
     for x in args:
         if isinstance(x, tuple):
@@ -76,9 +82,11 @@ def call(name, *args, nlhs=0):
     prhs = (C.POINTER(MxArray) * len(arrs))(*[C.pointer(a) for a in arrs])
     plhs = (C.POINTER(MxArray) * max(1, nlhs))()
     err = C.create_string_buffer(600)
-    torch.cuda.synchronize()
-    rc = _lib(name).shim_call(nlhs, C.cast(plhs, C.c_void_p), len(arrs), C.cast(prhs, C.c_void_p), err, 600)
-    torch.cuda.synchronize()
+    if sync:
+        torch.cuda.synchronize()
+    rc = _lib(name, libdir).shim_call(nlhs, C.cast(plhs, C.c_void_p), len(arrs), C.cast(prhs, C.c_void_p), err, 600)
+    if sync:
+        torch.cuda.synchronize()
     if rc:
         ident, _, msg = err.value.decode().partition("|")
         raise RefError(ident, msg)

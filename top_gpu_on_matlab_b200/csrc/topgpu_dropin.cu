@@ -194,8 +194,7 @@ int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const
     // Q_s = P_s^T K0 P_s, one CTA per child slot
     if (nCh > 0) {
         eye_upmap_kernel<<<(nCh * nCh + 255) / 256, 256, 0, st>>>(eyeScratch, nCh);
-        ptkp_kernel<double><<<nCh, kPtkpThreads, 0, st>>>(Qscratch, eyeScratch, nCh, nCh, Pch,
-                                                          K0Child<double>{K0}, NoSkip{}, 0, nullptr);
+        ptkp_f64(st, Qscratch, eyeScratch, nCh, nCh, Pch, K0Child<double>{K0}, NoSkip{}, 0, nullptr, nCh);
     }
     if (nElem == 0) return TOP_OK;
     if (nCh <= kGemmK) {
@@ -209,13 +208,11 @@ int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const
         // children with fixed DOFs: full triple products, accumulated; only the
         // coarse cells in bndList when the caller knows them (-1: all cells)
         if (hasFixed && nBnd != 0)
-            ptkp_kernel<double><<<(unsigned)(nBnd > 0 ? nBnd : nElem), kPtkpThreads, 0, st>>>(
-                Ks, upMap, nElem, nCh, Pch,
-                Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed},
-                RegularChild{mapUnique, hasFixed, 1}, 1, nBnd > 0 ? bndList : nullptr);
+            ptkp_f64(st, Ks, upMap, nElem, nCh, Pch, Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed},
+                     RegularChild{mapUnique, hasFixed, 1}, 1, nBnd > 0 ? bndList : nullptr, nBnd > 0 ? nBnd : nElem);
     } else {
-        ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
-            Ks, upMap, nElem, nCh, Pch, Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed}, NoSkip{}, 0, nullptr);
+        ptkp_f64(st, Ks, upMap, nElem, nCh, Pch, Level2Child<double>{E, K0, mapUnique, uFree, uFixed, hasFixed}, NoSkip{}, 0,
+                 nullptr, nElem);
     }
     return cudaGetLastError() == cudaSuccess ? TOP_OK : TOP_ERR_CUDA;
 }
@@ -224,8 +221,7 @@ int assemble_higher_f64(double *Ks, const int32_t *upMap, const double *KsPrev, 
                         int64_t nElem, int nSub, cudaStream_t st)
 {
     if (nElem == 0) return TOP_OK;
-    ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(Ks, upMap, nElem, nSub, Psub,
-                                                                  PrevChild<double>{KsPrev}, NoSkip{}, 0, nullptr);
+    ptkp_f64(st, Ks, upMap, nElem, nSub, Psub, PrevChild<double>{KsPrev}, NoSkip{}, 0, nullptr, nElem);
     return cudaGetLastError() == cudaSuccess ? TOP_OK : TOP_ERR_CUDA;
 }
 }  // namespace topgpu
@@ -282,8 +278,8 @@ extern "C" int top_assemble_ks_higher(void *Ks, const int32_t *upMap, const void
     if (!Ks || !upMap || !KsPrev || !Psub) { set_error("%s:Input null pointer", N); return TOP_ERR_ARGS; }
     cudaStream_t st = S(stream);
     if (dtype == TOP_F64)
-        ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>((double *)Ks, upMap, nElem, nSub, (const double *)Psub,
-                                                                      PrevChild<double>{(const double *)KsPrev}, NoSkip{}, 0, nullptr);
+        ptkp_f64(st, (double *)Ks, upMap, nElem, nSub, (const double *)Psub, PrevChild<double>{(const double *)KsPrev},
+                 NoSkip{}, 0, nullptr, nElem);
     else
         ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>((float *)Ks, upMap, nElem, nSub, (const float *)Psub,
                                                                      PrevChild<float>{(const float *)KsPrev}, NoSkip{}, 0, nullptr);
@@ -306,10 +302,9 @@ extern "C" int top_assemble_ks_level2_super(void *Ks, const int32_t *upMap, cons
     const int hasFixed = (nUnique > 0 && mapUnique && uniqueFree && uniqueFixed) ? 1 : 0;
     cudaStream_t st = S(stream);
     if (dtype == TOP_F64)
-        ptkp_kernel<double><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
-            (double *)Ks, upMap, nElem, nSub, (const double *)Psub,
-            SuperChild<double>{(const double *)Ks0, mapUnique, (const double *)eleModulus,
-                               (const double *)uniqueFree, (const double *)uniqueFixed, hasFixed}, NoSkip{}, 0, nullptr);
+        ptkp_f64(st, (double *)Ks, upMap, nElem, nSub, (const double *)Psub,
+                 SuperChild<double>{(const double *)Ks0, mapUnique, (const double *)eleModulus,
+                                    (const double *)uniqueFree, (const double *)uniqueFixed, hasFixed}, NoSkip{}, 0, nullptr, nElem);
     else
         ptkp_kernel<float><<<(unsigned)nElem, kPtkpThreads, 0, st>>>(
             (float *)Ks, upMap, nElem, nSub, (const float *)Psub,

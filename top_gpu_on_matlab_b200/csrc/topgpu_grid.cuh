@@ -42,6 +42,19 @@ __host__ __device__ constexpr int sym_pack(int r, int k)
 {
     return r <= k ? r * 24 - r * (r - 1) / 2 + (k - r) : k * 24 - k * (k - 1) / 2 + (r - k);
 }
+// Packed coarse matrices on the grid, tile-interleaved: the element at grid
+// slot e keeps entry p at  (e / 32) * 9600 + p * 32 + e % 32, i.e. runs of 32
+// consecutive element slots store their 300 entries together (38 KB in FP32),
+// so a CTA working on a run of nodes reads a few contiguous blocks instead of
+// one 128-byte piece from each of 300 entry planes.  Slot -1 (the guard before
+// node (0,0,0)'s elements) falls in a zero tile in front of the array.
+constexpr int kKsTile = 32;
+constexpr int kKsTileVals = 300 * kKsTile;
+__host__ __device__ inline int ks_slot_base(int e) { return (e >> 5) * kKsTileVals + (e & 31); }
+__host__ __device__ inline int64_t ks_off(int p, int64_t e) { return (e >> 5) * kKsTileVals + p * kKsTile + (e & 31); }
+// values to allocate for a level's packed matrices, and the zero tile in front
+inline int64_t ks_alloc_vals(int64_t cs) { return (cs / kKsTile + 3) * (int64_t)kKsTileVals; }
+constexpr int64_t kKsFront = kKsTileVals;
 
 template <typename T> struct KeParam { T k[576]; };
 
@@ -408,8 +421,7 @@ coarse_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, c
     T y[3] = {T(0), T(0), T(0)};
     if (valid) {
         const int64_t slot = idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i);
-        const T *ke = Ks + slot;
-        if (ke[g.cs * sym_pack(3 * i, 3 * i)] != T(0)) {       // void element: all zero
+        if (Ks[ks_off(sym_pack(3 * i, 3 * i), slot)] != T(0)) {       // void element: all zero
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 const int m = (int)(slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j));
@@ -418,7 +430,7 @@ coarse_kernel(In in0, Out out0, const T *__restrict__ Ks, Geom g, Reduce red0, c
                 for (int c = 0; c < 3; ++c)
 #pragma unroll
                     for (int d = 0; d < 3; ++d)
-                        y[c] = fma(__ldg(ke + g.cs * sym_pack(3 * i + c, 3 * j + d)), u[d], y[c]);
+                        y[c] = fma(__ldg(Ks + ks_off(sym_pack(3 * i + c, 3 * j + d), slot)), u[d], y[c]);
             }
         }
     }
@@ -476,10 +488,10 @@ inline bool vec4_ok(const Geom &g, std::initializer_list<const void *> ptrs, std
         if (v & 3) return false;
     return true;
 }
-// packed-entry offsets (entry * CS) of Ks(r, k) of a level, in shared memory
-__device__ __forceinline__ void coarse_offsets(int *offs, const Geom &g, int tid, int nthreads)
+// packed-entry offsets (entry * 32, tile-interleaved layout) of Ks(r, k), in shared memory
+__device__ __forceinline__ void coarse_offsets(int *offs, const Geom &, int tid, int nthreads)
 {
-    for (int k = tid; k < 24 * 24; k += nthreads) offs[k] = sym_pack(k / 24, k % 24) * (int)g.cs;
+    for (int k = tid; k < 24 * 24; k += nthreads) offs[k] = sym_pack(k / 24, k % 24) * kKsTile;
 }
 // One tile: the 32 node slots q = bx*32 .. bx*32+31 of z layer bz; thread
 // (n, i) of the 256 takes incident element i of node n.  Every thread of the
@@ -497,7 +509,7 @@ __device__ __forceinline__ double coarse_tile_unit(const In &in, const Out &out,
     T y[3] = {T(0), T(0), T(0)};
     if (valid) {
         const int slot = idx - cdy(i) - PY * cdx(i) - PL * cdz(i);
-        const T *ke = Ks + slot;
+        const T *ke = Ks + ks_slot_base(slot);
         // rows 3i+c, columns 3j+d of the packed symmetric Ks (i is warp-uniform:
         // the offset loads are shared-memory broadcasts)
         if constexpr (sizeof(T) == 4) {

@@ -159,4 +159,170 @@ dgemm_k64_kernel(double *__restrict__ C, int64_t M, int N, int64_t ldc,
 
 constexpr size_t kGemmSmem = sizeof(double) * (kGemmBM * (kGemmK + kGemmPad) + kGemmK * (kGemmBN + kGemmPad));
 
+// ---------------------------------------------------------------------------
+// FP64 Galerkin triple products on the tensor cores: Kout = sum over children
+// of P_s^T (K_s P_s), one coarse element per warp, every 24 x 24 product as
+// 3 x 3 tiles of mma.sync.m8n8k4.f64 (six k-steps each: 108 MMAs per child).
+// The child's K_s is gathered into the warp's shared memory (leading dimension
+// 25, which spreads a fragment's rows over the banks); T = K_s P_s goes
+// through shared memory once; P_s fragments are read straight from global
+// memory (one small matrix per child slot, shared by every warp, L1 resident);
+// the output tiles accumulate in registers over the children.  Same
+// arguments and results as ptkp_kernel (rounding aside).
+constexpr int kDmmaWarps = 4;
+constexpr int kDmmaLd = 25;
+
+template <class ChildK, class Skip>
+__global__ void __launch_bounds__(32 * kDmmaWarps)
+ptkp_dmma_kernel(double *__restrict__ Ks, const int32_t *__restrict__ upMap, int64_t nElem, int nCh,
+                 const double *__restrict__ P, ChildK childK, Skip skip, int accumulate,
+                 const int32_t *__restrict__ elist, int64_t nSel)
+{
+    __shared__ double smem[kDmmaWarps][2][24 * kDmmaLd];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int64_t w = (int64_t)blockIdx.x * kDmmaWarps + warp;
+    if (w >= nSel) return;                           // whole warps; no CTA-wide barrier below
+    const int64_t e = elist ? (int64_t)elist[w] : w;
+    double *sK = smem[warp][0], *sT = smem[warp][1];
+    double acc[3][3][2];
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+        for (int J = 0; J < 3; ++J) acc[I][J][0] = acc[I][J][1] = 0.0;
+    bool any = false;
+    for (int s = 0; s < nCh; ++s) {
+        const int32_t f1 = upMap[e + (int64_t)s * nElem];
+        if (f1 <= 0 || skip(f1 - 1)) continue;     // uniform across the warp
+        any = true;
+        const double *Ps = P + (size_t)s * 576;
+        __syncwarp();                                // the previous child's reads of sK / sT are done
+        for (int i = lane; i < 576; i += 32) sK[(i % 24) + kDmmaLd * (i / 24)] = childK(f1 - 1, i);
+        __syncwarp();
+        // T = K_s P_s: tile (I, J) = sum_kk K[8I.., 4kk..] P[4kk.., 8J..]
+#pragma unroll
+        for (int I = 0; I < 3; ++I)
+#pragma unroll
+            for (int J = 0; J < 3; ++J) {
+                double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < 6; ++kk)
+                    dmma_8x8x4(d0, d1, sK[(8 * I + g) + kDmmaLd * (4 * kk + q)], __ldg(Ps + (4 * kk + q) + 24 * (8 * J + g)));
+                sT[(8 * I + g) + kDmmaLd * (8 * J + 2 * q)] = d0;
+                sT[(8 * I + g) + kDmmaLd * (8 * J + 2 * q + 1)] = d1;
+            }
+        __syncwarp();
+        // Kout += P_s^T T: A = P^T (8I.., 4kk..) = P(4kk.., 8I..), B = T(4kk.., 8J..)
+#pragma unroll
+        for (int I = 0; I < 3; ++I)
+#pragma unroll
+            for (int J = 0; J < 3; ++J)
+#pragma unroll
+                for (int kk = 0; kk < 6; ++kk)
+                    dmma_8x8x4(acc[I][J][0], acc[I][J][1], __ldg(Ps + (4 * kk + q) + 24 * (8 * I + g)),
+                               sT[(4 * kk + q) + kDmmaLd * (8 * J + g)]);
+    }
+    if (accumulate && !any) return;
+    double *out = Ks + (size_t)e * 576;
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+        for (int J = 0; J < 3; ++J)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int idx = (8 * I + g) + 24 * (8 * J + 2 * q + h);
+                out[idx] = accumulate ? out[idx] + acc[I][J][h] : acc[I][J][h];
+            }
+}
+// Many children per coarse element (the 64 of a span-4 cell): one CTA per
+// element, its kSplitWarps warps take children w, w + kSplitWarps, ... and the
+// warps' partial sums are added in warp order through shared memory
+// (deterministic), so a level with few coarse elements still fills the GPU.
+constexpr int kSplitWarps = 8;
+
+template <class ChildK, class Skip>
+__global__ void __launch_bounds__(32 * kSplitWarps)
+ptkp_dmma_split_kernel(double *__restrict__ Ks, const int32_t *__restrict__ upMap, int64_t nElem, int nCh,
+                       const double *__restrict__ P, ChildK childK, Skip skip, int accumulate,
+                       const int32_t *__restrict__ elist)
+{
+    extern __shared__ double dsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int64_t e = elist ? (int64_t)elist[blockIdx.x] : (int64_t)blockIdx.x;
+    double *sK = dsm + warp * 2 * 24 * kDmmaLd, *sT = sK + 24 * kDmmaLd;
+    double *part = dsm + kSplitWarps * 2 * 24 * kDmmaLd;          // [kSplitWarps][576]
+    __shared__ int anyW[kSplitWarps];
+    double acc[3][3][2];
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+        for (int J = 0; J < 3; ++J) acc[I][J][0] = acc[I][J][1] = 0.0;
+    bool any = false;
+    for (int s = warp; s < nCh; s += kSplitWarps) {
+        const int32_t f1 = upMap[e + (int64_t)s * nElem];
+        if (f1 <= 0 || skip(f1 - 1)) continue;     // uniform across the warp
+        any = true;
+        const double *Ps = P + (size_t)s * 576;
+        __syncwarp();
+        for (int i = lane; i < 576; i += 32) sK[(i % 24) + kDmmaLd * (i / 24)] = childK(f1 - 1, i);
+        __syncwarp();
+#pragma unroll
+        for (int I = 0; I < 3; ++I)
+#pragma unroll
+            for (int J = 0; J < 3; ++J) {
+                double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+                for (int kk = 0; kk < 6; ++kk)
+                    dmma_8x8x4(d0, d1, sK[(8 * I + g) + kDmmaLd * (4 * kk + q)], __ldg(Ps + (4 * kk + q) + 24 * (8 * J + g)));
+                sT[(8 * I + g) + kDmmaLd * (8 * J + 2 * q)] = d0;
+                sT[(8 * I + g) + kDmmaLd * (8 * J + 2 * q + 1)] = d1;
+            }
+        __syncwarp();
+#pragma unroll
+        for (int I = 0; I < 3; ++I)
+#pragma unroll
+            for (int J = 0; J < 3; ++J)
+#pragma unroll
+                for (int kk = 0; kk < 6; ++kk)
+                    dmma_8x8x4(acc[I][J][0], acc[I][J][1], __ldg(Ps + (4 * kk + q) + 24 * (8 * I + g)),
+                               sT[(4 * kk + q) + kDmmaLd * (8 * J + g)]);
+    }
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+        for (int J = 0; J < 3; ++J)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) part[warp * 576 + (8 * I + g) + 24 * (8 * J + 2 * q + h)] = acc[I][J][h];
+    if (lane == 0) anyW[warp] = any ? 1 : 0;
+    __syncthreads();
+    bool anyC = false;
+    for (int w = 0; w < kSplitWarps; ++w) anyC = anyC || anyW[w];
+    if (accumulate && !anyC) return;
+    double *out = Ks + (size_t)e * 576;
+    for (int i = threadIdx.x; i < 576; i += 32 * kSplitWarps) {
+        double v = part[i];
+        for (int w = 1; w < kSplitWarps; ++w) v += part[w * 576 + i];
+        out[i] = accumulate ? out[i] + v : v;
+    }
+}
+constexpr size_t kSplitSmem = sizeof(double) * (kSplitWarps * 2 * 24 * kDmmaLd + kSplitWarps * 576);
+
+// launch over nSel coarse elements (elist, or 0 .. nSel-1): children split
+// over the warps of a CTA when a cell has many, one warp per cell otherwise
+template <class ChildK, class Skip>
+inline void ptkp_f64(cudaStream_t st, double *Ks, const int32_t *upMap, int64_t nElem, int nCh, const double *P,
+                     ChildK childK, Skip skip, int accumulate, const int32_t *elist, int64_t nSel)
+{
+    if (nSel <= 0) return;
+    if (nCh >= 2 * kSplitWarps) {
+        static const bool attr = cudaFuncSetAttribute(ptkp_dmma_split_kernel<ChildK, Skip>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem) == cudaSuccess;
+        (void)attr;
+        ptkp_dmma_split_kernel<ChildK, Skip><<<(unsigned)nSel, 32 * kSplitWarps, kSplitSmem, st>>>(
+            Ks, upMap, nElem, nCh, P, childK, skip, accumulate, elist);
+        return;
+    }
+    ptkp_dmma_kernel<ChildK, Skip><<<(unsigned)((nSel + kDmmaWarps - 1) / kDmmaWarps), 32 * kDmmaWarps, 0, st>>>(
+        Ks, upMap, nElem, nCh, P, childK, skip, accumulate, elist, nSel);
+}
+
 }  // namespace topgpu

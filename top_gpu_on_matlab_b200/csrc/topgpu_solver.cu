@@ -132,8 +132,8 @@ __global__ void pack_ks_kernel(const double *__restrict__ KsC, const int32_t *__
         while (base + (24 - r) <= p) { base += 24 - r; ++r; }
         const int k = r + (p - base);
         const double v = sK[el * 576 + r + 24 * k];
-        P64[(int64_t)p * cs + sSlot[el]] = v;
-        P32[(int64_t)p * cs + sSlot[el]] = float(v);
+        P64[ks_off(p, sSlot[el])] = v;
+        P32[ks_off(p, sSlot[el])] = float(v);
     }
 }
 __global__ void diag_coarse_kernel(const double *__restrict__ P64, Geom g, const uint8_t *__restrict__ flags,
@@ -146,7 +146,7 @@ __global__ void diag_coarse_kernel(const double *__restrict__ P64, Geom g, const
     for (int c = 0; c < 3; ++c) {
         double d = 0;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) d += P64[g.cs * sym_pack(3 * i + c, 3 * i + c) + idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i)];
+        for (int i = 0; i < 8; ++i) d += P64[ks_off(sym_pack(3 * i + c, 3 * i + c), idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i))];
         const bool on = (flags[idx] & kActive) && d != 0.0;
         diag[c * g.cs + idx] = d;
         inv64[c * g.cs + idx] = on ? 1.0 / d : 0.0;
@@ -238,11 +238,21 @@ __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restri
     const Reduce red = red0.at(vk);
     const double lambda = st->rho / st->pv;
     double rr = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double rv = r[i] - lambda * v[i];
-        r[i] = rv;
-        z1[i] = omega * invD[i] * T(rv);
-        rr += rv * rv;
+    // two consecutive values per access (n and the vector bases are multiples
+    // of four values, 16-byte aligned)
+    const int64_t n2 = n >> 1;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += (int64_t)gridDim.x * blockDim.x) {
+        double ra, rb, va, vb;
+        T da, db;
+        ld2(r + 2 * j, ra, rb);
+        ld2(v + 2 * j, va, vb);
+        ld2(invD + 2 * j, da, db);
+        ra = ra - lambda * va;
+        rb = rb - lambda * vb;
+        st2(r + 2 * j, ra, rb);
+        st2(z1 + 2 * j, T(omega * da * T(ra)), T(omega * db * T(rb)));
+        rr += ra * ra;
+        rr += rb * rb;
     }
     block_sum_to<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
 }
@@ -638,7 +648,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         const int64_t cs = d.g.cs;
         // 32-bit in-array indices: the vectors of all right-hand sides (batched
         // launches index vector k at k * 3 CS) and the packed coarse matrices
-        if ((int64_t)s->kMax * 3 * cs >= (int64_t(1) << 31) - 1 || (l > 0 && 300 * cs >= (int64_t(1) << 31))) {
+        if ((int64_t)s->kMax * 3 * cs >= (int64_t(1) << 31) - 1 || ((l > 0 || mesh->superElement) && ks_alloc_vals(cs) >= (int64_t(1) << 31))) {
             set_error("top_solver_create: level %d grid too large for 32-bit in-array indices", l); top_solver_destroy(s); return TOP_ERR_SHAPE;
         }
         // host-side flags, node and element maps
@@ -682,8 +692,8 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
             if (!d.upMap || !d.KsC) return fail("out of device memory");
             cudaMemcpy(d.upMap, M.elementUpwardMap.data(), sizeof(int32_t) * M.Ne * nch, cudaMemcpyHostToDevice);
             if (l < s->nL - 1) {
-                d.KsP64 = s->galloc<double>(cs, 300);
-                d.KsP32 = s->galloc<float>(cs, 300);
+                d.KsP64 = s->ksalloc<double>(cs);
+                d.KsP32 = s->ksalloc<float>(cs);
                 if (!d.KsP64 || !d.KsP32) return fail("out of device memory");
             }
         }
@@ -747,8 +757,8 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         s->stage = s->dalloc<double>((size_t)64 * M0.Ne);
         s->Imat = s->dalloc<double>((size_t)576 * 64);
         l0.KsC = s->dalloc<double>((size_t)M0.Ne * 576);
-        l0.KsP64 = s->galloc<double>(l0.g.cs, 300);
-        l0.KsP32 = s->galloc<float>(l0.g.cs, 300);
+        l0.KsP64 = s->ksalloc<double>(l0.g.cs);
+        l0.KsP32 = s->ksalloc<float>(l0.g.cs);
         if (!s->Esub || !s->stage || !s->Imat || !l0.KsC || !l0.KsP64 || !l0.KsP32) return fail("out of device memory");
         cudaMemcpy(s->Imat, mesh->I_mat.data(), sizeof(double) * 576 * 64, cudaMemcpyHostToDevice);
     }
@@ -1257,6 +1267,8 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     const int64_t cs = l0.g.cs, nv = 3 * cs;    // whole grid vectors, margins included
     cudaStream_t st = s->st;
     const int VB = vec_blocks(nv);
+    // the residual update: one resident wave of 256-thread CTAs (8 per SM)
+    const int UB = (int)std::min<int64_t>(std::min<int64_t>(8 * (int64_t)s->numSMs, (nv / 2 + 255) / 256), s->nPartials);
     const int64_t M = kMargin;
     const unsigned K = (unsigned)nrhs;
     // mixed precision keeps the FP32 V-cycle's output z in FP32
@@ -1307,10 +1319,10 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     auto iteration = [&](cudaStream_t q) {
         outer_op(s, s->pv, s->v, &s->state->pv, done, nrhs, nv);                             // v = A p, p.v
         if (z32)
-            launch_k(s, pcg_update_kernel<float>, dim3(VB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
+            launch_k(s, pcg_update_kernel<float>, dim3(UB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                 l0.x32 - M, l0.invD32 - M, float(s->p.omega));
         else
-            launch_k(s, pcg_update_kernel<double>, dim3(VB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
+            launch_k(s, pcg_update_kernel<double>, dim3(UB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                  l0.x64 - M, l0.invD64 - M, double(s->p.omega));
         TOPGPU_COUNT_LAUNCH();
         launch_k(s, pcg_check_kernel, 1, 32, 0, q, s->state, nrhs);

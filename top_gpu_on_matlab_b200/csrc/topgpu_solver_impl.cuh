@@ -119,6 +119,12 @@ struct top_solver {
         T *b = dalloc<T>((size_t)cs * ncomp);
         return b ? b + topgpu::kMargin : nullptr;
     }
+    // packed coarse matrices in the tile-interleaved layout (topgpu_grid.cuh)
+    template <typename T> T *ksalloc(int64_t cs)
+    {
+        T *b = dalloc<T>((size_t)topgpu::ks_alloc_vals(cs));
+        return b ? b + topgpu::kKsFront : nullptr;
+    }
     Reduce red(double *result) const { return Reduce{partials, counter, result}; }
     // per-right-hand-side sums into consecutive PcgState's (batched launches)
     Reduce redk(double *result) const { return Reduce{partials, counter, result, nPartials, topgpu::kStateDoubles}; }
