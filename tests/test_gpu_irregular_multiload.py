@@ -1,11 +1,14 @@
 """The batching configuration at full size: a synthetic irregular domain in a
 192x384x192 grid (the union of three seeded ellipsoids, semi-axes 40-90
-voxels, and a cylinder of radius 30 along x; 4.8 M active voxels), all DOFs
-fixed on the active nodes of the x = 0 face, four load cases (unit loads in
--y, +z, -z, +y spread over seeded 200-node patches of the x = max face),
-solved as one batched PCG per iteration.  Mixed precision against the FP64
-path over two optimisation iterations (ft = 2, V0 = 0.3): compliance within
-1e-6, densities within 1e-4; plus the batched solves against per-load solves."""
+voxels, and a cylinder of radius 30 along x; 4.8 M active voxels, 34 % fill --
+the fullest domain among seeds 30-59 for those semi-axes, which do not reach
+40 % in this grid), all DOFs fixed on the active nodes of the x = 0 face, four
+load cases (unit loads in -y, +z, -z, +y spread over seeded 200-node patches
+of the x = max face), solved as one batched PCG per iteration.  Mixed
+precision against the FP64 path over the configuration's 30 optimisation
+iterations (ft = 2, V0 = 0.3): compliance within 1e-6 at every iteration,
+densities within 1e-4 at the end; plus the batched solves against per-load
+solves."""
 import numpy as np
 import pytest
 import torch
@@ -78,17 +81,26 @@ def test_batched_solves_equal_per_load_solves(model):
         assert torch.equal(Ub[k * nd:(k + 1) * nd], Uk)
 
 
-def test_mixed_tracks_fp64_over_two_iterations(model):
+def test_mixed_tracks_fp64_over_thirty_iterations(model):
     from top_gpu_on_matlab_b200.fea import Solver
     out = {}
     for name, mixed in (("fp64", False), ("mixed", True)):
         s = Solver(model, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6, mixed=mixed)
         s.autotune(nrep=2, flush_bytes=0)
         s.opt_begin(V0=0.3, rMin=np.sqrt(3), nLoop=30, ft=2)
-        recs = [s.opt_step() for _ in range(2)]
+        recs = []
+        for _ in range(30):
+            recs.append(s.opt_step())
+            loop, change, sharp = s.opt_state()
+            if change <= 1e-4 or sharp <= 0.01:       # the reference's stop rule
+                break
         xp, _ = s.design()
         out[name] = (recs, xp)
         del s
-    for a, b in zip(out["mixed"][0], out["fp64"][0]):
-        assert abs(a["c"] - b["c"]) <= 1e-6 * abs(b["c"])
-    assert float((out["mixed"][1] - out["fp64"][1]).abs().max()) <= 1e-4
+    assert len(out["mixed"][0]) == len(out["fp64"][0])
+    cerr = max(abs(a["c"] - b["c"]) / abs(b["c"]) for a, b in zip(out["mixed"][0], out["fp64"][0]))
+    xerr = float((out["mixed"][1] - out["fp64"][1]).abs().max())
+    print("cfg4 %d iterations: compliance rel err max %.2e, final density max-abs err %.2e, PCG its mixed %d / fp64 %d"
+          % (len(out["mixed"][0]), cerr, xerr, sum(r["pcgIts"] for r in out["mixed"][0]), sum(r["pcgIts"] for r in out["fp64"][0])))
+    assert cerr <= 1e-6
+    assert xerr <= 1e-4
