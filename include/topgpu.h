@@ -345,11 +345,11 @@ int top_solver_set_graphs(top_solver *s, int on);
  * iterates; compliance and the stopping test are unchanged.  No counterpart
  * in the reference. */
 int top_solver_set_pcg_beta(top_solver *s, int flexible);
-/* The V-cycle below level 0 (coarse products, span-2 transfers, coarsest
- * solve) as one persistent cooperative launch with grid-wide barriers
- * (on = 1) or one launch per step (0, default: inside the captured PCG
- * iteration graphs the separate launches run faster); identical results.
- * No counterpart in the reference. */
+/* The coarse part of the V-cycle (coarse products, span-2 transfers,
+ * coarsest solve) as one persistent cooperative launch with grid-wide
+ * barriers: on = 1 from level 1 down, on = 2 from level 2 down (level 1
+ * launched per step; one CTA per SM for the small grids), 0 one launch per
+ * step (the default); identical results.  No counterpart in the reference. */
 int top_solver_set_coarse_persistent(top_solver *s, int on);
 /* Autotuner: times each level-0 kernel configuration (kind, tile shape, CTA
  * count; nrep launches each, L2 flushed by writing flushBytes before every

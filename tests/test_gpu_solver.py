@@ -188,9 +188,11 @@ def test_persistent_coarse_vcycle_matches_per_level_launches(pair, mixed):
     r = torch.from_numpy(np.random.default_rng(8).standard_normal(o.level(0).numDOFs)).cuda()
     s2.set_coarse_persistent(True)
     za = s2.vcycle(r)
+    s2.set_coarse_persistent(2)                 # from level 2 down (level 1 launched per step)
+    zc = s2.vcycle(r)
     s2.set_coarse_persistent(False)
     zb = s2.vcycle(r)
-    assert torch.equal(za, zb)
+    assert torch.equal(za, zb) and torch.equal(zc, zb)
 
 
 @pytest.mark.parametrize("mixed", [False, True])

@@ -495,14 +495,16 @@ void level_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, co
     else coarse_op<T>(s, l, in, out, red, done);
 }
 
-// the persistent coarse kernel covers levels 1 .. nL-1 when every transfer
-// among them is span 2 (and the solver was not told to launch per level)
-bool coarse_persistent_ok(const top_solver *s)
+// first level of the V-cycle run by the persistent coarse kernel (0: none):
+// levels p .. nL-1 when the solver was told so (p = 1 or 2), there are at
+// least two of them and every transfer among them is span 2
+int coarse_persistent_level(const top_solver *s)
 {
-    if (!s->coarsePersistent || s->nL < 2 || s->nL - 1 > kCoarseMaxLevels) return false;
-    for (int l = 2; l < s->nL; ++l)
-        if (s->L[l].span != 2) return false;
-    return true;
+    const int p = s->coarsePersistent;
+    if (p < 1 || s->nL - p < 2 || s->nL - p > kCoarseMaxLevels) return 0;
+    for (int l = p + 1; l < s->nL; ++l)
+        if (s->L[l].span != 2) return 0;
+    return p;
 }
 
 // V-cycle 'Standard' (TOP_GPU.m:766-816) in precision T on the level-0
@@ -522,8 +524,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     const T omega = T(s->p.omega);
     const Reduce none{nullptr, nullptr, nullptr};
     const unsigned K = (unsigned)nv;
-    // levels below 0 as one persistent kernel where their transfers are span 2
-    const bool persist = coarse_persistent_ok(s);
+    // levels pl .. nL-1 as one persistent kernel where their transfers are span 2
+    const int pl = coarse_persistent_level(s);
+    const bool persist = pl > 0;
     if (!z1Ready) {
         DevLevel &l0 = s->L[0];
         const int64_t n0 = lvs(l0), M = kMargin;
@@ -532,7 +535,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     }
     // restriction leg
-    for (int l = 0; l < (persist ? 1 : nL - 1); ++l) {
+    for (int l = 0; l < (persist ? pl : nL - 1); ++l) {
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
         const int64_t vs = lvs(lv);
@@ -547,17 +550,18 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     const int64_t n = 3 * lc.Nn;
     if (persist) {
         CoarseVc<T> A{};
-        A.n = nL - 1;
-        for (int l = 1; l < nL; ++l) {
+        A.n = nL - pl;
+        for (int l = pl; l < nL; ++l) {
             DevLevel &d = s->L[l];
-            A.L[l - 1] = CoarseLv<T>{d.g, l < nL - 1 ? ks_packed<T>(d) : nullptr, vr<T>(d), vx<T>(d), vt<T>(d), invd<T>(d), d.flags};
+            A.L[l - pl] = CoarseLv<T>{d.g, l < nL - 1 ? ks_packed<T>(d) : nullptr, vr<T>(d), vx<T>(d), vt<T>(d), invd<T>(d), d.flags};
         }
         A.omega = omega; A.Ainv = s->Ainv; A.cr = s->cr; A.nC = n; A.nodeGridC = lc.nodeGrid; A.nv = nv;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeCooperative;
         attr[0].val.cooperative = 1;
         cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3((unsigned)coarse_vcycle_ctas<T>(s->numSMs));
+        // from level 2 down the grids are small: one CTA per SM keeps the grid-wide barriers cheap
+        cfg.gridDim = dim3((unsigned)(pl >= 2 ? s->numSMs : coarse_vcycle_ctas<T>(s->numSMs)));
         cfg.blockDim = dim3(kCoarseThreads);
         cfg.stream = s->st;
         cfg.attrs = attr; cfg.numAttrs = 1;
@@ -572,7 +576,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
-    for (int l = (persist ? 0 : nL - 2); l >= 0; --l) {
+    for (int l = (persist ? pl - 1 : nL - 2); l >= 0; --l) {
         DevLevel &lv = s->L[l], &lcn = s->L[l + 1];
         const T *xc = vt<T>(lcn);
         T *x = vx<T>(lv);
@@ -920,8 +924,8 @@ extern "C" int top_solver_autotune(top_solver *s, int nrep, int64_t flushBytes, 
 
 extern "C" int top_solver_set_coarse_persistent(top_solver *s, int on)
 {
-    if (!s) return TOP_ERR_ARGS;
-    s->coarsePersistent = on != 0;
+    if (!s || on < 0 || on > 2) return TOP_ERR_ARGS;
+    s->coarsePersistent = on;
     ++s->opGen;                      // captured PCG graphs change
     return TOP_OK;
 }

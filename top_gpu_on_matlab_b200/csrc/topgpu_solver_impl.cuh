@@ -45,7 +45,7 @@ struct top_solver {
     cudaStream_t capStream = nullptr; cudaEvent_t capIn = nullptr, capOut = nullptr;
     bool useGraphs = true;
     bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
-    bool coarsePersistent = false;   // levels below 0 of the V-cycle in one cooperative launch
+    int coarsePersistent = 0;        // levels from 1 (1) or from 2 (2) down of the V-cycle in one cooperative launch; 0 off
     bool pdl = std::getenv("TOPGPU_NO_PDL") == nullptr;
     // span-4 transfers read and write four fine y slots as one aligned vector
     // (identical results; TOPGPU_NO_VEC4 selects the per-slot kernels)

@@ -355,8 +355,9 @@ class Solver:
         return out
 
     def set_coarse_persistent(self, on):
-        """V-cycle levels below 0 in one cooperative launch (default) or one launch per step."""
-        check(lib().top_solver_set_coarse_persistent(self._h, int(bool(on))), "top_solver_set_coarse_persistent")
+        """V-cycle levels from 1 (on = 1 / True) or from 2 (on = 2) down in one cooperative
+        launch, or one launch per step (0 / False)."""
+        check(lib().top_solver_set_coarse_persistent(self._h, int(on)), "top_solver_set_coarse_persistent")
 
     def set_pcg_beta(self, flexible):
         """False: the reference's beta = rho/rhoOld; True: flexible (Polak-Ribiere) beta."""
