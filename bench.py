@@ -61,8 +61,12 @@ WORKLOAD = "cantilever_96x192x96_ft1_optimisation_iterations"
 # dram__bytes_write.sum), keyed by precision and the kernel configuration
 # (kind, tile y, tile x, CTAs); a configuration without a capture reports null
 NCU_TRAFFIC = {
-    ("fp64", 3, 16, 8, 1184): 74.3e6,
-    ("fp32", 3, 16, 8, 888): 37.5e6,
+    ("fp64", 3, 16, 8, 1184): 74.58e6,
+    ("fp64", 3, 16, 8, 1776): 74.51e6,
+    ("fp32", 3, 16, 16, 888): 32.61e6,
+    ("fp32", 3, 16, 8, 888): 37.71e6,
+    ("fp32", 3, 16, 8, 1776): 31.80e6,
+    ("fp32", 3, 16, 8, 2368): 31.69e6,
 }
 ITS_RECORD = ROOT / "bench_fp64_its.json"
 

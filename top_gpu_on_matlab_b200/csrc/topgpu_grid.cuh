@@ -65,6 +65,9 @@ template <int NT>
 __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result,
                                              unsigned nb, unsigned bid);
 template <int NT>
+__device__ __forceinline__ bool block_sum_last(double v, double *partials, unsigned *counter, double *result,
+                                               unsigned nb, unsigned bid);
+template <int NT>
 __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result)
 {
     block_sum_to<NT>(v, partials, counter, result, gridDim.x * gridDim.y * gridDim.z,
@@ -74,6 +77,15 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
 template <int NT>
 __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigned *counter, double *result,
                                              unsigned nb, unsigned bid)
+{
+    block_sum_last<NT>(v, partials, counter, result, nb, bid);
+}
+// the same; returns true in thread 0 of the CTA that wrote *result (after
+// the write), so that code depending on the whole sum can follow in the
+// same launch
+template <int NT>
+__device__ __forceinline__ bool block_sum_last(double v, double *partials, unsigned *counter, double *result,
+                                               unsigned nb, unsigned bid)
 {
     __shared__ double red[NT / 32];
     __shared__ bool last;
@@ -91,7 +103,7 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
         last = (atomicAdd(counter, 1u) == nb - 1);
     }
     __syncthreads();
-    if (!last) return;
+    if (!last) return false;
     __threadfence();
     double s = 0;
     for (unsigned i = tid; i < nb; i += NT) s += ((volatile double *)partials)[i];
@@ -103,7 +115,9 @@ __device__ __forceinline__ void block_sum_to(double v, double *partials, unsigne
         for (int i = 0; i < NT / 32; ++i) t += red[i];
         *result = t;
         *counter = 0;
+        return true;
     }
+    return false;
 }
 
 // PCG scalars of one right-hand side; batched solves keep one per vector

@@ -225,6 +225,20 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__
 // z1 = omega*invD.*r in the V-cycle's precision T (stored in the level-0 x
 // vector the V-cycle prolongs into).  x += lambda p is left to the p kernel,
 // which reads p anyway (pcg_check records lambda and that it is pending).
+// The CTA that completes rr = r . r then runs the iteration's check
+// (TOP_GPU.m:630-649) for its right-hand side, in the same launch.
+__device__ __forceinline__ void pcg_check_one(PcgState *st)
+{
+    st->lam = st->rho / st->pv;          // the update's lambda; x += lam p is pending
+    st->xPend = 1;
+    st->its += 1;
+    const double res = sqrt(st->rr) / st->normB;
+    st->resnorm = res;
+    if (!isfinite(res) || !isfinite(st->rho) || !isfinite(st->pv)) { st->status = TOP_ERR_NAN; st->done = 1; return; }
+    if (res < st->tol) { st->done = 1; return; }
+    if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
+    st->rhoOld = st->rho;
+}
 template <typename T>
 __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restrict__ v, int64_t n, PcgState *st, Reduce red0,
                                   T *__restrict__ z1, const T *__restrict__ invD, T omega)
@@ -232,7 +246,10 @@ __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restri
     pdl_enter();
     const int vk = blockIdx.y;           // right-hand side; vectors at stride n
     st += vk;
-    if (st->done) return;
+    if (st->done) {                      // stopped: nothing pending for the p kernel
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->xPend = 0;
+        return;
+    }
     r += vk * n; v += vk * n;
     z1 += vk * n;
     const Reduce red = red0.at(vk);
@@ -254,7 +271,10 @@ __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restri
         rr += ra * ra;
         rr += rb * rb;
     }
-    block_sum_to<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
+    if (block_sum_last<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x)) {
+        __threadfence();
+        pcg_check_one(st);
+    }
 }
 // z1 = omega*invD.*r on whole grid vectors (n = 3 CS values per right-hand
 // side; r at stride vsR, z1 at stride n; invD shared)
@@ -269,22 +289,6 @@ __global__ void jacobi_base_kernel(const TR *__restrict__ r, const T *__restrict
     r += vk * vsR; z1 += vk * n;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         z1[i] = omega * invD[i] * T(r[i]);
-}
-__global__ void pcg_check_kernel(PcgState *st, int nv)
-{
-    pdl_enter();   // TOP_GPU.m:630-649, one thread per right-hand side
-    if ((int)threadIdx.x >= nv) return;
-    st += threadIdx.x;
-    if (st->done) { st->xPend = 0; return; }
-    st->lam = st->rho / st->pv;          // the update kernel's lambda; x += lam p is pending
-    st->xPend = 1;
-    st->its += 1;
-    const double res = sqrt(st->rr) / st->normB;
-    st->resnorm = res;
-    if (!isfinite(res) || !isfinite(st->rho) || !isfinite(st->pv)) { st->status = TOP_ERR_NAN; st->done = 1; return; }
-    if (res < st->tol) { st->done = 1; return; }
-    if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
-    st->rhoOld = st->rho;
 }
 // p = z + beta p (first: p = z), and the pending x += lambda p of the last
 // update with the old p (also for a right-hand side that has just stopped).
@@ -1328,8 +1332,6 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
         else
             launch_k(s, pcg_update_kernel<double>, dim3(UB, K), 256, 0, q, s->r - M, s->v - M, nv, s->state, red(&s->state->rr),
                                                                  l0.x64 - M, l0.invD64 - M, double(s->p.omega));
-        TOPGPU_COUNT_LAUNCH();
-        launch_k(s, pcg_check_kernel, 1, 32, 0, q, s->state, nrhs);
         TOPGPU_COUNT_LAUNCH();
         precond_p(q, 0);
     };

@@ -641,8 +641,17 @@ __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, 
             walsh2(ht[c]);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                U[c][k] = Ee * (hb[c][k] + ht[c][k]);
-                U[c][k + 4] = Ee * (hb[c][k] - ht[c][k]);
+                if constexpr (sizeof(T) == 4) {
+                    // FP32: E (hb +- ht) as one multiply and two multiply-adds (12
+                    // fewer issued operations per element layer); FP64 keeps the
+                    // sum-then-scale rounding of the parity-tested outer product
+                    const T a = Ee * ht[c][k];
+                    U[c][k] = fma(Ee, hb[c][k], a);
+                    U[c][k + 4] = fma(Ee, hb[c][k], -a);
+                } else {
+                    U[c][k] = Ee * (hb[c][k] + ht[c][k]);
+                    U[c][k + 4] = Ee * (hb[c][k] - ht[c][k]);
+                }
                 hb[c][k] = ht[c][k];
             }
         }
