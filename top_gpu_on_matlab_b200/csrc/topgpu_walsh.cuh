@@ -703,6 +703,139 @@ __device__ __forceinline__ void l0d_march(const WalshParam<T> &B, const In &in, 
     }
 }
 
+// FP32 form of l0d_march with displacement components 0 and 1 carried as one
+// float2 through every step that treats the components alike (the (y, x)
+// and z butterflies, the modulus, the node sums): those run as the paired
+// sm_100 instructions (__fadd2_rn / __fmul2_rn / __ffma2_rn), one issue for
+// two values; component 2 and the block products, which mix the components,
+// stay scalar.  The same operations in the same order as l0d_march, so the
+// results are bit-identical; about a quarter fewer floating-point
+// instructions per element layer.
+__device__ __forceinline__ void walsh2p(float2 v[4])
+{
+    const float2 p0 = padd(v[0], v[1]), m0 = psub(v[0], v[1]), p1 = padd(v[2], v[3]), m1 = psub(v[2], v[3]);
+    v[0] = padd(p0, p1); v[1] = padd(m0, m1); v[2] = psub(p0, p1); v[3] = psub(m0, m1);
+}
+template <int TY, int TX, bool MASK, class In, class Out>
+__device__ __forceinline__ void l0d_march_c2(const WalshParam<float> &B, const In &in, const Out &out,
+                                             const float *__restrict__ E, const uint8_t *__restrict__ flags,
+                                             const Geom &g, int y0, int x0, int z0, int z1, float E0,
+                                             float *so, double &dot)
+{
+    constexpr int NT = TY * TX;
+    const int tid = threadIdx.x, ty = tid % TY, tx = tid / TY;
+    const int PY = g.PY, PL = (int)g.plane;
+    const int ey = y0 - 1 + ty, ex = x0 - 1 + tx;
+    const bool cOn = ey <= g.NY - 1 && ex <= g.NX - 1;
+    const int base = cOn ? (int)(g.origin + ey + (int64_t)PY * ex) : 0;
+    const bool nOut = ty >= 1 && tx >= 1 && ey < g.NY && ex < g.NX;
+    auto load = [&](int z, float2 v01[4], float v2[4]) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int m = base + (k & 1) + PY * (k >> 1) + PL * z;
+            uint8_t f = 0;
+            if (MASK && cOn) f = flags[m];
+            float u0 = cOn ? in(m, 0) : 0.f, u1 = cOn ? in(m, 1) : 0.f, u2 = cOn ? in(m, 2) : 0.f;
+            if (MASK) {
+                if (f & 1) u0 = 0.f;
+                if (f & 2) u1 = 0.f;
+                if (f & 4) u2 = 0.f;
+            }
+            v01[k] = make_float2(u0, u1);
+            v2[k] = u2;
+        }
+    };
+    auto eload = [&](int z) { return cOn ? E[base + PL * z] : 0.f; };
+
+    float2 hb01[4], gt01[4], pre01[4];
+    float hb2[4], gt2[4], pre2[4];
+    __syncthreads();                     // the previous range's reads of so are done
+    load(z0 - 1, hb01, hb2);
+    walsh2p(hb01);
+    walsh2(hb2);
+    load(z0, pre01, pre2);
+    float eNext = eload(z0 - 1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { gt01[k] = make_float2(0.f, 0.f); gt2[k] = 0.f; }
+
+    for (int ez = z0 - 1; ez < z1; ++ez) {
+        typename Out::Pre po{};
+        if (nOut && ez >= z0) po = out.pre(base + PL * ez);
+        float2 ht01[4];
+        float ht2[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { ht01[k] = pre01[k]; ht2[k] = pre2[k]; }
+        if (ez + 2 <= z1) load(ez + 2, pre01, pre2);
+        const float Ee = eNext;
+        if (ez + 1 < z1) eNext = eload(ez + 1);
+        const float2 EE = make_float2(Ee, Ee);
+        walsh2p(ht01);
+        walsh2(ht2);
+        // U[c][k] = E (hb + ht), U[c][k + 4] = E (hb - ht): components 0, 1 paired
+        float2 U01[8];
+        float U2[8];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float2 a = pmul(EE, ht01[k]);
+            U01[k] = pfma(EE, hb01[k], a);
+            U01[k + 4] = pfma(EE, hb01[k], make_float2(-a.x, -a.y));
+            hb01[k] = ht01[k];
+            const float a2 = Ee * ht2[k];
+            U2[k] = fmaf(Ee, hb2[k], a2);
+            U2[k + 4] = fmaf(Ee, hb2[k], -a2);
+            hb2[k] = ht2[k];
+        }
+        // block products (mix the components): scalar
+        auto Uv = [&](int d, int j) { return d == 0 ? U01[j].x : (d == 1 ? U01[j].y : U2[j]); };
+        float2 V01[8];
+        float V2[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float acc = 0.f;
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    if ((walsh_pattern(t) >> (3 * c + d)) & 1u) acc = fmaf(B.b[t][3 * c + d], Uv(d, t ^ walsh_axis_bit(d)), acc);
+                const int j = t ^ walsh_axis_bit(c);
+                if (c == 0) V01[j].x = acc;
+                else if (c == 1) V01[j].y = acc;
+                else V2[j] = acc;
+            }
+        float2 G01[4];
+        float G2[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            G01[k] = padd(gt01[k], padd(V01[k], V01[k + 4]));
+            gt01[k] = psub(V01[k], V01[k + 4]);
+            G2[k] = gt2[k] + (V2[k] + V2[k + 4]);
+            gt2[k] = V2[k] - V2[k + 4];
+        }
+        if (ez < z0) continue;
+        walsh2p(G01);
+        walsh2(G2);
+        float2 *b01 = reinterpret_cast<float2 *>(so + (ez & 1) * 9 * NT);     // [3][NT] pairs
+        float *b2 = so + (ez & 1) * 9 * NT + 6 * NT;                          // [3][NT]
+#pragma unroll
+        for (int k = 1; k < 4; ++k) { b01[(k - 1) * NT + tid] = G01[k]; b2[(k - 1) * NT + tid] = G2[k]; }
+        __syncthreads();
+        if (nOut) {
+            const float2 y01 = padd(padd(padd(G01[0], b01[0 * NT + tid - 1]), b01[1 * NT + tid - TY]), b01[2 * NT + tid - TY - 1]);
+            float y[3];
+            y[0] = y01.x;
+            y[1] = y01.y;
+            y[2] = G2[0] + b2[0 * NT + tid - 1] + b2[1 * NT + tid - TY] + b2[2 * NT + tid - TY - 1];
+            const int idx = base + PL * ez;
+            if (MASK) {
+                const uint8_t f = flags[idx];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) if (f & (1 << c)) y[c] = E0 * in(idx, c);
+            }
+            out.apply(idx, y, po, dot);
+        }
+    }
+}
+
 template <typename T, int TY, int TX, class In, class Out>
 __global__ void __launch_bounds__(TY * TX, (WalshOccD<T, TY * TX, Out>::value))
 l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, const uint8_t *__restrict__ flags,
@@ -713,7 +846,7 @@ l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, con
     const int *done = done_of(done0, vk);
     if (done && *done) return;
     const In in = in0.shift(vk); const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
-    __shared__ T so[2 * 9 * TY * TX];
+    __shared__ __align__(16) T so[2 * 9 * TY * TX];
     const int tilesY = (g.NY + TY - 2) / (TY - 1);
     const int64_t total = (int64_t)walsh_tiles(g, TY, TX) * g.NZ;
     int64_t a = total * blockIdx.x / gridDim.x;
@@ -723,10 +856,17 @@ l0d_kernel(const WalshParam<T> B, In in0, Out out0, const T *__restrict__ E, con
         const int tile = (int)(a / g.NZ), z0 = (int)(a % g.NZ);
         const int z1 = (int)(z0 + (b - a) < g.NZ ? z0 + (b - a) : g.NZ);
         const int y0 = (tile % tilesY) * (TY - 1), x0 = (tile / tilesY) * (TX - 1);
-        if (tileMask[tile])
-            l0d_march<T, TY, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
-        else
-            l0d_march<T, TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        if constexpr (sizeof(T) == 4) {
+            if (tileMask[tile])
+                l0d_march_c2<TY, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+            else
+                l0d_march_c2<TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        } else {
+            if (tileMask[tile])
+                l0d_march<T, TY, TX, true>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+            else
+                l0d_march<T, TY, TX, false>(B, in, out, E, flags, g, y0, x0, z0, z1, E0, so, dot);
+        }
         a += z1 - z0;
     }
     if (red.result) block_sum_to<TY * TX>(dot, red.partials, red.counter, red.result, gridDim.x, blockIdx.x);
