@@ -63,9 +63,9 @@ WORKLOAD = "cantilever_96x192x96_ft1_optimisation_iterations"
 NCU_TRAFFIC = {
     ("fp64", 3, 16, 8, 1184): 74.58e6,
     ("fp64", 3, 16, 8, 1776): 74.51e6,
-    ("fp32", 3, 16, 16, 888): 32.61e6,
-    ("fp32", 3, 16, 8, 888): 37.71e6,
-    ("fp32", 3, 16, 8, 1776): 31.80e6,
+    ("fp32", 3, 16, 16, 888): 32.90e6,
+    ("fp32", 3, 16, 8, 888): 38.11e6,
+    ("fp32", 3, 16, 8, 1776): 31.79e6,
     ("fp32", 3, 16, 8, 2368): 31.69e6,
 }
 ITS_RECORD = ROOT / "bench_fp64_its.json"
