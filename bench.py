@@ -468,8 +468,8 @@ def oracle_check(ow, s, xPhys):
 
 def run_kernels_only(args):
     """Build the workload's mixed solver, assemble, and time --steps launches
-    each of the level-0 stiffness products (FP64 outer, FP32 smoother) and of
-    one V-cycle, L2 not flushed.  Few launches: the command the ncu captures
+    each of the level-0 stiffness products (FP64 outer, FP32 smoother), of
+    one V-cycle and of the level-1 FP32 product, L2 not flushed.  Few launches: the command the ncu captures
     of those kernels run.  --l0 fp64=K,TY,TX,CTAS / fp32=... selects the
     level-0 kernel configurations (default: the solver's)."""
     import ctypes as C
@@ -486,7 +486,7 @@ def run_kernels_only(args):
         prec, vals = spec.split("=")
         s.set_l0_kernel(prec == "fp32", *[int(v) for v in vals.split(",")])
     out = {}
-    for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32")):
+    for which, key in ((0, "l0_f64"), (1, "l0_f32"), (2, "vcycle_f32"), (3, "l1_f32")):
         ms = C.c_double(0)
         check(lib().top_solver_time_kernel(s._h, which, args.steps, 0, C.byref(ms)), "time_kernel")
         out[key] = ms.value

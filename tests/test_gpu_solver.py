@@ -237,6 +237,31 @@ def test_vector_transfers_change_no_result(pair, mixed, monkeypatch):
     assert out[0][1] == out[1][1] and torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][2], out[1][2])
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_two_pass_coarse_product_changes_no_result(pair, mixed, monkeypatch):
+    """the two-pass coarse product (packed tiles staged in shared memory,
+    element outputs, then node sums) gives the one-pass tile kernel's results
+    bit for bit: coarse products in both precisions, V-cycle and PCG"""
+    o, s, m, _ = pair
+    from top_gpu_on_matlab_b200.fea import Solver
+    x = torch.from_numpy(0.2 + 0.7 * np.random.default_rng(5).random(o.level(0).numElements)).cuda()
+    rng = np.random.default_rng(8)
+    us = [torch.from_numpy(rng.standard_normal(3 * o.level(l).numNodes)).cuda() for l in range(o.numLevels)]
+    r = torch.from_numpy(np.random.default_rng(9).standard_normal(o.level(0).numDOFs)).cuda()
+    out = []
+    for minTiles in ("0", "1000000000"):          # every coarse level two-pass / none
+        monkeypatch.setenv("TOPGPU_COARSE_TWOPASS_MIN", minTiles)
+        s2 = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-8, maxIT=800, omega=0.6, mixed=mixed)
+        s2.set_density(x)
+        s2.assemble()
+        prods = [s2.matvec(l, us[l], fp32=f) for l in range(1, o.numLevels - 1) for f in (False, True)]
+        U, its, _ = s2.pcg(0)
+        out.append((prods, U, its, s2.vcycle(r)))
+    (pa, Ua, ia, za), (pb, Ub, ib, zb) = out
+    assert len(pa) == 2 * (o.numLevels - 2) and all(torch.equal(a, b) for a, b in zip(pa, pb))
+    assert ia == ib and torch.equal(Ua, Ub) and torch.equal(za, zb)
+
+
 def test_filter_graph_matches_launches(pair):
     """the PDE filter's PCG chunks as CUDA graphs give the launch-by-launch result bit for bit"""
     o, s, m, _ = pair

@@ -603,6 +603,208 @@ inline unsigned coarse_blocks(const Geom &g)
 }
 
 // ---------------------------------------------------------------------------
+// Two-pass coarse product (the larger coarse levels).  The one-pass tile
+// kernel issues 72 scattered scalar loads of packed matrix entries per thread
+// and waits on their latency.  Here:
+//
+//  pass 1 (coarse_elem_kernel): a persistent loop over the packed tiles (32
+//    consecutive element slots x 300 entries, contiguous in the
+//    tile-interleaved layout).  One thread copies each tile into shared
+//    memory with a single bulk copy (cp.async.bulk, completion on an
+//    mbarrier), two tiles in flight per CTA, and the CTA forms the outputs
+//    w_e = K_e u_e of its 32 elements there: thread (e, i) gathers u at
+//    corner i of element slot e, then computes rows 3i..3i+2 (corner i) with
+//    the multiply-add order of coarse_tile_unit.  w goes to W, laid out
+//    [tile][24][32] like the packed matrices;
+//  pass 2 (coarse_gather_kernel): one thread per node slot adds the rows of
+//    its corner in its eight incident elements, corners 0..7 in order (the
+//    tile kernel's order), and applies the epilogue.
+//
+// Both passes evaluate the same expressions in the same order as the tile
+// kernel, so the products agree bit for bit.  W slots that pass 1 never
+// writes (guards before the first and after the last element) stay zero from
+// the allocation; slots in its range without an element hold zero matrices.
+// Every mbarrier wait is bounded: when one gives up, the CTA stops, raises
+// the error flag and waits (bounded) for its copies still in flight.
+constexpr int kWTileVals = 24 * kKsTile;
+inline int64_t w_alloc_vals(int64_t cs) { return (cs / kKsTile + 3) * (int64_t)kWTileVals; }
+constexpr int64_t kWFront = kWTileVals;
+constexpr int kElemThreads = 256;                  // 32 element slots x 8 corners
+
+namespace bulk {
+constexpr uint32_t kWaitLimit = 1u << 22;
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void arrive_expect(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+}
+// bounded wait for the phase of the given parity; false when the limit ran out
+__device__ __forceinline__ bool wait(uint32_t bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < kWaitLimit; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+// bytes (a multiple of 16) from a 16-byte aligned global address into this
+// CTA's shared memory (16-byte aligned), completing on the mbarrier
+__device__ __forceinline__ void copy(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+}  // namespace bulk
+
+template <typename T> struct CoarseElem {
+    static constexpr uint32_t kTileBytes = (uint32_t)(sizeof(T) * kKsTileVals);   // one packed tile
+    static constexpr size_t kOffBar = sizeof(T) * (2 * (size_t)kKsTileVals + kWTileVals);
+    static constexpr size_t kSmem = kOffBar + 16;                                 // + two mbarriers
+    static_assert(kTileBytes % 16 == 0 && kOffBar % 8 == 0, "bulk copy sizes and mbarrier alignment");
+};
+// first and count of the packed tiles holding a level's element slots
+// (element (Y, X, Z) at its base node's slot, Y < NY - 1, X < NX - 1, Z < NZ - 1)
+inline void coarse_elem_tiles(const Geom &g, int &t0, int &nt)
+{
+    if (g.NY < 2 || g.NX < 2 || g.NZ < 2) { t0 = 0; nt = 0; return; }
+    const int64_t lo = g.origin, hi = g.origin + (g.NY - 2) + (int64_t)g.PY * (g.NX - 2) + g.plane * (g.NZ - 2);
+    t0 = (int)(lo / kKsTile);
+    nt = (int)(hi / kKsTile) - t0 + 1;
+}
+// rows 3I..3I+2 of element lane e (packed tile ks [300][32], operand us
+// [24][32]) into w[(3I + c) * 32], w = the lane's slot of the W tile
+template <typename T, int I>
+__device__ __forceinline__ void coarse_elem_rows(const T *ks, const T *us, int e, T *w)
+{
+    T y[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                y[c] = fma(ks[sym_pack(3 * I + c, 3 * j + d) * kKsTile + e], us[(3 * j + d) * kKsTile + e], y[c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) w[(3 * I + c) * kKsTile] = y[c];
+}
+template <typename T, class In>
+__global__ void __launch_bounds__(kElemThreads)
+coarse_elem_kernel(In in0, const T *__restrict__ Ks, T *__restrict__ W0, int64_t wvs, Geom g, int t0, int nt,
+                   const int *__restrict__ done0, int *err)
+{
+    pdl_enter();
+    const int vk = blockIdx.y;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    const In in = in0.shift(vk);
+    T *W = W0 + vk * wvs;
+    extern __shared__ __align__(128) unsigned char coarse_smem[];
+    T *kbuf = reinterpret_cast<T *>(coarse_smem);          // two packed tiles
+    T *us = kbuf + 2 * kKsTileVals;                          // [24][32] element operands
+    const uint32_t bar = bulk::smem_addr(coarse_smem + CoarseElem<T>::kOffBar);   // one mbarrier per tile buffer
+    const int tid = threadIdx.x, e = tid & 31, i = tid >> 5;
+    const int cornerOff = cdy(i) + g.PY * cdx(i) + (int)g.plane * cdz(i);
+    if (tid == 0) {
+        bulk::bar_init(bar, 1u);
+        bulk::bar_init(bar + 8, 1u);
+        bulk::fence_init();
+    }
+    __syncthreads();
+    // tile k of this CTA's share into buffer k & 1 (thread 0)
+    auto issued = [&](int k) { return blockIdx.x + k * gridDim.x < nt; };
+    auto issue = [&](int k) {
+        if (!issued(k)) return;
+        const uint32_t b = bar + 8 * (k & 1);
+        bulk::arrive_expect(b, CoarseElem<T>::kTileBytes);
+        bulk::copy(bulk::smem_addr(kbuf + (k & 1) * kKsTileVals), Ks + (int64_t)(t0 + blockIdx.x + k * gridDim.x) * kKsTileVals,
+                   CoarseElem<T>::kTileBytes, b);
+    };
+    if (tid == 0) { issue(0); issue(1); }
+    // operand of corner i of element slot t*32 + e: node m = t*32 + e + cornerOff
+    const int mStep = (int)gridDim.x * kKsTile;
+    int m = (t0 + (int)blockIdx.x) * kKsTile + e + cornerOff;
+    T u0 = T(0), u1 = T(0), u2 = T(0);
+    if (issued(0)) { u0 = in(m, 0); u1 = in(m, 1); u2 = in(m, 2); }
+    int k = 0;
+    bool failed = false;
+    for (; issued(k); ++k) {
+        const int t = t0 + blockIdx.x + k * gridDim.x;
+        us[(3 * i + 0) * kKsTile + e] = u0;
+        us[(3 * i + 1) * kKsTile + e] = u1;
+        us[(3 * i + 2) * kKsTile + e] = u2;
+        const bool got = bulk::wait(bar + 8 * (k & 1), (uint32_t)(k >> 1) & 1u);
+        if (!__syncthreads_and(got)) { failed = true; break; }     // uniform: every thread leaves
+        m += mStep;
+        if (issued(k + 1)) { u0 = in(m, 0); u1 = in(m, 1); u2 = in(m, 2); }   // the next tile's operand, loaded during this one
+        const T *ks = kbuf + (k & 1) * kKsTileVals;
+        T *w = W + (int64_t)t * kWTileVals + e;
+        switch (i) {                                         // warp-uniform: immediate entry offsets
+        case 0: coarse_elem_rows<T, 0>(ks, us, e, w); break;
+        case 1: coarse_elem_rows<T, 1>(ks, us, e, w); break;
+        case 2: coarse_elem_rows<T, 2>(ks, us, e, w); break;
+        case 3: coarse_elem_rows<T, 3>(ks, us, e, w); break;
+        case 4: coarse_elem_rows<T, 4>(ks, us, e, w); break;
+        case 5: coarse_elem_rows<T, 5>(ks, us, e, w); break;
+        case 6: coarse_elem_rows<T, 6>(ks, us, e, w); break;
+        default: coarse_elem_rows<T, 7>(ks, us, e, w); break;
+        }
+        __syncthreads();                                     // buffer k & 1 and the operands are free
+        if (tid == 0) issue(k + 2);
+    }
+    if (failed && tid == 0) {
+        atomicExch(err, 1);
+        // tiles k and k + 1 may still be landing: wait for them (bounded)
+        for (int kk = k; kk < k + 2; ++kk)
+            if (issued(kk)) (void)bulk::wait(bar + 8 * (kk & 1), (uint32_t)(kk >> 1) & 1u);
+    }
+}
+template <typename T, class Out>
+__global__ void __launch_bounds__(kNodeThreads)
+coarse_gather_kernel(Out out0, const T *__restrict__ W0, int64_t wvs, Geom g, Reduce red0, const int *__restrict__ done0)
+{
+    pdl_enter();
+    const int vk = blockIdx.z;
+    const int *done = done_of(done0, vk);
+    if (done && *done) return;
+    const Out out = out0.shift(vk); const Reduce red = red0.at(vk);
+    const T *W = W0 + vk * wvs;
+    const int q = blockIdx.x * kNodeThreads + threadIdx.x;
+    const int Y = q % g.PY, X = q / g.PY, Z = blockIdx.y;
+    double dot = 0.0;
+    if (Y < g.NY && X < g.NX) {
+        const int idx = (int)(g.origin + Y + (int64_t)g.PY * X + g.plane * Z);
+        T p[8][3];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int slot = idx - cdy(i) - g.PY * cdx(i) - (int)g.plane * cdz(i);
+            const T *w = W + (int64_t)(slot >> 5) * kWTileVals + (slot & 31);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) p[i][c] = w[(3 * i + c) * kKsTile];
+        }
+        T s[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            s[c] = p[0][c];
+#pragma unroll
+            for (int k = 1; k < 8; ++k) s[c] += p[k][c];
+        }
+        out(idx, s, dot);
+    }
+    if (red.result) block_sum_to<kNodeThreads>(dot, red.partials, red.counter, red.result, gridDim.x * gridDim.y,
+                                               blockIdx.x + gridDim.x * blockIdx.y);
+}
+
+// ---------------------------------------------------------------------------
 // Transfers between level l (fine) and l+1 (coarse), span S.  Prolongation
 // is trilinear interpolation of the coarse field at the fine active nodes;
 // restriction is its transpose.  (TOP_GPU.m:817-878 express the same

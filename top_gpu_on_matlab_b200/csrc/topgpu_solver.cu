@@ -428,6 +428,21 @@ Geom make_geom(int ny, int nx, int nz)
 }
 inline int64_t gidx(const Geom &g, int Y, int X, int Z) { return g.origin + Y + (int64_t)g.PY * X + g.plane * Z; }
 
+// the device error flag of the two-pass coarse product (a tile copy wait that
+// gave up): read, cleared, reported
+int op_err_status(top_solver *s)
+{
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, s->opErr, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (e) {
+        CK(cudaMemsetAsync(s->opErr, 0, sizeof(int), s->st));
+        set_error("coarse product: a packed-matrix tile copy did not complete");
+        return TOP_ERR_CUDA;
+    }
+    return TOP_OK;
+}
+
 // ---- level operators ------------------------------------------------------
 template <typename T> const T *ks_packed(const DevLevel &l);
 template <> const double *ks_packed<double>(const DevLevel &l) { return l.KsP64; }
@@ -445,14 +460,54 @@ template <typename T> T *vt(DevLevel &l);
 template <> double *vt<double>(DevLevel &l) { return l.t64; }
 template <> float *vt<float>(DevLevel &l) { return l.t32; }
 
+template <typename T> T *wbuf(DevLevel &l);
+template <> double *wbuf<double>(DevLevel &l) { return l.W64; }
+template <> float *wbuf<float>(DevLevel &l) { return l.W32; }
+// resident CTAs per SM of the two-pass product's first pass (its dynamic
+// shared memory allowance set once; 0 when that fails)
+template <typename T, class In>
+int coarse_elem_occ()
+{
+    static const int occ = [] {
+        int n = 0;
+        if (cudaFuncSetAttribute(coarse_elem_kernel<T, In>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CoarseElem<T>::kSmem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, coarse_elem_kernel<T, In>, kElemThreads, CoarseElem<T>::kSmem) != cudaSuccess) {
+            (void)cudaGetLastError();
+            n = 0;
+        }
+        return n;
+    }();
+    return occ;
+}
+// the first-pass kernels of the V-cycle's coarse products, configured before
+// any launch is captured into a graph
+void coarse_elem_setup()
+{
+    (void)coarse_elem_occ<float, JacobiIn<float, float>>();
+    (void)coarse_elem_occ<float, VecIn<float, float>>();
+    (void)coarse_elem_occ<double, JacobiIn<double, double>>();
+    (void)coarse_elem_occ<double, VecIn<double, double>>();
+}
+
 // y-epilogue applied to (K_level in)(node) for every node of a coarse level;
 // nv right-hand sides in one launch (vectors at the functors' strides)
 template <typename T, class In, class Out>
 void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, const int *done, int nv = 1)
 {
     DevLevel &lv = s->L[l];
+    int t0 = 0, nt = 0;
+    coarse_elem_tiles(lv.g, t0, nt);
+    T *W = wbuf<T>(lv);
     if (s->coarseLanes) {
         launch_k(s, coarse_kernel<T, In, Out>, dim3(coarse_blocks(lv.g), (unsigned)nv), kNodeThreads, 0, s->st, in, out, ks_packed<T>(lv), lv.g, red, done);
+    } else if (W && s->opErr && nt > 0 && nt >= s->coarseTwoPassMin && coarse_elem_occ<T, In>() > 0) {
+        const int64_t wvs = w_alloc_vals(lv.g.cs);
+        const unsigned ctas = (unsigned)std::min<int64_t>(nt, (int64_t)s->numSMs * coarse_elem_occ<T, In>());
+        launch_k(s, coarse_elem_kernel<T, In>, dim3(ctas, (unsigned)nv), kElemThreads, CoarseElem<T>::kSmem, s->st,
+                 in, ks_packed<T>(lv), W, wvs, lv.g, t0, nt, done, s->opErr);
+        TOPGPU_COUNT_LAUNCH();
+        launch_k(s, coarse_gather_kernel<T, Out>, dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ, (unsigned)nv), kNodeThreads, 0, s->st,
+                 out, W, wvs, lv.g, red, done);
     } else {
         dim3 gr = coarse_tile_grid(lv.g); gr.z = (unsigned)nv;
         launch_k(s, coarse_tile_kernel<T, In, Out>, gr, dim3(kCoarseTileX, 8), 0, s->st, in, out, ks_packed<T>(lv), lv.g, red, done);
@@ -702,7 +757,9 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
             if (l < s->nL - 1) {
                 d.KsP64 = s->ksalloc<double>(cs);
                 d.KsP32 = s->ksalloc<float>(cs);
-                if (!d.KsP64 || !d.KsP32) return fail("out of device memory");
+                d.W64 = s->walloc<double>(cs, KM);
+                d.W32 = s->walloc<float>(cs, KM);
+                if (!d.KsP64 || !d.KsP32 || !d.W64 || !d.W32) return fail("out of device memory");
             }
         }
         if (!d.diag || !d.invD64 || !d.invD32 || !d.x64 || !d.t64 || !d.x32 || !d.t32) return fail("out of device memory");
@@ -842,9 +899,10 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
     s->counter = s->dalloc<unsigned>(4 + s->kMax);
     s->scal = s->dalloc<double>(16);
     s->zeroDone = s->dalloc<int>(4);
+    s->opErr = s->dalloc<int>(1);
     s->state = s->dalloc<PcgState>(s->kMax);
     if (cudaMallocHost(&s->hstate, sizeof(PcgState) * s->kMax) != cudaSuccess) s->hstate = nullptr;
-    if (!s->partials || !s->counter || !s->scal || !s->zeroDone || !s->state || !s->hstate) return fail("out of memory");
+    if (!s->partials || !s->counter || !s->scal || !s->zeroDone || !s->opErr || !s->state || !s->hstate) return fail("out of memory");
     // coarsest level maps
     {
         DevLevel &lc = s->L[s->nL - 1];
@@ -885,6 +943,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
             s->numSMs = nsm;
     }
+    coarse_elem_setup();
     // level-0 products in the Walsh basis where Ke allows it (voxel mode)
     if (s->super) s->walshOK = false;
     if (s->walshOK)
@@ -1127,8 +1186,7 @@ extern "C" int top_solver_matvec(top_solver *s, int level, const double *u, doub
     grid_to_compact_kernel<double, double><<<nb256(d.Nn), 256, 0, s->st>>>(d.t64, y, d.nodeGrid, d.Nn, d.g.cs);
     TOPGPU_COUNT_LAUNCH();
     CKL();
-    CK(cudaStreamSynchronize(s->st));
-    return TOP_OK;
+    return op_err_status(s);
 }
 
 extern "C" int top_solver_vcycle(top_solver *s, const double *r, double *z)
@@ -1143,8 +1201,7 @@ extern "C" int top_solver_vcycle(top_solver *s, const double *r, double *z)
     grid_to_compact_kernel<double, double><<<nb256(l0.Nn), 256, 0, s->st>>>(s->z, z, l0.nodeGrid, l0.Nn, l0.g.cs);
     TOPGPU_COUNT_LAUNCH();
     CKL();
-    CK(cudaStreamSynchronize(s->st));
-    return TOP_OK;
+    return op_err_status(s);
 }
 
 extern "C" int top_solver_restrict(top_solver *s, int ii, const double *rF, double *rC)
@@ -1359,7 +1416,8 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
         for (int k = 0; k < nrhs; ++k) all = all && s->hstate[k].done;
         if (all) break;
     }
-    int rc = TOP_OK;
+    int rc = op_err_status(s);
+    if (rc != TOP_OK) return rc;
     for (int k = 0; k < nrhs; ++k) {
         const PcgState &f = s->hstate[k];
         if (f.normB == 0.0) CK(cudaMemsetAsync(xg + k * nv - kMargin, 0, sizeof(double) * nv, st));
@@ -1512,5 +1570,5 @@ extern "C" int top_solver_time_kernel(top_solver *s, int which, int nrep, int64_
     }
     CKL();
     *msPerLaunch = total / nrep;
-    return TOP_OK;
+    return op_err_status(s);
 }

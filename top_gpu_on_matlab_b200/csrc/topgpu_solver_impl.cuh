@@ -21,6 +21,7 @@ struct DevLevel {
     uint8_t *flags = nullptr;
     int32_t *nodeGrid = nullptr, *eleGrid = nullptr, *upMap = nullptr;
     double *KsC = nullptr, *KsP64 = nullptr; float *KsP32 = nullptr;
+    double *W64 = nullptr; float *W32 = nullptr;   // element outputs of the two-pass coarse product
     double *diag = nullptr, *invD64 = nullptr; float *invD32 = nullptr;
     double *r64 = nullptr, *x64 = nullptr, *t64 = nullptr;
     float *r32 = nullptr, *x32 = nullptr, *t32 = nullptr;
@@ -46,6 +47,9 @@ struct top_solver {
     bool useGraphs = true;
     bool coarseLanes = std::getenv("TOPGPU_COARSE_LANES") != nullptr;   // 8-lanes-per-node coarse kernel
     int coarsePersistent = 0;        // levels from 1 (1) or from 2 (2) down of the V-cycle in one cooperative launch; 0 off
+    // coarse levels with at least this many packed tiles take the two-pass
+    // product (element outputs, then node sums; identical results)
+    int coarseTwoPassMin = std::getenv("TOPGPU_COARSE_TWOPASS_MIN") ? std::atoi(std::getenv("TOPGPU_COARSE_TWOPASS_MIN")) : 0;
     bool pdl = std::getenv("TOPGPU_NO_PDL") == nullptr;
     // span-4 transfers read and write four fine y slots as one aligned vector
     // (identical results; TOPGPU_NO_VEC4 selects the per-slot kernels)
@@ -74,6 +78,7 @@ struct top_solver {
     bool walshOK = false;            // Ke has the cube's reflection symmetry
     topgpu::TcOperandB *tcB = nullptr;   // kind 5: Ke as TF32 hi/lo tensor-core operand (device)
     int *tcErr = nullptr;            // kind 5: set by a kernel whose MMA wait gave up
+    int *opErr = nullptr;            // set by a two-pass coarse product whose tile copy wait gave up
     topgpu::WalshParam<double> W64{}; topgpu::WalshParam<float> W32{};
     topgpu::WalshPairParam<double> WP64{}; topgpu::WalshPairParam<float> WP32{};
     double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;
@@ -124,6 +129,13 @@ struct top_solver {
     {
         T *b = dalloc<T>((size_t)topgpu::ks_alloc_vals(cs));
         return b ? b + topgpu::kKsFront : nullptr;
+    }
+    // element outputs of the two-pass coarse product, nv right-hand sides
+    // (stride w_alloc_vals(cs)), each behind a zero guard tile
+    template <typename T> T *walloc(int64_t cs, int nv)
+    {
+        T *b = dalloc<T>((size_t)topgpu::w_alloc_vals(cs) * nv);
+        return b ? b + topgpu::kWFront : nullptr;
     }
     Reduce red(double *result) const { return Reduce{partials, counter, result}; }
     // per-right-hand-side sums into consecutive PcgState's (batched launches)
