@@ -352,10 +352,15 @@ int top_solver_set_pcg_beta(top_solver *s, int flexible);
  * step (the default); identical results.  No counterpart in the reference. */
 int top_solver_set_coarse_persistent(top_solver *s, int on);
 /* Autotuner: times each level-0 kernel configuration (kind, tile shape, CTA
- * count; nrep launches each, L2 flushed by writing flushBytes before every
- * launch) on this model and keeps the fastest per precision.  msBest2 gets
- * {FP64, FP32} ms per launch of the winners, configs8 their {kind, ty, tx,
- * ctas} (either may be NULL).  No counterpart in the reference. */
+ * count; nrep rounds, L2 flushed by writing flushBytes before every launch)
+ * on this model and keeps the fastest per precision.  A round is the
+ * level-0 products one PCG iteration of this solver makes with that
+ * precision's kernel, epilogues included: the outer product with its dot
+ * product, and the V-cycle's residual and post-smoothing products (FP32 in
+ * mixed precision, FP64 otherwise); a precision that serves none is timed on
+ * the plain product.  msBest2 gets {FP64, FP32} ms per round of the winners,
+ * configs8 their {kind, ty, tx, ctas} (either may be NULL).  No counterpart
+ * in the reference. */
 int top_solver_autotune(top_solver *s, int nrep, int64_t flushBytes, double *msBest2, int *configs8);
 
 /* Kernels this solver has launched since it was created (every entry point

@@ -73,6 +73,36 @@ def test_autotune_picks_a_working_kernel(model):
         s.set_l0_kernel(fp32, *k)
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_autotune_on_the_pcg_products(mixed):
+    """the autotuner times the products a PCG iteration makes (outer product
+    with its dot, V-cycle residual and post-smoothing products); a solver
+    tuned that way solves to the FP64 oracle's compliance"""
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    mask = np.ones((12, 24, 12), bool)
+    o = O.Model(mask, control=20000)
+    o.apply_optcase(1)
+    o.set_material(1.0, 1e-9, 3.0)
+    o.set_solver(1e-8, 800, 0.6)
+    m = Mesh(mask, control=20000)
+    m.apply_optcase(1)
+    s = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-8, maxIT=800, omega=0.6, mixed=mixed)
+    x = np.full(o.level(0).numElements, 0.3)
+    o.set_density(x)
+    o.assemble()
+    s.set_density(torch.from_numpy(x).cuda())
+    s.assemble()
+    res = s.autotune(nrep=2, flush_bytes=0)
+    assert res["fp64"][0] > 0 and res["fp32"][0] > 0
+    assert s.l0_kernel(False) == res["fp64"][1] and s.l0_kernel(True) == res["fp32"][1]
+    b = o.F()[:, 0]
+    xo, _, _ = o.pcg(b)
+    U, its, r = s.pcg(0)
+    assert r < 1e-8
+    c_o, c = b @ xo, float(torch.from_numpy(b).cuda() @ U)
+    assert abs(c - c_o) <= 1e-7 * abs(c_o)
+
+
 @pytest.mark.parametrize("shape", SHAPES)
 @pytest.mark.parametrize("ctas", [0, 1, 7, 100000])
 def test_walsh_matvec_matches_oracle(model, shape, ctas):

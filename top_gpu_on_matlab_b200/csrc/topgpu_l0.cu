@@ -370,21 +370,62 @@ int set_l0_kernel(top_solver *s, int p, int kind, int ty, int tx, int ctas)
 // y = K u launches on the solver's stream, L2 flushed before each) and keeps
 // the fastest per precision.
 namespace {
+// time per PCG iteration of the level-0 products precision slot p's kernel
+// serves, with their epilogues (L2 flushed before each): the outer product
+// v = A p with p . v (slot 0, or slot 1 when the outer product runs in FP32),
+// and the V-cycle's residual and post-smoothing products (slot 1 in mixed
+// precision, slot 0 in FP64).  The epilogues change the registers a kernel
+// holds and the bytes it moves, so the fastest configuration is chosen on the
+// launches the solver makes.  A slot that serves none times the plain product.
 double time_l0(top_solver *s, int p, int nrep, void *flush, size_t flushBytes, cudaEvent_t a, cudaEvent_t b)
 {
     DevLevel &l0 = s->L[0];
+    const int64_t cs = l0.g.cs;
+    const bool mixed = s->p.precision == TOP_PREC_MIXED, outer32 = s->p.outerFP32 != 0;
+    const bool outerHere = p == 0 ? !outer32 : outer32;
+    const bool vcycleHere = p == 0 ? !mixed : mixed;
     const Reduce none{nullptr, nullptr, nullptr};
+    const Reduce dot{s->partials, s->counter, s->scal + 8};
+    const float om32 = float(s->p.omega);
+    const double om64 = s->p.omega;
     double total = 0.0;
     for (int k = 0; k < nrep + 1; ++k) {
-        if (flush) cudaMemsetAsync(flush, k & 0xff, flushBytes, s->st);
-        cudaEventRecord(a, s->st);
-        if (p == 0) l0_op<double>(s, VecIn<double, double>{s->pv, l0.g.cs}, StoreOut<double, double>{s->v, l0.g.cs}, none, nullptr, 1);
-        else l0_op<float>(s, VecIn<float, float>{l0.x32, l0.g.cs}, StoreOut<float, float>{l0.t32, l0.g.cs}, none, nullptr, 1);
-        cudaEventRecord(b, s->st);
-        if (cudaEventSynchronize(b) != cudaSuccess) return -1.0;
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, a, b);
-        if (k > 0) total += ms;              // the first launch warms up
+        double t = 0.0;
+        bool ok = true;
+        auto timed = [&](auto &&launch) {
+            if (!ok) return;
+            if (flush) cudaMemsetAsync(flush, k & 0xff, flushBytes, s->st);
+            cudaEventRecord(a, s->st);
+            launch();
+            cudaEventRecord(b, s->st);
+            if (cudaEventSynchronize(b) != cudaSuccess) { ok = false; return; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, a, b);
+            t += ms;
+        };
+        if (p == 0) {
+            if (outerHere)
+                timed([&] { l0_op<double>(s, VecIn<double, double>{s->pv, cs}, DotStoreOut<double, double, double>{s->v, s->pv, cs}, dot, nullptr, 1); });
+            if (vcycleHere) {
+                timed([&] { l0_op<double>(s, VecIn<double, double>{l0.x64, cs}, ResidOut<double, double, double>{s->r, l0.t64, cs}, none, nullptr, 1); });
+                timed([&] { l0_op<double>(s, VecIn<double, double>{l0.x64, cs},
+                                          PostSmoothOut<double, double, double>{l0.x64, s->r, l0.invD64, s->z, cs, om64}, dot, nullptr, 1); });
+            }
+            if (!outerHere && !vcycleHere)
+                timed([&] { l0_op<double>(s, VecIn<double, double>{s->pv, cs}, StoreOut<double, double>{s->v, cs}, none, nullptr, 1); });
+        } else {
+            if (outerHere)
+                timed([&] { l0_op<float>(s, VecIn<float, double>{s->pv, cs}, DotStoreOut<float, double, double>{s->v, s->pv, cs}, dot, nullptr, 1); });
+            if (vcycleHere) {
+                timed([&] { l0_op<float>(s, VecIn<float, float>{l0.x32, cs}, ResidOut<float, double, float>{s->r, l0.t32, cs}, none, nullptr, 1); });
+                timed([&] { l0_op<float>(s, VecIn<float, float>{l0.x32, cs},
+                                         PostSmoothOut<float, double, float>{l0.x32, s->r, l0.invD32, s->z32, cs, om32}, dot, nullptr, 1); });
+            }
+            if (!outerHere && !vcycleHere)
+                timed([&] { l0_op<float>(s, VecIn<float, float>{l0.x32, cs}, StoreOut<float, float>{l0.t32, cs}, none, nullptr, 1); });
+        }
+        if (!ok) return -1.0;
+        if (k > 0) total += t;              // the first round warms up
     }
     return total / nrep;
 }

@@ -258,6 +258,7 @@ __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restri
     // two consecutive values per access (n and the vector bases are multiples
     // of four values, 16-byte aligned)
     const int64_t n2 = n >> 1;
+#pragma unroll 2
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += (int64_t)gridDim.x * blockDim.x) {
         double ra, rb, va, vb;
         T da, db;
@@ -1332,8 +1333,17 @@ int topgpu::pcg_block(top_solver *s, const double *bGrid, double *xg, int nrhs, 
     const int64_t cs = l0.g.cs, nv = 3 * cs;    // whole grid vectors, margins included
     cudaStream_t st = s->st;
     const int VB = vec_blocks(nv);
-    // the residual update: one resident wave of 256-thread CTAs (8 per SM)
-    const int UB = (int)std::min<int64_t>(std::min<int64_t>(8 * (int64_t)s->numSMs, (nv / 2 + 255) / 256), s->nPartials);
+    // the residual update: one resident wave of 256-thread CTAs
+    static const int updOcc = [] {
+        int n32 = 0, n64 = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n32, pcg_update_kernel<float>, 256, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n64, pcg_update_kernel<double>, 256, 0) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return 4;
+        }
+        return std::max(1, std::min(n32, n64));
+    }();
+    const int UB = (int)std::min<int64_t>(std::min<int64_t>((int64_t)updOcc * s->numSMs, (nv / 2 + 255) / 256), s->nPartials);
     const int64_t M = kMargin;
     const unsigned K = (unsigned)nrhs;
     // mixed precision keeps the FP32 V-cycle's output z in FP32

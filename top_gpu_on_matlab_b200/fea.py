@@ -368,8 +368,9 @@ class Solver:
         check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
 
     def autotune(self, nrep=5, flush_bytes=512 << 20):
-        """Pick the fastest level-0 kernel per precision on this model; returns
-        {"fp64": (ms, (kind, ty, tx, ctas)), "fp32": (...)}."""
+        """Pick the fastest level-0 kernel per precision on the products this
+        solver's PCG iteration makes (epilogues included); returns
+        {"fp64": (ms per iteration, (kind, ty, tx, ctas)), "fp32": (...)}."""
         ms = (C.c_double * 2)()
         cfg = (C.c_int * 8)()
         check(lib().top_solver_autotune(self._h, nrep, flush_bytes, ms, cfg), "top_solver_autotune")
