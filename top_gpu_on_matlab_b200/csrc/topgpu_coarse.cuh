@@ -102,7 +102,7 @@ coarse_vcycle_kernel(const CoarseVc<T> A, const int *__restrict__ done0)
                 }
                 if (!any) continue;                               // uniform in the CTA
                 double out[4];
-                coarsest_row(A.Ainv + nC * row, A.cr, nC, v0, act, red, out);
+                coarsest_row(A.Ainv + nC * row, CompactRhs{A.cr, nC}, nC, v0, act, red, out);
                 if (tid == 0)
 #pragma unroll
                     for (int q = 0; q < 4; ++q)

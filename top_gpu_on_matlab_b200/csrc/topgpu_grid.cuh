@@ -197,6 +197,7 @@ struct VecIn {
     __host__ __device__ VecIn(const TV *base, int64_t cs, int64_t vstride = 0) : u(base, cs), vs(vstride) {}
     __device__ __forceinline__ VecIn shift(int k) const { VecIn r = *this; if (k) r.u = u.shifted(k * vs); return r; }
     __device__ __forceinline__ T operator()(int m, int c) const { return T(u[c][m]); }
+    __device__ __forceinline__ void node3(int m, T v[3]) const { for (int c = 0; c < 3; ++c) v[c] = T(u[c][m]); }
 };
 // x = omega * invD .* r  (the Jacobi pre-smoothing step, evaluated on the fly)
 template <typename T, typename TR>
@@ -205,6 +206,7 @@ struct JacobiIn {
     __host__ __device__ JacobiIn(const TR *rb, const T *ib, int64_t cs, T om, int64_t vstride = 0) : r(rb, cs), invD(ib, cs), omega(om), vs(vstride) {}
     __device__ __forceinline__ JacobiIn shift(int k) const { JacobiIn o = *this; if (k) o.r = r.shifted(k * vs); return o; }
     __device__ __forceinline__ T operator()(int m, int c) const { return omega * invD[c][m] * T(r[c][m]); }
+    __device__ __forceinline__ void node3(int m, T v[3]) const { for (int c = 0; c < 3; ++c) v[c] = omega * invD[c][m] * T(r[c][m]); }
 };
 
 // Epilogues: what a node kernel does with y = (K u)(node).  pre(i) loads
@@ -733,19 +735,18 @@ coarse_elem_kernel(In in0, const T *__restrict__ Ks, T *__restrict__ W0, int64_t
     // operand of corner i of element slot t*32 + e: node m = t*32 + e + cornerOff
     const int mStep = (int)gridDim.x * kKsTile;
     int m = (t0 + (int)blockIdx.x) * kKsTile + e + cornerOff;
-    T u0 = T(0), u1 = T(0), u2 = T(0);
-    if (issued(0)) { u0 = in(m, 0); u1 = in(m, 1); u2 = in(m, 2); }
+    T u[3] = {T(0), T(0), T(0)};
+    if (issued(0)) in.node3(m, u);
     int k = 0;
     bool failed = false;
     for (; issued(k); ++k) {
         const int t = t0 + blockIdx.x + k * gridDim.x;
-        us[(3 * i + 0) * kKsTile + e] = u0;
-        us[(3 * i + 1) * kKsTile + e] = u1;
-        us[(3 * i + 2) * kKsTile + e] = u2;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) us[(3 * i + c) * kKsTile + e] = u[c];
         const bool got = bulk::wait(bar + 8 * (k & 1), (uint32_t)(k >> 1) & 1u);
         if (!__syncthreads_and(got)) { failed = true; break; }     // uniform: every thread leaves
         m += mStep;
-        if (issued(k + 1)) { u0 = in(m, 0); u1 = in(m, 1); u2 = in(m, 2); }   // the next tile's operand, loaded during this one
+        if (issued(k + 1)) in.node3(m, u);                   // the next tile's operand, loaded during this one
         const T *ks = kbuf + (k & 1) * kKsTileVals;
         T *w = W + (int64_t)t * kWTileVals + e;
         switch (i) {                                         // warp-uniform: immediate entry offsets
@@ -992,12 +993,23 @@ restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc
 }
 
 // One row of the coarsest direct solve, x(row) = A^-1(row, :) c, for the
-// right-hand sides v0 .. v0+3 whose act flag is set (c of right-hand side k
-// at cr + k n).  All kCoarsestThreads threads of the CTA call it: each keeps
+// right-hand sides v0 .. v0+3 whose act flag is set (cr(k, j): entry j of
+// right-hand side k).  All kCoarsestThreads threads of the CTA call it: each keeps
 // eight loads of the row in flight, the warps reduce by shuffles and thread
 // 0 adds the warp sums in a fixed order and returns them in out.
 constexpr int kCoarsestThreads = 256;
-__device__ __forceinline__ void coarsest_row(const double *__restrict__ a, const double *__restrict__ cr, int64_t n, int v0,
+// coarsest right-hand sides gathered in compact order (k at cr + k n)
+struct CompactRhs {
+    const double *cr; int64_t n;
+    __device__ __forceinline__ double operator()(int k, int64_t j) const { return cr[k * n + j]; }
+};
+// ... or read from the level's grid vector (k at r + k vs)
+template <typename T> struct GridRhs {
+    const T *r; int64_t vs, cs; const int32_t *nodeGrid;
+    __device__ __forceinline__ double operator()(int k, int64_t j) const { return double(r[k * vs + (j % 3) * cs + nodeGrid[j / 3]]); }
+};
+template <class Rhs>
+__device__ __forceinline__ void coarsest_row(const double *__restrict__ a, const Rhs &cr, int64_t n, int v0,
                                              const bool act[4], double (*red)[4], double out[4])
 {
     constexpr int U = 8, NW = kCoarsestThreads / 32;
@@ -1013,7 +1025,7 @@ __device__ __forceinline__ void coarsest_row(const double *__restrict__ a, const
             if (j >= n) break;
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-                if (act[q]) s[q] = fma(av[u], cr[(v0 + q) * n + j], s[q]);
+                if (act[q]) s[q] = fma(av[u], cr(v0 + q, j), s[q]);
         }
     }
 #pragma unroll
@@ -1166,17 +1178,17 @@ prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
     }
 }
 
-// one fine node (linear in-plane index q, layer Z) of the prolongation;
-// XB: the base omega*invD.*r was stored in xf beforehand (added in place)
+// the prolongation's value at the grid node (Y, X, Z) = slot i of the fine
+// grid (a node of the grid, Y < NY, X < NX): 0 at an inactive node, else
+// P xc (span S) plus the base -- the value xf holds there when XB,
+// omega*invD.*r when r is set
 template <typename T, int S, typename TR, bool XB = false>
-__device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geom &gc, T *__restrict__ xf, const Geom &gf,
-                                             const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
-                                             const T *__restrict__ invD, T omega, int q, int Z)
+__device__ __forceinline__ void prolong_value(const T *__restrict__ xc, const Geom &gc, const T *__restrict__ xf, const Geom &gf,
+                                              const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
+                                              const T *__restrict__ invD, T omega, int Y, int X, int Z, int64_t i, T v[3])
 {
-    const int Y = q % gf.PY, X = q / gf.PY;
-    if (Y >= gf.NY || X >= gf.NX) return;
-    const int64_t i = gf.origin + Y + (int64_t)gf.PY * X + gf.plane * Z;
-    T v[3] = {T(0), T(0), T(0)};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = T(0);
     if (flagsF[i] & kActive) {
         const int qy = Y / S, ry = Y - qy * S, qx = X / S, rx = X - qx * S, qz = Z / S, rz = Z - qz * S;
         const T wy[2] = {T(S - ry) / T(S), T(ry) / T(S)};
@@ -1206,6 +1218,19 @@ __device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geo
             for (int c = 0; c < 3; ++c) v[c] += omega * invD[c * gf.cs + i] * T(r[c * gf.cs + i]);
         }
     }
+}
+// one fine node (linear in-plane index q, layer Z) of the prolongation;
+// XB: the base omega*invD.*r was stored in xf beforehand (added in place)
+template <typename T, int S, typename TR, bool XB = false>
+__device__ __forceinline__ void prolong_node(const T *__restrict__ xc, const Geom &gc, T *__restrict__ xf, const Geom &gf,
+                                             const uint8_t *__restrict__ flagsF, const TR *__restrict__ r,
+                                             const T *__restrict__ invD, T omega, int q, int Z)
+{
+    const int Y = q % gf.PY, X = q / gf.PY;
+    if (Y >= gf.NY || X >= gf.NX) return;
+    const int64_t i = gf.origin + Y + (int64_t)gf.PY * X + gf.plane * Z;
+    T v[3];
+    prolong_value<T, S, TR, XB>(xc, gc, xf, gf, flagsF, r, invD, omega, Y, X, Z, i, v);
 #pragma unroll
     for (int c = 0; c < 3; ++c) xf[c * gf.cs + i] = v[c];
 }

@@ -175,24 +175,12 @@ __global__ void coarsest_assemble_kernel(const double *__restrict__ KsC, const i
     }
 }
 // ---- coarsest level ----
-// coarsest solve: x_grid = Ainv * r (r gathered from the grid in compact order)
-template <typename T>
-__global__ void coarsest_gather_kernel(const T *__restrict__ r, Geom g, const int32_t *__restrict__ nodeGrid,
-                                       int64_t Nn, double *__restrict__ cr, const int *__restrict__ done0, int64_t vs)
-{
-    pdl_enter();
-    const int vk = blockIdx.y;
-    const int *done = done_of(done0, vk);
-    if (done && *done) return;
-    r += vk * vs; cr += vk * 3 * Nn;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * Nn) return;
-    cr[t] = double(r[(t % 3) * g.cs + nodeGrid[t / 3]]);
-}
-// one CTA per row of A^-1, every right-hand side (up to four per pass over the row)
+// coarsest solve: x_grid = Ainv * r
+// one CTA per row of A^-1, every right-hand side (up to four per pass over the
+// row), read from the level's grid vector r in compact order
 template <typename T>
 __global__ void __launch_bounds__(kCoarsestThreads)
-coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__ cr, int64_t n,
+coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, int64_t n,
                      T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
                      const int *__restrict__ done0, int64_t vs, int nv)
 {
@@ -210,7 +198,7 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const double *__restrict__
         }
         if (!any) continue;                      // uniform in the CTA
         double out[4];
-        coarsest_row(Ainv + n * row, cr, n, v0, act, red, out);
+        coarsest_row(Ainv + n * row, GridRhs<T>{r, vs, g.cs, nodeGrid}, n, v0, act, red, out);
         if (threadIdx.x == 0)
 #pragma unroll
             for (int q = 0; q < 4; ++q)
@@ -628,11 +616,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         cudaLaunchKernelEx(&cfg, coarse_vcycle_kernel<T>, A, done);
         TOPGPU_COUNT_LAUNCH();
     } else {
-        // coarsest direct solve, FP64
-        launch_k(s, coarsest_gather_kernel<T>, dim3(nb256(n), K), 256, 0, s->st, vr<T>(lc), lc.g, lc.nodeGrid, lc.Nn, s->cr, done, lvs(lc));
-        TOPGPU_COUNT_LAUNCH();
-        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, 0, s->st, s->Ainv, s->cr, n, vt<T>(lc), lc.g,
-                                                                           lc.nodeGrid, done, lvs(lc), nv);
+        // coarsest direct solve, FP64 (the right-hand side read from the grid by the product)
+        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, 0, s->st, s->Ainv, (const T *)vr<T>(lc), n, vt<T>(lc), lc.g,
+                 lc.nodeGrid, done, lvs(lc), nv);
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
