@@ -63,10 +63,10 @@ WORKLOAD = "cantilever_96x192x96_ft1_optimisation_iterations"
 NCU_TRAFFIC = {
     ("fp64", 3, 16, 8, 1184): 74.58e6,
     ("fp64", 3, 16, 8, 1776): 74.51e6,
-    ("fp32", 3, 16, 16, 888): 32.90e6,
-    ("fp32", 3, 16, 8, 888): 38.11e6,
-    ("fp32", 3, 16, 8, 1776): 31.79e6,
-    ("fp32", 3, 16, 8, 2368): 31.69e6,
+    ("fp32", 3, 16, 16, 888): 32.89e6,
+    ("fp32", 3, 16, 8, 888): 38.16e6,
+    ("fp32", 3, 16, 8, 1776): 31.75e6,
+    ("fp32", 3, 16, 8, 2368): 31.68e6,
 }
 ITS_RECORD = ROOT / "bench_fp64_its.json"
 
