@@ -345,6 +345,13 @@ int top_solver_set_graphs(top_solver *s, int on);
  * iterates; compliance and the stopping test are unchanged.  No counterpart
  * in the reference. */
 int top_solver_set_pcg_beta(top_solver *s, int flexible);
+/* Test of the coarse product's failure path: the next two-pass coarse
+ * product withholds one packed-tile copy, so that copy's bounded wait
+ * (one second) runs out; the kernel raises its error flag and the calling
+ * entry point (top_solver_pcg, _vcycle, _matvec) returns TOP_ERR_CUDA with
+ * the message set.  One-shot; the solver stays usable.  No counterpart in
+ * the reference. */
+int top_solver_test_withhold_tile(top_solver *s);
 /* The coarse part of the V-cycle (coarse products, span-2 transfers,
  * coarsest solve) as one persistent cooperative launch with grid-wide
  * barriers: on = 1 from level 1 down, on = 2 from level 2 down (level 1

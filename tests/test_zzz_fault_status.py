@@ -1,7 +1,9 @@
 """Failures injected from the host, reported as statuses (none traps the GPU):
 element-node ids outside [1, numNodes] gather zeros instead of reading out of
 bounds, PCG at maxIT reports NOT_CONVERGED (the reference's warning,
-TOP_GPU.m:656-659), a non-finite right-hand side reports TOP_ERR_NAN."""
+TOP_GPU.m:656-659), a non-finite right-hand side reports TOP_ERR_NAN, and a
+withheld packed-tile copy makes the coarse product's bounded wait give up and
+report TOP_ERR_CUDA."""
 import numpy as np
 import pytest
 import torch
@@ -61,3 +63,35 @@ def test_pcg_non_finite_rhs_reports_nan():
     with pytest.raises(TopGpuError) as e:
         s.pcg(b=b)
     assert e.value.status == TOP_ERR_NAN and "non-finite" in str(e.value)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_coarse_tile_copy_wait_gives_up_and_reports(mixed):
+    """A packed-tile copy withheld by the test hook: the two-pass coarse
+    product's bounded wait for it runs out (one second), the kernel raises its
+    error flag and skips the rest of its tiles, and the V-cycle call reports
+    TOP_ERR_CUDA; the next calls on the same solver give the V-cycle and PCG
+    of a solver that never failed, bit for bit."""
+    from top_gpu_on_matlab_b200._lib import TOP_ERR_CUDA, TopGpuError
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    m = Mesh(np.ones((24, 48, 24), bool), control=50)
+    m.apply_optcase(1)
+    ne = m.info()[0]["numElements"]
+    x = torch.from_numpy(0.2 + 0.7 * np.random.default_rng(4).random(ne)).cuda()
+    r = torch.from_numpy(np.random.default_rng(5).standard_normal(3 * m.info()[0]["numNodes"])).cuda()
+    solvers = []
+    for _ in range(2):
+        s = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-8, maxIT=400, omega=0.6, mixed=mixed)
+        s.set_density(x)
+        s.assemble()
+        solvers.append(s)
+    ref = solvers[0].vcycle(r)
+    s = solvers[1]
+    s.test_withhold_tile()
+    with pytest.raises(TopGpuError) as e:
+        s.vcycle(r)
+    assert e.value.status == TOP_ERR_CUDA and "tile copy did not complete" in str(e.value)
+    assert torch.equal(s.vcycle(r), ref)
+    U0, its0, _ = solvers[0].pcg(0)
+    U1, its1, _ = s.pcg(0)
+    assert its0 == its1 and torch.equal(U0, U1)

@@ -493,7 +493,8 @@ void coarse_op(top_solver *s, int l, const In &in, const Out &out, Reduce red, c
         const int64_t wvs = w_alloc_vals(lv.g.cs);
         const unsigned ctas = (unsigned)std::min<int64_t>(nt, (int64_t)s->numSMs * coarse_elem_occ<T, In>());
         launch_k(s, coarse_elem_kernel<T, In>, dim3(ctas, (unsigned)nv), kElemThreads, CoarseElem<T>::kSmem, s->st,
-                 in, ks_packed<T>(lv), W, wvs, lv.g, t0, nt, done, s->opErr);
+                 in, ks_packed<T>(lv), W, wvs, lv.g, t0, nt, done, s->opErr, s->withholdTile ? 1 : 0);
+        s->withholdTile = false;
         TOPGPU_COUNT_LAUNCH();
         launch_k(s, coarse_gather_kernel<T, Out>, dim3((unsigned)lv.g.nbx, (unsigned)lv.g.NZ, (unsigned)nv), kNodeThreads, 0, s->st,
                  out, W, wvs, lv.g, red, done);
@@ -985,6 +986,13 @@ extern "C" int top_solver_set_pcg_beta(top_solver *s, int flexible)
     if (!s) return TOP_ERR_ARGS;
     s->flexible = flexible != 0;
     ++s->opGen;                      // captured PCG graphs change
+    return TOP_OK;
+}
+
+extern "C" int top_solver_test_withhold_tile(top_solver *s)
+{
+    if (!s) return TOP_ERR_ARGS;
+    s->withholdTile = true;
     return TOP_OK;
 }
 

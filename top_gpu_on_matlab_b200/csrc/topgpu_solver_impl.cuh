@@ -79,6 +79,9 @@ struct top_solver {
     topgpu::TcOperandB *tcB = nullptr;   // kind 5: Ke as TF32 hi/lo tensor-core operand (device)
     int *tcErr = nullptr;            // kind 5: set by a kernel whose MMA wait gave up
     int *opErr = nullptr;            // set by a two-pass coarse product whose tile copy wait gave up
+    // test of that give-up path: the next two-pass product withholds one tile copy
+    // (one-shot, armed by top_solver_test_withhold_tile)
+    bool withholdTile = false;
     topgpu::WalshParam<double> W64{}; topgpu::WalshParam<float> W32{};
     topgpu::WalshPairParam<double> WP64{}; topgpu::WalshPairParam<float> WP32{};
     double *KeDev = nullptr, *P4 = nullptr, *P2 = nullptr;

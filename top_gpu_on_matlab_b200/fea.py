@@ -363,6 +363,11 @@ class Solver:
         """False: the reference's beta = rho/rhoOld; True: flexible (Polak-Ribiere) beta."""
         check(lib().top_solver_set_pcg_beta(self._h, int(bool(flexible))), "top_solver_set_pcg_beta")
 
+    def test_withhold_tile(self):
+        """Arm the coarse product's failure-path test: the next two-pass
+        coarse product withholds one tile copy and the call reports it."""
+        check(lib().top_solver_test_withhold_tile(self._h), "top_solver_test_withhold_tile")
+
     def set_graphs(self, on):
         """Run PCG iterations as captured CUDA graphs (default) or launch by launch."""
         check(lib().top_solver_set_graphs(self._h, int(bool(on))), "top_solver_set_graphs")
