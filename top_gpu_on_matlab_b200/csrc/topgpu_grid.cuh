@@ -1016,6 +1016,11 @@ struct CompactRhs {
     const double *cr; int64_t n;
     __device__ __forceinline__ double operator()(int k, int64_t j) const { return cr[k * n + j]; }
 };
+// ... or staged in shared memory ([k - v0][n] for the group starting at v0)
+struct StagedRhs {
+    const double *s; int64_t n; int v0;
+    __device__ __forceinline__ double operator()(int k, int64_t j) const { return s[(k - v0) * n + j]; }
+};
 // ... or read from the level's grid vector (k at r + k vs)
 template <typename T> struct GridRhs {
     const T *r; int64_t vs, cs; const int32_t *nodeGrid;

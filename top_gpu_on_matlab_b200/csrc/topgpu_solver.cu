@@ -182,10 +182,11 @@ template <typename T>
 __global__ void __launch_bounds__(kCoarsestThreads)
 coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, int64_t n,
                      T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
-                     const int *__restrict__ done0, int64_t vs, int nv)
+                     const int *__restrict__ done0, int64_t vs, int nv, int staged)
 {
     pdl_enter();
     __shared__ double red[kCoarsestThreads / 32][4];
+    extern __shared__ double rstage[];           // staged: the right-hand sides [4][n]
     const int64_t row = blockIdx.x;
     for (int v0 = 0; v0 < nv; v0 += 4) {
         bool act[4];
@@ -198,7 +199,31 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, i
         }
         if (!any) continue;                      // uniform in the CTA
         double out[4];
-        coarsest_row(Ainv + n * row, GridRhs<T>{r, vs, g.cs, nodeGrid}, n, v0, act, red, out);
+        if (staged) {
+            // the right-hand sides into shared memory first (all the node-map
+            // loads of a thread, then all its value loads), then the same sums
+            __syncthreads();                     // the previous group's reads are done
+            for (int64_t j0 = threadIdx.x; j0 < n; j0 += (int64_t)kCoarsestThreads * 4) {
+                int32_t slot[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int64_t j = j0 + (int64_t)kCoarsestThreads * u;
+                    slot[u] = j < n ? nodeGrid[j / 3] : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int64_t j = j0 + (int64_t)kCoarsestThreads * u;
+                    if (j >= n) break;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (act[q]) rstage[q * n + j] = double(r[(v0 + q) * vs + (j % 3) * g.cs + slot[u]]);
+                }
+            }
+            __syncthreads();
+            coarsest_row(Ainv + n * row, StagedRhs{rstage, n, v0}, n, v0, act, red, out);
+        } else {
+            coarsest_row(Ainv + n * row, GridRhs<T>{r, vs, g.cs, nodeGrid}, n, v0, act, red, out);
+        }
         if (threadIdx.x == 0)
 #pragma unroll
             for (int q = 0; q < 4; ++q)
@@ -389,6 +414,17 @@ __global__ void compliance_kmat_kernel(const double *__restrict__ Kc, const doub
 
 using namespace topgpu;
 
+// dynamic shared memory of a GEMV that stages its right-hand sides (up to
+// four groups of n FP64 values, at most 96 KB), 0 beyond: those read them
+// from the grid
+template <typename T>
+size_t gemv_stage_bytes(int64_t n, int nv)
+{
+    constexpr size_t kMax = 96 * 1024;
+    static const bool attr = cudaFuncSetAttribute(coarsest_gemv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax) == cudaSuccess;
+    const size_t b = sizeof(double) * (size_t)(nv < 4 ? nv : 4) * (size_t)n;
+    return (attr && b <= kMax) ? b : 0;
+}
 
 namespace {
 
@@ -468,14 +504,16 @@ int coarse_elem_occ()
     }();
     return occ;
 }
-// the first-pass kernels of the V-cycle's coarse products, configured before
-// any launch is captured into a graph
+// the first-pass kernels of the V-cycle's coarse products and the coarsest
+// GEMV, configured before any launch is captured into a graph
 void coarse_elem_setup()
 {
     (void)coarse_elem_occ<float, JacobiIn<float, float>>();
     (void)coarse_elem_occ<float, VecIn<float, float>>();
     (void)coarse_elem_occ<double, JacobiIn<double, double>>();
     (void)coarse_elem_occ<double, VecIn<double, double>>();
+    (void)gemv_stage_bytes<float>(1, 1);
+    (void)gemv_stage_bytes<double>(1, 1);
 }
 
 // y-epilogue applied to (K_level in)(node) for every node of a coarse level;
@@ -618,8 +656,9 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     } else {
         // coarsest direct solve, FP64 (the right-hand side read from the grid by the product)
-        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, 0, s->st, s->Ainv, (const T *)vr<T>(lc), n, vt<T>(lc), lc.g,
-                 lc.nodeGrid, done, lvs(lc), nv);
+        const size_t sm = gemv_stage_bytes<T>(n, nv);
+        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, sm, s->st, s->Ainv, (const T *)vr<T>(lc), n, vt<T>(lc), lc.g,
+                 lc.nodeGrid, done, lvs(lc), nv, sm ? 1 : 0);
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
