@@ -270,20 +270,29 @@ __global__ void pcg_update_kernel(double *__restrict__ r, const double *__restri
     double rr = 0;
     // two consecutive values per access (n and the vector bases are multiples
     // of four values, 16-byte aligned)
-    const int64_t n2 = n >> 1;
-#pragma unroll 2
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += (int64_t)gridDim.x * blockDim.x) {
-        double ra, rb, va, vb;
-        T da, db;
-        ld2(r + 2 * j, ra, rb);
-        ld2(v + 2 * j, va, vb);
-        ld2(invD + 2 * j, da, db);
-        ra = ra - lambda * va;
-        rb = rb - lambda * vb;
-        st2(r + 2 * j, ra, rb);
-        st2(z1 + 2 * j, T(omega * da * T(ra)), T(omega * db * T(rb)));
-        rr += ra * ra;
-        rr += rb * rb;
+    const int64_t n2 = n >> 1, S = (int64_t)gridDim.x * blockDim.x;
+    // four grid strides per pass, every load issued before the first store (r
+    // is read and written, so the compiler cannot move the next pass's loads
+    // up); each thread still adds its rr terms in index order
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += 4 * S) {
+        double ra[4], rb[4], va[4], vb[4];
+        T da[4], db[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (j + q * S < n2) {
+                ld2(r + 2 * (j + q * S), ra[q], rb[q]);
+                ld2(v + 2 * (j + q * S), va[q], vb[q]);
+                ld2(invD + 2 * (j + q * S), da[q], db[q]);
+            }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (j + q * S < n2) {
+                const double a = ra[q] - lambda * va[q], b = rb[q] - lambda * vb[q];
+                st2(r + 2 * (j + q * S), a, b);
+                st2(z1 + 2 * (j + q * S), T(omega * da[q] * T(a)), T(omega * db[q] * T(b)));
+                rr += a * a;
+                rr += b * b;
+            }
     }
     if (block_sum_last<256>(rr, red.partials, red.counter, red.result, gridDim.x, blockIdx.x)) {
         __threadfence();
