@@ -345,6 +345,19 @@ int top_solver_set_graphs(top_solver *s, int on);
  * iterates; compliance and the stopping test are unchanged.  No counterpart
  * in the reference. */
 int top_solver_set_pcg_beta(top_solver *s, int flexible);
+/* The V-cycle from its highest level with at most 2500 active DOFs (above the
+ * coarsest) down, as one operator.  At assembly the library forms, in FP64 on
+ * that level's active DOFs, M = 2J - J K J + Q M' Q^T (J = omega D^-1,
+ * Q = (I - J K) P, P the prolongation from the level below, M' that level's
+ * operator or the coarsest inverse), and every V-cycle applies it with one
+ * GEMV (in the V-cycle's precision) instead of the smoothing products,
+ * transfers and coarsest solve of those levels.  Equal to those steps in
+ * exact arithmetic.  on = 1: use it, 0: do not, -1: the default (in mixed
+ * precision, not in FP64).  *level (may be NULL) receives the level it starts
+ * at, 0 when not in use (no level qualifies, super-element mode, or off).
+ * Takes effect at once on an assembled solver.  No counterpart in the
+ * reference. */
+int top_solver_set_tail_operator(top_solver *s, int on, int *level);
 /* Test of the coarse product's failure path: the next two-pass coarse
  * product withholds one packed-tile copy, so that copy's bounded wait
  * (one second) runs out; the kernel raises its error flag and the calling

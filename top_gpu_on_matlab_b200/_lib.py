@@ -121,6 +121,7 @@ SIGNATURES = {
     "top_solver_set_graphs": (_int, [_vp, _int]),
     "top_solver_set_pcg_beta": (_int, [_vp, _int]),
     "top_solver_test_withhold_tile": (_int, [_vp]),
+    "top_solver_set_tail_operator": (_int, [_vp, _int, _vp]),
     "top_solver_set_coarse_persistent": (_int, [_vp, _int]),
     "top_solver_sensitivity": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "top_solver_optimize": (_int, [_vp, _vp, _vp, _vp, _vp, _vp]),

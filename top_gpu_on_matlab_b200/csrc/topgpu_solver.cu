@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <type_traits>
 #include <vector>
 #include "topgpu_kernels.cuh"
 #include "topgpu_solver_impl.cuh"
@@ -231,6 +232,108 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, i
     }
 }
 
+// ---- the V-cycle's condensed tail: t = M r on one level's active DOFs ----
+// M (symmetric) by rows at stride ld (a multiple of four, zero beyond n), in
+// the V-cycle's precision T.  One warp per row, kTailRows rows per CTA.  Each
+// CTA first stages the right-hand sides (NQ per pass: 1, or up to 4) from the
+// level's grid vector into shared memory as FP64 (every node-map load of a
+// thread before its value loads), value j at [j % W][j / W] so that the lanes
+// of a warp, reading the W values of consecutive 16-byte row pieces, touch
+// consecutive words; each lane then reads its row in 16-byte pieces, eight in
+// flight, and sums in FP64; the lanes combine in a fixed shuffle tree.
+constexpr int kTailRows = 8, kTailThreads = 32 * kTailRows;
+constexpr int kTailStage = 10;                   // staged values per thread and right-hand side
+static_assert(top_solver::kTailMaxDofs <= (int64_t)kTailThreads * kTailStage, "tail staging covers every DOF");
+__device__ __forceinline__ double tail_piece(const float4 &v, int e) { return double(e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w); }
+__device__ __forceinline__ double tail_piece(const double2 &v, int e) { return e == 0 ? v.x : v.y; }
+template <typename T, int NQ>
+__global__ void __launch_bounds__(kTailThreads)
+tail_gemv_kernel(const T *__restrict__ M, int64_t ld, const T *__restrict__ r, int64_t n, T *__restrict__ x, Geom g,
+                 const int32_t *__restrict__ nodeGrid, const int *__restrict__ done0, int64_t vs, int nv)
+{
+    pdl_enter();
+    using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+    constexpr int W = 16 / (int)sizeof(T);       // values per piece
+    constexpr int PB = sizeof(T) == 4 ? 16 : 8;  // pieces per lane in flight
+    extern __shared__ double rs[];               // [NQ][W][ld / W]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t row = (int64_t)blockIdx.x * kTailRows + warp;
+    const int64_t nw = ld / W;
+    const V *Mr = reinterpret_cast<const V *>(M + (row < n ? row : 0) * ld);
+    // issued first, before the stopping flags are read: the row's first pieces,
+    // the node-map slots of the staged values and of the output (none of them
+    // written by the kernels this one follows)
+    V p[PB];
+#pragma unroll
+    for (int u = 0; u < PB; ++u) {
+        const int64_t b = lane + 32 * u;
+        if (row < n && b < nw) p[u] = __ldg(Mr + b);
+    }
+    int32_t slot[kTailStage];
+#pragma unroll
+    for (int u = 0; u < kTailStage; ++u) {
+        const int64_t j = threadIdx.x + (int64_t)kTailThreads * u;
+        slot[u] = j < n ? nodeGrid[j / 3] : 0;
+    }
+    const int64_t out = row < n ? (row % 3) * g.cs + nodeGrid[row / 3] : 0;
+    bool first = true;                           // p holds the row's first pieces
+    for (int v0 = 0; v0 < nv; v0 += NQ) {
+        bool act[NQ];
+        bool any = false;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int *d = done_of(done0, v0 + q);
+            act[q] = v0 + q < nv && !(d && *d);
+            any = any || act[q];
+        }
+        if (!any) continue;                      // uniform in the CTA
+        __syncthreads();                         // the previous pass's reads of rs are done
+#pragma unroll
+        for (int u = 0; u < kTailStage; ++u) {
+            const int64_t j = threadIdx.x + (int64_t)kTailThreads * u;
+            if (j < ld)
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                    rs[q * ld + (j % W) * nw + j / W] = (act[q] && j < n) ? double(r[(v0 + q) * vs + (j % 3) * g.cs + slot[u]]) : 0.0;
+        }
+        __syncthreads();
+        if (row < n) {
+            double acc[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+            for (int64_t b0 = lane; b0 < nw; b0 += 32 * PB) {
+                if (!first || b0 != lane) {
+#pragma unroll
+                    for (int u = 0; u < PB; ++u) {
+                        const int64_t b = b0 + 32 * u;
+                        if (b < nw) p[u] = __ldg(Mr + b);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < PB; ++u) {
+                    const int64_t b = b0 + 32 * u;
+                    if (b >= nw) break;
+#pragma unroll
+                    for (int e = 0; e < W; ++e) {
+                        const double mv = tail_piece(p[u], e);
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) acc[q] = fma(mv, rs[q * ld + e * nw + b], acc[q]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+            if (lane == 0)
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                    if (act[q]) x[(v0 + q) * vs + out] = T(acc[q]);
+        }
+        first = false;
+    }
+}
+
 // ---- PCG vector kernels (FP64, level-0 grid arrays) ----
 // PCG vector kernels run over whole grid vectors, margins and guard slots
 // included (all zero), as one contiguous range of n = 3 CS values
@@ -423,6 +526,10 @@ __global__ void compliance_kmat_kernel(const double *__restrict__ Kc, const doub
 
 using namespace topgpu;
 
+// the V-cycle's condensed tail (defined with the coarsest solve below)
+bool tail_on(const top_solver *s);
+int build_tail(top_solver *s, cudaStream_t st);
+
 // dynamic shared memory of a GEMV that stages its right-hand sides (up to
 // four groups of n FP64 values, at most 96 KB), 0 beyond: those read them
 // from the grid
@@ -433,6 +540,17 @@ size_t gemv_stage_bytes(int64_t n, int nv)
     static const bool attr = cudaFuncSetAttribute(coarsest_gemv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMax) == cudaSuccess;
     const size_t b = sizeof(double) * (size_t)(nv < 4 ? nv : 4) * (size_t)n;
     return (attr && b <= kMax) ? b : 0;
+}
+// dynamic shared memory of the tail GEMV (the right-hand sides of one pass);
+// 0 if the attribute could not be set (the V-cycle then runs every level)
+template <typename T>
+size_t tail_gemv_smem(int64_t ld, int nv)
+{
+    static const bool attr = cudaFuncSetAttribute(tail_gemv_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)(sizeof(double) * top_solver::kTailMaxDofs)) == cudaSuccess &&
+                             cudaFuncSetAttribute(tail_gemv_kernel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)(sizeof(double) * 4 * top_solver::kTailMaxDofs)) == cudaSuccess;
+    return attr ? sizeof(double) * (size_t)(nv == 1 ? 1 : 4) * (size_t)ld : 0;
 }
 
 namespace {
@@ -523,6 +641,8 @@ void coarse_elem_setup()
     (void)coarse_elem_occ<double, VecIn<double, double>>();
     (void)gemv_stage_bytes<float>(1, 1);
     (void)gemv_stage_bytes<double>(1, 1);
+    (void)tail_gemv_smem<float>(4, 1);
+    (void)tail_gemv_smem<double>(4, 1);
 }
 
 // y-epilogue applied to (K_level in)(node) for every node of a coarse level;
@@ -623,6 +743,10 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     // levels pl .. nL-1 as one persistent kernel where their transfers are span 2
     const int pl = coarse_persistent_level(s);
     const bool persist = pl > 0;
+    // levels tl .. nL-1 as the condensed tail's one GEMV (0: none); M is held
+    // in the precision of the solver's V-cycle
+    const bool tailT = sizeof(T) == (s->p.precision == TOP_PREC_MIXED ? 4u : 8u);
+    const int tl = (!persist && tailT && s->tailReady && tail_on(s) && tail_gemv_smem<T>(s->tailLd, nv) > 0) ? s->tailL : 0;
     if (!z1Ready) {
         DevLevel &l0 = s->L[0];
         const int64_t n0 = lvs(l0), M = kMargin;
@@ -631,7 +755,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     }
     // restriction leg
-    for (int l = 0; l < (persist ? pl : nL - 1); ++l) {
+    for (int l = 0; l < (persist ? pl : (tl ? tl : nL - 1)); ++l) {
         DevLevel &lv = s->L[l], &lc = s->L[l + 1];
         T *d = vt<T>(lv);
         const int64_t vs = lvs(lv);
@@ -644,7 +768,19 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     }
     DevLevel &lc = s->L[nL - 1];
     const int64_t n = 3 * lc.Nn;
-    if (persist) {
+    if (tl) {
+        // t = M r on level tl: the V-cycle of levels tl .. nL-1 in one operator
+        DevLevel &lt = s->L[tl];
+        const int64_t nt = 3 * lt.Nn;
+        const unsigned gt = (unsigned)((nt + kTailRows - 1) / kTailRows);
+        if (nv == 1)
+            launch_k(s, tail_gemv_kernel<T, 1>, gt, kTailThreads, tail_gemv_smem<T>(s->tailLd, nv), s->st,
+                     (const T *)s->tailMp, s->tailLd, (const T *)vr<T>(lt), nt, vt<T>(lt), lt.g, lt.nodeGrid, done, lvs(lt), nv);
+        else
+            launch_k(s, tail_gemv_kernel<T, 4>, gt, kTailThreads, tail_gemv_smem<T>(s->tailLd, nv), s->st,
+                     (const T *)s->tailMp, s->tailLd, (const T *)vr<T>(lt), nt, vt<T>(lt), lt.g, lt.nodeGrid, done, lvs(lt), nv);
+        TOPGPU_COUNT_LAUNCH();
+    } else if (persist) {
         CoarseVc<T> A{};
         A.n = nL - pl;
         for (int l = pl; l < nL; ++l) {
@@ -671,7 +807,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
-    for (int l = (persist ? pl - 1 : nL - 2); l >= 0; --l) {
+    for (int l = (persist ? pl - 1 : (tl ? tl - 1 : nL - 2)); l >= 0; --l) {
         DevLevel &lv = s->L[l], &lcn = s->L[l + 1];
         const T *xc = vt<T>(lcn);
         T *x = vx<T>(lv);
@@ -974,6 +1110,91 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         cudaMemcpy(s->nodeCompactC, nc.data(), sizeof(int32_t) * lc.g.cs, cudaMemcpyHostToDevice);
         s->eleCompactC += kMargin; s->nodeCompactC += kMargin;
     }
+    // the V-cycle's condensed tail: the highest level l >= 1 above the coarsest
+    // with at most kTailMaxDofs active DOFs (every level below it is smaller)
+    if (std::getenv("TOPGPU_NO_TAIL_OPERATOR")) s->tailMode = 0;
+    for (int l = 1; l <= s->nL - 2 && !s->tailL && !s->super; ++l)
+        if (3 * mesh->L[l].Nn <= top_solver::kTailMaxDofs) s->tailL = l;
+    if (s->tailL) {
+        for (int l = s->tailL; l <= s->nL - 2; ++l) {
+            const MeshLevel &Mf = mesh->L[l], &Mc = mesh->L[l + 1];
+            DevLevel &d = s->L[l];
+            const int NYf = d.ny + 1, NXf = d.nx + 1, NZf = d.nz + 1;
+            // grid slot -> compact node and element (as for the coarsest level)
+            std::vector<int32_t> ecl(d.g.cs, -1), ncl(d.g.cs, -1), nbr((size_t)Mf.Nn * 27, -1);
+            for (int64_t t = 0; t < (int64_t)Mf.nodMapForward.size(); ++t) {
+                const int32_t c = Mf.nodMapForward[t];
+                if (!c) continue;
+                const int Y = int(t % NYf), X = int((t / NYf) % NXf), Z = int(t / ((int64_t)NYf * NXf));
+                ncl[gidx(d.g, Y, X, Z) + kMargin] = c - 1;
+                // the nodes that share an element with it (K's nonzero blocks of the row)
+                int q = 0;
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dx = -1; dx <= 1; ++dx)
+                        for (int dy = -1; dy <= 1; ++dy, ++q) {
+                            const int y = Y + dy, x = X + dx, z = Z + dz;
+                            if (y < 0 || y >= NYf || x < 0 || x >= NXf || z < 0 || z >= NZf) continue;
+                            const int32_t cn = Mf.nodMapForward[y + (int64_t)NYf * x + (int64_t)NYf * NXf * z];
+                            if (cn) nbr[(size_t)(c - 1) * 27 + q] = cn - 1;
+                        }
+            }
+            for (int64_t e = 0; e < Mf.Ne; ++e) {
+                const int64_t gE = Mf.eleMapBack[e] - 1;
+                const int ey = int(gE % d.ny), ex = int((gE / d.ny) % d.nx), ez = int(gE / ((int64_t)d.ny * d.nx));
+                ecl[gidx(d.g, ey, ex, ez) + kMargin] = (int32_t)e;
+            }
+            // the prolongation from level l+1 on the active DOFs (DOF 3 node + c):
+            // the trilinear weights the V-cycle's prolongation applies per component,
+            // stored transposed (row k of P contiguous)
+            const int S = s->L[l + 1].span, NYc = s->L[l + 1].ny + 1, NXc = s->L[l + 1].nx + 1;
+            const int64_t nf = 3 * Mf.Nn, nco = 3 * Mc.Nn;
+            std::vector<double> Pt((size_t)(nf * nco), 0.0);
+            for (int64_t t = 0; t < (int64_t)Mf.nodMapForward.size(); ++t) {
+                const int32_t cf = Mf.nodMapForward[t];
+                if (!cf) continue;
+                const int Y = int(t % NYf), X = int((t / NYf) % NXf), Z = int(t / ((int64_t)NYf * NXf));
+                const int qy = Y / S, ry = Y - qy * S, qx = X / S, rx = X - qx * S, qz = Z / S, rz = Z - qz * S;
+                const double wy[2] = {double(S - ry) / S, double(ry) / S};
+                const double wx[2] = {double(S - rx) / S, double(rx) / S};
+                const double wz[2] = {double(S - rz) / S, double(rz) / S};
+                for (int bz = 0; bz < 2; ++bz) {
+                    if (bz && rz == 0) continue;
+                    for (int bx = 0; bx < 2; ++bx) {
+                        if (bx && rx == 0) continue;
+                        for (int by = 0; by < 2; ++by) {
+                            if (by && ry == 0) continue;
+                            const int32_t cc = Mc.nodMapForward[(qy + by) + (int64_t)NYc * (qx + bx) + (int64_t)NYc * NXc * (qz + bz)];
+                            if (!cc) continue;
+                            const double w = wz[bz] * wx[bx] * wy[by];
+                            for (int c = 0; c < 3; ++c) Pt[(size_t)((3 * (cc - 1) + c) + nco * (3 * (cf - 1) + c))] = w;
+                        }
+                    }
+                }
+            }
+            int32_t *ne = s->dalloc<int32_t>(d.g.cs), *nn = s->dalloc<int32_t>(d.g.cs), *nb = s->dalloc<int32_t>(nbr.size());
+            double *Pd = s->dalloc<double>(Pt.size()), *Md = s->dalloc<double>((size_t)(nf * nf));
+            if (!ne || !nn || !nb || !Pd || !Md) return fail("out of device memory");
+            cudaMemcpy(ne, ecl.data(), sizeof(int32_t) * d.g.cs, cudaMemcpyHostToDevice);
+            cudaMemcpy(nn, ncl.data(), sizeof(int32_t) * d.g.cs, cudaMemcpyHostToDevice);
+            cudaMemcpy(nb, nbr.data(), sizeof(int32_t) * nbr.size(), cudaMemcpyHostToDevice);
+            cudaMemcpy(Pd, Pt.data(), sizeof(double) * Pt.size(), cudaMemcpyHostToDevice);
+            s->tailEleCompact.push_back(ne + kMargin);
+            s->tailNodeCompact.push_back(nn + kMargin);
+            s->tailNbr.push_back(nb);
+            s->tailPt.push_back(Pd);
+            s->tailMs.push_back(Md);
+        }
+        // scratch sized by the top tail level (the largest n and m)
+        const int64_t n = 3 * mesh->L[s->tailL].Nn, m = 3 * mesh->L[s->tailL + 1].Nn;
+        s->tailLd = (n + 3) / 4 * 4;
+        s->tailK = s->dalloc<double>((size_t)(n * n));
+        s->tailQ = s->dalloc<double>((size_t)(n * m));
+        s->tailT = s->dalloc<double>((size_t)(n * m));
+        s->tailJ = s->dalloc<double>((size_t)n);
+        if (s->p.precision == TOP_PREC_MIXED) s->tailMp = s->dalloc<float>((size_t)(n * s->tailLd));
+        else s->tailMp = s->dalloc<double>((size_t)(n * s->tailLd));
+        if (!s->tailK || !s->tailQ || !s->tailT || !s->tailJ || !s->tailMp) return fail("out of device memory");
+    }
     {
         int dev = 0, nsm = 0;
         if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
@@ -1027,6 +1248,21 @@ extern "C" int top_solver_set_coarse_persistent(top_solver *s, int on)
     s->coarsePersistent = on;
     ++s->opGen;                      // captured PCG graphs change
     return TOP_OK;
+}
+
+extern "C" int top_solver_set_tail_operator(top_solver *s, int on, int *level)
+{
+    if (!s || on < -1 || on > 1) { set_error("top_solver_set_tail_operator: bad arguments"); return TOP_ERR_ARGS; }
+    s->tailMode = on;
+    s->tailReady = false;
+    ++s->opGen;                      // captured PCG graphs change
+    int rc = TOP_OK;
+    if (tail_on(s) && s->assembled) {
+        rc = build_tail(s, s->st);
+        if (rc == TOP_OK && cudaStreamSynchronize(s->st) != cudaSuccess) { set_error("top_solver_set_tail_operator: CUDA error"); rc = TOP_ERR_CUDA; }
+    }
+    if (level) *level = tail_on(s) ? s->tailL : 0;
+    return rc;
 }
 
 extern "C" int top_solver_set_pcg_beta(top_solver *s, int flexible)
@@ -1119,6 +1355,101 @@ void dgemm(cudaStream_t st, bool ta, bool tb, double *C, int64_t ldc, const doub
 }
 }  // namespace
 
+// ---- the V-cycle's condensed tail: its operator, at assembly --------------
+// The V-cycle at level l (one damped-Jacobi step from zero, residual,
+// restriction, the levels below, prolongation onto the Jacobi iterate, one
+// damped-Jacobi step) is linear in the level's residual r:
+//     t = J r,  x = t + P M' P^T (r - K t),  z = x + J (r - K x)
+//     =>  M = 2 J - J K J + Q M' Q^T,   Q = (I - J K) P,   J = omega D^-1,
+// M' the operator of the level below (the coarsest level's: its inverse);
+// TOP_GPU.m:766-816 in matrix form, the restriction being the prolongation's
+// transpose on the active DOFs.  Dense FP64 on the levels' active DOFs (DOF
+// 3 node + component), column-major, symmetric.
+__global__ void tail_jacobi_kernel(double *__restrict__ J, const double *__restrict__ invD, const int32_t *__restrict__ nodeGrid,
+                                   int64_t Nn, int64_t cs, double omega)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3 * Nn) return;
+    J[i] = omega * invD[(i % 3) * cs + nodeGrid[i / 3]];
+}
+// Q = P - diag(J) K P; (K P)(i, j) sums over the 27 nodes that share an
+// element with row i's node (K's nonzero blocks of the row), in a fixed order
+__global__ void tail_q_kernel(double *__restrict__ Q, const double *__restrict__ Pt, const double *__restrict__ K,
+                              const double *__restrict__ J, const int32_t *__restrict__ nbr, int64_t n, int64_t m)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n * m) return;
+    const int64_t i = k / m, j = k % m;          // j fastest: the reads of P^T coalesce
+    double acc = 0.0;
+    for (int t = 0; t < 27; ++t) {
+        const int32_t nb = nbr[(i / 3) * 27 + t];
+        if (nb < 0) continue;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int64_t c = 3 * (int64_t)nb + d;
+            acc = fma(K[i + n * c], Pt[j + m * c], acc);
+        }
+    }
+    Q[i + n * j] = Pt[j + m * i] - J[i] * acc;
+}
+// M (lower triangle from the GEMM) += 2 diag(J) - diag(J) K diag(J), mirrored
+// into the upper triangle: M exactly symmetric
+__global__ void tail_m_kernel(double *__restrict__ M, const double *__restrict__ K, const double *__restrict__ J, int64_t n)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n * n) return;
+    const int64_t i = k % n, j = k / n;
+    if (i < j) return;
+    const double v = M[k] + (i == j ? 2.0 * J[i] : 0.0) - J[i] * K[k] * J[j];
+    M[k] = v;
+    if (i != j) M[j + n * i] = v;
+}
+// the V-cycle's copy: row i of M (= column i) at stride ld, zero beyond n
+template <typename T>
+__global__ void tail_pack_kernel(T *__restrict__ Mp, int64_t ld, const double *__restrict__ M, int64_t n)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n * ld) return;
+    const int64_t i = k / ld, j = k % ld;
+    Mp[k] = j < n ? T(M[j + n * i]) : T(0);
+}
+
+bool tail_on(const top_solver *s)
+{
+    return s->tailL > 0 && (s->tailMode == 1 || (s->tailMode == -1 && s->p.precision == TOP_PREC_MIXED));
+}
+// M of levels nL-2 .. tailL from the current assembly (after the coarsest inverse)
+int build_tail(top_solver *s, cudaStream_t st)
+{
+    s->tailReady = false;
+    if (!tail_on(s)) return TOP_OK;
+    const double *Mnext = s->Ainv;
+    for (int l = s->nL - 2; l >= s->tailL; --l) {
+        const size_t k = (size_t)(l - s->tailL);
+        DevLevel &lv = s->L[l];
+        const int64_t n = 3 * lv.Nn, m = 3 * s->L[l + 1].Nn;
+        double *K = s->tailK, *M = s->tailMs[k];
+        CK(cudaMemsetAsync(K, 0, sizeof(double) * n * n, st));
+        coarsest_assemble_kernel<<<nb256(n), 256, 0, st>>>(lv.KsC, lv.nodeGrid, s->tailEleCompact[k], s->tailNodeCompact[k], lv.g, lv.Nn, K);
+        tail_jacobi_kernel<<<nb256(n), 256, 0, st>>>(s->tailJ, lv.invD64, lv.nodeGrid, lv.Nn, lv.g.cs, s->p.omega);
+        tail_q_kernel<<<nb256(n * m), 256, 0, st>>>(s->tailQ, s->tailPt[k], K, s->tailJ, s->tailNbr[k], n, m);
+        dgemm(st, false, true, s->tailT, n, s->tailQ, n, Mnext, m, n, m, m, 1.0, 0.0, false, false);   // T = Q M'
+        dgemm(st, false, false, M, n, s->tailT, n, s->tailQ, n, n, n, m, 1.0, 0.0, true, false);      // T Q^T, lower
+        tail_m_kernel<<<nb256(n * n), 256, 0, st>>>(M, K, s->tailJ, n);
+        s->launches += 6;
+        Mnext = M;
+    }
+    const int64_t n = 3 * s->L[s->tailL].Nn;
+    if (s->p.precision == TOP_PREC_MIXED)
+        tail_pack_kernel<float><<<nb256(n * s->tailLd), 256, 0, st>>>(static_cast<float *>(s->tailMp), s->tailLd, s->tailMs[0], n);
+    else
+        tail_pack_kernel<double><<<nb256(n * s->tailLd), 256, 0, st>>>(static_cast<double *>(s->tailMp), s->tailLd, s->tailMs[0], n);
+    TOPGPU_COUNT_LAUNCH();
+    CKL();
+    s->tailReady = true;
+    return TOP_OK;
+}
+
 int coarsest_inverse(top_solver *s, cudaStream_t st)
 {
     const int64_t n = s->nC, nblk = (n + kDb - 1) / kDb;
@@ -1203,6 +1534,7 @@ extern "C" int top_solver_assemble(top_solver *s)
     CK(cudaMemcpyAsync(&flag, s->zeroDone + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (flag) { set_error("top_solver_assemble: coarsest matrix is not positive definite"); return TOP_ERR_NAN; }
+    { const int rc = build_tail(s, st); if (rc) return rc; }
     s->assembled = true;
     return TOP_OK;
 }

@@ -79,6 +79,20 @@ struct top_solver {
     topgpu::TcOperandB *tcB = nullptr;   // kind 5: Ke as TF32 hi/lo tensor-core operand (device)
     int *tcErr = nullptr;            // kind 5: set by a kernel whose MMA wait gave up
     int *opErr = nullptr;            // set by a two-pass coarse product whose tile copy wait gave up
+    // The V-cycle from level tailL down as one operator M (dense, symmetric, on
+    // that level's active DOFs), formed at assembly and applied by one GEMV.
+    // tailL 0: no level qualifies.  tailMode: -1 the default (on in mixed
+    // precision, off in FP64), 0 off, 1 on.
+    static constexpr int64_t kTailMaxDofs = 2500;
+    int tailL = 0, tailMode = -1;
+    bool tailReady = false;          // tailMp matches the current assembly
+    std::vector<double *> tailPt;    // prolongation of level l+1 into l, transposed: [j + m k], l = tailL..nL-2
+    std::vector<int32_t *> tailNbr;  // per compact node of those levels: 27 neighbour nodes (-1: none)
+    std::vector<int32_t *> tailNodeCompact, tailEleCompact;   // grid slot -> compact node / element
+    std::vector<double *> tailMs;    // M of levels tailL..nL-2, column-major, FP64
+    double *tailK = nullptr, *tailQ = nullptr, *tailT = nullptr, *tailJ = nullptr;
+    void *tailMp = nullptr;          // M of level tailL by rows at stride tailLd, in the V-cycle's precision
+    int64_t tailLd = 0;
     // test of that give-up path: the next two-pass product withholds one tile copy
     // (one-shot, armed by top_solver_test_withhold_tile)
     bool withholdTile = false;

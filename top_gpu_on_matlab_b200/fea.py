@@ -363,6 +363,15 @@ class Solver:
         """False: the reference's beta = rho/rhoOld; True: flexible (Polak-Ribiere) beta."""
         check(lib().top_solver_set_pcg_beta(self._h, int(bool(flexible))), "top_solver_set_pcg_beta")
 
+    def set_tail_operator(self, on):
+        """The V-cycle from its highest level with at most 2500 DOFs down as one
+        operator formed at assembly: True / False / None (the default: in mixed
+        precision only).  Returns the level it starts at (0: not in use)."""
+        level = C.c_int(0)
+        mode = -1 if on is None else int(bool(on))
+        check(lib().top_solver_set_tail_operator(self._h, mode, C.byref(level)), "top_solver_set_tail_operator")
+        return level.value
+
     def test_withhold_tile(self):
         """Arm the coarse product's failure-path test: the next two-pass
         coarse product withholds one tile copy and the call reports it."""
