@@ -890,11 +890,11 @@ inline unsigned restrict_blocks(const Geom &gc)
     return (unsigned)((threads + kNodeThreads - 1) / kNodeThreads);
 }
 
-// Separable restriction (trilinear weights factor per axis), one axis per
-// pass: pass A folds the fine y taps, t[c][QY][X][Z] = sum_oy w(oy)
-// r_f[c][S QY + oy][X][Z] (dense NYc x NXf x NZf per component), passes B and
-// C fold x and z.  Same weights and clipping as restrict_kernel; every pass
-// reads runs of consecutive QY.  V4 (S = 4): the seven taps 4 QY - 3 ..
+// Separable restriction (trilinear weights factor per axis): pass A folds the
+// fine y taps, t[c][QY][X][Z] = sum_oy w(oy) r_f[c][S QY + oy][X][Z] (dense
+// NYc x NXf x NZf per component), passes B and C (one launch) fold x, then z.
+// Same weights and clipping as restrict_kernel; every pass reads runs of
+// consecutive QY.  V4 (S = 4): the seven taps 4 QY - 3 ..
 // 4 QY + 3 come from two aligned four-value loads per component (slots
 // 4 QY - 4 .. 4 QY + 3 of the column; the first and any past NY are not used),
 // summed in the same order.
@@ -944,65 +944,59 @@ restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc,
 #pragma unroll
     for (int c = 0; c < 3; ++c) t[c * nt + k] = acc[c];
 }
-// pass B: fold the x taps, t2[c][QY][QX][Z] = sum_ox w(ox) t[c][QY][S QX + ox][Z]
+// passes B and C in one launch: CTA (QX, QZ, 32 coarse y nodes) of 2S-1
+// warps; warp w folds the x taps of fine plane Z = S QZ + w - (S-1) (the x
+// pass's sum, in its order) into shared memory, then the first warp folds the
+// z taps in the z pass's order: the two passes' results, bit for bit, without
+// their intermediate array and second launch
 template <typename T, int S>
-__global__ void __launch_bounds__(256)
-restrict_x_kernel(const T *__restrict__ t, int NYc, int NXf, int NXc, int NZf, T *__restrict__ t2, const int *__restrict__ done0,
-                  int64_t vsT = 0, int64_t vsT2 = 0)
+__global__ void __launch_bounds__(32 * (2 * S - 1))
+restrict_xz_kernel(const T *__restrict__ t, int NXf, int NZf, T *__restrict__ rc, Geom gc,
+                   const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsT = 0, int64_t vsC = 0)
 {
     pdl_enter();
-    const int vk = blockIdx.y;
+    const int vk = blockIdx.z;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
-    t += vk * vsT; t2 += vk * vsT2;
-    const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf;
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n2) return;
-    const int QY = (int)(k % NYc), QX = (int)((k / NYc) % NXc), Z = (int)(k / ((int64_t)NYc * NXc));
-    T acc[3] = {T(0), T(0), T(0)};
-#pragma unroll
-    for (int ox = -(S - 1); ox <= S - 1; ++ox) {
-        const int X = S * QX + ox;
-        if (X < 0 || X >= NXf) continue;
-        const T w = T(S - (ox < 0 ? -ox : ox)) / T(S);
-        const int64_t o = QY + (int64_t)NYc * (X + (int64_t)NXf * Z);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) acc[c] = fma(w, t[c * nt + o], acc[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) t2[c * n2 + k] = acc[c];
-}
-// pass C: fold the z taps into every active coarse node
-template <typename T, int S>
-__global__ void __launch_bounds__(256)
-restrict_z_kernel(const T *__restrict__ t2, int NZf, T *__restrict__ rc, Geom gc,
-                  const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsT2 = 0, int64_t vsC = 0)
-{
-    pdl_enter();
-    const int vk = blockIdx.y;
-    const int *done = done_of(done0, vk);
-    if (done && *done) return;
-    t2 += vk * vsT2; rc += vk * vsC;
+    t += vk * vsT; rc += vk * vsC;
     const int NYc = gc.NY, NXc = gc.NX;
-    const int64_t nq = (int64_t)NYc * NXc * gc.NZ, n2 = (int64_t)NYc * NXc * NZf;
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nq) return;
-    const int QY = (int)(k % NYc), QX = (int)((k / NYc) % NXc), QZ = (int)(k / ((int64_t)NYc * NXc));
-    const int64_t ic = gc.origin + QY + (int64_t)gc.PY * QX + gc.plane * QZ;
+    const int64_t nt = (int64_t)NYc * NXf * NZf;
+    const int QX = (int)(blockIdx.x % NXc), QZ = (int)(blockIdx.x / NXc);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int QY = (int)blockIdx.y * 32 + lane;
+    __shared__ T sx[2 * S - 1][3][32];
+    const int Z = S * QZ + w - (S - 1);
     T acc[3] = {T(0), T(0), T(0)};
-    if (flagsC[ic] & kActive) {
+    if (QY < NYc && Z >= 0 && Z < NZf) {
 #pragma unroll
-        for (int oz = -(S - 1); oz <= S - 1; ++oz) {
-            const int Z = S * QZ + oz;
-            if (Z < 0 || Z >= NZf) continue;
-            const T w = T(S - (oz < 0 ? -oz : oz)) / T(S);
-            const int64_t o = QY + (int64_t)NYc * (QX + (int64_t)NXc * Z);
+        for (int ox = -(S - 1); ox <= S - 1; ++ox) {
+            const int X = S * QX + ox;
+            if (X < 0 || X >= NXf) continue;
+            const T wt = T(S - (ox < 0 ? -ox : ox)) / T(S);
+            const int64_t o = QY + (int64_t)NYc * (X + (int64_t)NXf * Z);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) acc[c] = fma(w, t2[c * n2 + o], acc[c]);
+            for (int c = 0; c < 3; ++c) acc[c] = fma(wt, t[c * nt + o], acc[c]);
         }
     }
 #pragma unroll
-    for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
+    for (int c = 0; c < 3; ++c) sx[w][c][lane] = acc[c];
+    __syncthreads();
+    if (w == 0 && QY < NYc) {
+        const int64_t ic = gc.origin + QY + (int64_t)gc.PY * QX + gc.plane * QZ;
+        T out[3] = {T(0), T(0), T(0)};
+        if (flagsC[ic] & kActive) {
+#pragma unroll
+            for (int oz = -(S - 1); oz <= S - 1; ++oz) {
+                const int Zz = S * QZ + oz;
+                if (Zz < 0 || Zz >= NZf) continue;
+                const T wt = T(S - (oz < 0 ? -oz : oz)) / T(S);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) out[c] = fma(wt, sx[oz + S - 1][c][lane], out[c]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = out[c];
+    }
 }
 
 // One row of the coarsest direct solve, x(row) = A^-1(row, :) c, for the

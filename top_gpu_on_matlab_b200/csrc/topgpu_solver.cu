@@ -685,18 +685,17 @@ void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int n
     const unsigned K = (unsigned)nv;
     if (lc.span == 4) {
         const int NYc = lc.g.NY, NXf = lv.g.NX, NXc = lc.g.NX, NZf = lv.g.NZ;
-        const int64_t nt = (int64_t)NYc * NXf * NZf, n2 = (int64_t)NYc * NXc * NZf, nq = (int64_t)NYc * NXc * lc.g.NZ;
-        const int64_t vsS = 3 * (nt + n2);          // scratch per right-hand side
-        T *t1 = rscratch<T>(s), *t2 = t1 + 3 * nt;
+        const int64_t nt = (int64_t)NYc * NXf * NZf;
+        const int64_t vsS = 3 * nt;                 // scratch per right-hand side
+        T *t1 = rscratch<T>(s);
         const dim3 gy((unsigned)((nt + 255) / 256), K);
         if (s->vec4 && vec4_ok(lv.g, {d}, {lvs(lv)}))
             launch_k(s, restrict_y_kernel<T, 4, true>, gy, 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
         else
             launch_k(s, restrict_y_kernel<T, 4>, gy, 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
         TOPGPU_COUNT_LAUNCH();
-        launch_k(s, restrict_x_kernel<T, 4>, dim3((unsigned)((n2 + 255) / 256), K), 256, 0, s->st, t1, NYc, NXf, NXc, NZf, t2, done, vsS, vsS);
-        TOPGPU_COUNT_LAUNCH();
-        launch_k(s, restrict_z_kernel<T, 4>, dim3((unsigned)((nq + 255) / 256), K), 256, 0, s->st, t2, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc));
+        launch_k(s, restrict_xz_kernel<T, 4>, dim3((unsigned)(NXc * lc.g.NZ), (unsigned)((NYc + 31) / 32), K), 32 * 7, 0, s->st,
+                 t1, NXf, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc));
     } else {
         launch_k(s, restrict_kernel<T, 2>, dim3(restrict_blocks<2>(lc.g), K), kNodeThreads, 0, s->st, d, lv.g, rc, lc.g, lc.flags, done,
                                                                                            lvs(lv), lvs(lc));
@@ -962,7 +961,7 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         int64_t nt = 1;
         for (int l = 0; l + 1 < s->nL; ++l)
             if (s->L[l + 1].span == 4)
-                nt = std::max<int64_t>(nt, (int64_t)s->L[l + 1].g.NY * (s->L[l].g.NX + s->L[l + 1].g.NX) * s->L[l].g.NZ);
+                nt = std::max<int64_t>(nt, (int64_t)s->L[l + 1].g.NY * s->L[l].g.NX * s->L[l].g.NZ);
         s->rscr64 = s->dalloc<double>((size_t)3 * nt * s->kMax);
         s->rscr32 = s->dalloc<float>((size_t)3 * nt * s->kMax);
         if (!s->rscr64 || !s->rscr32) return fail("out of device memory");
