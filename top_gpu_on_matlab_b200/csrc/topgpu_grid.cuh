@@ -833,7 +833,8 @@ template <int S> struct RestrictLanes { static constexpr int value = (S >= 4) ? 
 // lane layout (LPN lanes per coarse node; every lane of a warp must call it)
 template <typename T, int S>
 __device__ __forceinline__ void restrict_lanes(const T *__restrict__ rf, const Geom &gf, T *__restrict__ rc, const Geom &gc,
-                                               const uint8_t *__restrict__ flagsC, int64_t gt)
+                                               const uint8_t *__restrict__ flagsC, int64_t gt, T *__restrict__ cmp = nullptr,
+                                               const int32_t *__restrict__ slotCmp = nullptr)
 {
     constexpr int LPN = RestrictLanes<S>::value, W = 2 * S - 1;
     const int64_t node = gt / LPN;
@@ -869,19 +870,28 @@ __device__ __forceinline__ void restrict_lanes(const T *__restrict__ rf, const G
     if (valid && lane == 0) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = acc[c];
+        // also in compact order (3 node + c) when asked: the condensed tail's operand
+        if (cmp) {
+            const int32_t kc = slotCmp[ic];
+            if (kc >= 0)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) cmp[3 * (int64_t)kc + c] = acc[c];
+        }
     }
 }
 template <typename T, int S>
 __global__ void __launch_bounds__(kNodeThreads)
 restrict_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ rc, Geom gc,
-                const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsF = 0, int64_t vsC = 0)
+                const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsF = 0, int64_t vsC = 0,
+                T *__restrict__ cmp = nullptr, const int32_t *__restrict__ slotCmp = nullptr, int64_t vsCmp = 0)
 {
     pdl_enter();
     const int vk = blockIdx.y;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
     rf += vk * vsF; rc += vk * vsC;
-    restrict_lanes<T, S>(rf, gf, rc, gc, flagsC, (int64_t)blockIdx.x * kNodeThreads + threadIdx.x);
+    if (cmp) cmp += vk * vsCmp;
+    restrict_lanes<T, S>(rf, gf, rc, gc, flagsC, (int64_t)blockIdx.x * kNodeThreads + threadIdx.x, cmp, slotCmp);
 }
 template <int S>
 inline unsigned restrict_blocks(const Geom &gc)
@@ -952,13 +962,15 @@ restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc,
 template <typename T, int S>
 __global__ void __launch_bounds__(32 * (2 * S - 1))
 restrict_xz_kernel(const T *__restrict__ t, int NXf, int NZf, T *__restrict__ rc, Geom gc,
-                   const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsT = 0, int64_t vsC = 0)
+                   const uint8_t *__restrict__ flagsC, const int *__restrict__ done0, int64_t vsT = 0, int64_t vsC = 0,
+                   T *__restrict__ cmp = nullptr, const int32_t *__restrict__ slotCmp = nullptr, int64_t vsCmp = 0)
 {
     pdl_enter();
     const int vk = blockIdx.z;
     const int *done = done_of(done0, vk);
     if (done && *done) return;
     t += vk * vsT; rc += vk * vsC;
+    if (cmp) cmp += vk * vsCmp;
     const int NYc = gc.NY, NXc = gc.NX;
     const int64_t nt = (int64_t)NYc * NXf * NZf;
     const int QX = (int)(blockIdx.x % NXc), QZ = (int)(blockIdx.x / NXc);
@@ -996,6 +1008,12 @@ restrict_xz_kernel(const T *__restrict__ t, int NXf, int NZf, T *__restrict__ rc
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) rc[c * gc.cs + ic] = out[c];
+        if (cmp) {                               // also in compact order (the condensed tail's operand)
+            const int32_t kc = slotCmp[ic];
+            if (kc >= 0)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) cmp[3 * (int64_t)kc + c] = out[c];
+        }
     }
 }
 

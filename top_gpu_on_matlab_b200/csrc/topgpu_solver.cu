@@ -234,48 +234,37 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, i
 
 // ---- the V-cycle's condensed tail: t = M r on one level's active DOFs ----
 // M (symmetric) by rows at stride ld (a multiple of four, zero beyond n), in
-// the V-cycle's precision T.  One warp per row, kTailRows rows per CTA.  Each
-// CTA first stages the right-hand sides (NQ per pass: 1, or up to 4) from the
-// level's grid vector into shared memory as FP64 (every node-map load of a
-// thread before its value loads), value j at [j % W][j / W] so that the lanes
-// of a warp, reading the W values of consecutive 16-byte row pieces, touch
-// consecutive words; each lane then reads its row in 16-byte pieces, eight in
-// flight, and sums in FP64; the lanes combine in a fixed shuffle tree.
+// the V-cycle's precision T; r in compact order (DOF 3 node + component, zero
+// beyond n, right-hand side k at rc + k ld), written by the restriction into
+// the level.  One warp per row, kTailRows rows per CTA; each lane reads its
+// row and r in 16-byte pieces (r, 8 KB per right-hand side, from L1 after the
+// first warp), PB pieces of each in flight, the first batch of M issued before
+// the stopping flags are read, and sums in FP64; the lanes combine in a fixed
+// shuffle tree.  The result goes to the level's grid vector.
 constexpr int kTailRows = 8, kTailThreads = 32 * kTailRows;
-constexpr int kTailStage = 10;                   // staged values per thread and right-hand side
-static_assert(top_solver::kTailMaxDofs <= (int64_t)kTailThreads * kTailStage, "tail staging covers every DOF");
 __device__ __forceinline__ double tail_piece(const float4 &v, int e) { return double(e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w); }
 __device__ __forceinline__ double tail_piece(const double2 &v, int e) { return e == 0 ? v.x : v.y; }
 template <typename T, int NQ>
 __global__ void __launch_bounds__(kTailThreads)
-tail_gemv_kernel(const T *__restrict__ M, int64_t ld, const T *__restrict__ r, int64_t n, T *__restrict__ x, Geom g,
+tail_gemv_kernel(const T *__restrict__ M, int64_t ld, const T *__restrict__ rc, int64_t n, T *__restrict__ x, Geom g,
                  const int32_t *__restrict__ nodeGrid, const int *__restrict__ done0, int64_t vs, int nv)
 {
     pdl_enter();
     using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
     constexpr int W = 16 / (int)sizeof(T);       // values per piece
-    constexpr int PB = sizeof(T) == 4 ? 16 : 8;  // pieces per lane in flight
-    extern __shared__ double rs[];               // [NQ][W][ld / W]
+    constexpr int PB = NQ == 1 ? 8 : 4;          // pieces of M per lane in flight
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t row = (int64_t)blockIdx.x * kTailRows + warp;
+    if (row >= n) return;                        // no barriers below
     const int64_t nw = ld / W;
-    const V *Mr = reinterpret_cast<const V *>(M + (row < n ? row : 0) * ld);
-    // issued first, before the stopping flags are read: the row's first pieces,
-    // the node-map slots of the staged values and of the output (none of them
-    // written by the kernels this one follows)
+    const V *Mr = reinterpret_cast<const V *>(M + row * ld);
     V p[PB];
 #pragma unroll
     for (int u = 0; u < PB; ++u) {
         const int64_t b = lane + 32 * u;
-        if (row < n && b < nw) p[u] = __ldg(Mr + b);
+        if (b < nw) p[u] = __ldg(Mr + b);
     }
-    int32_t slot[kTailStage];
-#pragma unroll
-    for (int u = 0; u < kTailStage; ++u) {
-        const int64_t j = threadIdx.x + (int64_t)kTailThreads * u;
-        slot[u] = j < n ? nodeGrid[j / 3] : 0;
-    }
-    const int64_t out = row < n ? (row % 3) * g.cs + nodeGrid[row / 3] : 0;
+    const int64_t out = (row % 3) * g.cs + nodeGrid[row / 3];
     bool first = true;                           // p holds the row's first pieces
     for (int v0 = 0; v0 < nv; v0 += NQ) {
         bool act[NQ];
@@ -286,50 +275,48 @@ tail_gemv_kernel(const T *__restrict__ M, int64_t ld, const T *__restrict__ r, i
             act[q] = v0 + q < nv && !(d && *d);
             any = any || act[q];
         }
-        if (!any) continue;                      // uniform in the CTA
-        __syncthreads();                         // the previous pass's reads of rs are done
+        if (!any) continue;
+        double acc[NQ];
 #pragma unroll
-        for (int u = 0; u < kTailStage; ++u) {
-            const int64_t j = threadIdx.x + (int64_t)kTailThreads * u;
-            if (j < ld)
-#pragma unroll
-                for (int q = 0; q < NQ; ++q)
-                    rs[q * ld + (j % W) * nw + j / W] = (act[q] && j < n) ? double(r[(v0 + q) * vs + (j % 3) * g.cs + slot[u]]) : 0.0;
-        }
-        __syncthreads();
-        if (row < n) {
-            double acc[NQ];
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
-            for (int64_t b0 = lane; b0 < nw; b0 += 32 * PB) {
-                if (!first || b0 != lane) {
-#pragma unroll
-                    for (int u = 0; u < PB; ++u) {
-                        const int64_t b = b0 + 32 * u;
-                        if (b < nw) p[u] = __ldg(Mr + b);
-                    }
-                }
+        for (int q = 0; q < NQ; ++q) acc[q] = 0.0;
+        for (int64_t b0 = lane; b0 < nw; b0 += 32 * PB) {
+            if (!first || b0 != lane) {
 #pragma unroll
                 for (int u = 0; u < PB; ++u) {
                     const int64_t b = b0 + 32 * u;
-                    if (b >= nw) break;
+                    if (b < nw) p[u] = __ldg(Mr + b);
+                }
+            }
+            V rv[NQ][PB];
 #pragma unroll
-                    for (int e = 0; e < W; ++e) {
-                        const double mv = tail_piece(p[u], e);
+            for (int q = 0; q < NQ; ++q) {
+                const V *R = reinterpret_cast<const V *>(rc + (int64_t)(act[q] ? v0 + q : v0) * ld);
 #pragma unroll
-                        for (int q = 0; q < NQ; ++q) acc[q] = fma(mv, rs[q * ld + e * nw + b], acc[q]);
-                    }
+                for (int u = 0; u < PB; ++u) {
+                    const int64_t b = b0 + 32 * u;
+                    if (b < nw) rv[q][u] = __ldg(R + b);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < NQ; ++q)
+            for (int u = 0; u < PB; ++u) {
+                const int64_t b = b0 + 32 * u;
+                if (b >= nw) break;
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-            if (lane == 0)
+                for (int e = 0; e < W; ++e) {
+                    const double mv = tail_piece(p[u], e);
 #pragma unroll
-                for (int q = 0; q < NQ; ++q)
-                    if (act[q]) x[(v0 + q) * vs + out] = T(acc[q]);
+                    for (int q = 0; q < NQ; ++q) acc[q] = fma(mv, tail_piece(rv[q][u], e), acc[q]);
+                }
+            }
         }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < NQ; ++q)
+                if (act[q]) x[(v0 + q) * vs + out] = T(acc[q]);
         first = false;
     }
 }
@@ -541,17 +528,6 @@ size_t gemv_stage_bytes(int64_t n, int nv)
     const size_t b = sizeof(double) * (size_t)(nv < 4 ? nv : 4) * (size_t)n;
     return (attr && b <= kMax) ? b : 0;
 }
-// dynamic shared memory of the tail GEMV (the right-hand sides of one pass);
-// 0 if the attribute could not be set (the V-cycle then runs every level)
-template <typename T>
-size_t tail_gemv_smem(int64_t ld, int nv)
-{
-    static const bool attr = cudaFuncSetAttribute(tail_gemv_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)(sizeof(double) * top_solver::kTailMaxDofs)) == cudaSuccess &&
-                             cudaFuncSetAttribute(tail_gemv_kernel<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)(sizeof(double) * 4 * top_solver::kTailMaxDofs)) == cudaSuccess;
-    return attr ? sizeof(double) * (size_t)(nv == 1 ? 1 : 4) * (size_t)ld : 0;
-}
 
 namespace {
 
@@ -641,8 +617,6 @@ void coarse_elem_setup()
     (void)coarse_elem_occ<double, VecIn<double, double>>();
     (void)gemv_stage_bytes<float>(1, 1);
     (void)gemv_stage_bytes<double>(1, 1);
-    (void)tail_gemv_smem<float>(4, 1);
-    (void)tail_gemv_smem<double>(4, 1);
 }
 
 // y-epilogue applied to (K_level in)(node) for every node of a coarse level;
@@ -679,7 +653,8 @@ inline int64_t lvs(const DevLevel &l) { return 3 * l.g.cs; }
 // restriction of the level-l residual d onto level l+1 (TOP_GPU.m:817-847);
 // d and rc at the level vector strides
 template <typename T>
-void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int nv = 1)
+void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int nv = 1, T *cmp = nullptr,
+                 const int32_t *slotCmp = nullptr, int64_t vsCmp = 0)
 {
     DevLevel &lv = s->L[l], &lc = s->L[l + 1];
     const unsigned K = (unsigned)nv;
@@ -695,10 +670,10 @@ void restrict_op(top_solver *s, int l, const T *d, T *rc, const int *done, int n
             launch_k(s, restrict_y_kernel<T, 4>, gy, 256, 0, s->st, d, lv.g, t1, NYc, done, lvs(lv), vsS);
         TOPGPU_COUNT_LAUNCH();
         launch_k(s, restrict_xz_kernel<T, 4>, dim3((unsigned)(NXc * lc.g.NZ), (unsigned)((NYc + 31) / 32), K), 32 * 7, 0, s->st,
-                 t1, NXf, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc));
+                 t1, NXf, NZf, rc, lc.g, lc.flags, done, vsS, lvs(lc), cmp, slotCmp, vsCmp);
     } else {
         launch_k(s, restrict_kernel<T, 2>, dim3(restrict_blocks<2>(lc.g), K), kNodeThreads, 0, s->st, d, lv.g, rc, lc.g, lc.flags, done,
-                                                                                           lvs(lv), lvs(lc));
+                                                                                           lvs(lv), lvs(lc), cmp, slotCmp, vsCmp);
     }
     TOPGPU_COUNT_LAUNCH();
 }
@@ -745,7 +720,7 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     // levels tl .. nL-1 as the condensed tail's one GEMV (0: none); M is held
     // in the precision of the solver's V-cycle
     const bool tailT = sizeof(T) == (s->p.precision == TOP_PREC_MIXED ? 4u : 8u);
-    const int tl = (!persist && tailT && s->tailReady && tail_on(s) && tail_gemv_smem<T>(s->tailLd, nv) > 0) ? s->tailL : 0;
+    const int tl = (!persist && tailT && s->tailReady && tail_on(s)) ? s->tailL : 0;
     if (!z1Ready) {
         DevLevel &l0 = s->L[0];
         const int64_t n0 = lvs(l0), M = kMargin;
@@ -763,7 +738,11 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         else
             coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega, vs}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs, vs},
                          none, done, nv);
-        restrict_op<T>(s, l, d, vr<T>(lc), done, nv);
+        // into the tail's level: r also in compact order, the GEMV's operand
+        if (tl && l + 1 == tl)
+            restrict_op<T>(s, l, d, vr<T>(lc), done, nv, static_cast<T *>(s->tailR), s->tailNodeCompact[0], s->tailLd);
+        else
+            restrict_op<T>(s, l, d, vr<T>(lc), done, nv);
     }
     DevLevel &lc = s->L[nL - 1];
     const int64_t n = 3 * lc.Nn;
@@ -773,11 +752,11 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         const int64_t nt = 3 * lt.Nn;
         const unsigned gt = (unsigned)((nt + kTailRows - 1) / kTailRows);
         if (nv == 1)
-            launch_k(s, tail_gemv_kernel<T, 1>, gt, kTailThreads, tail_gemv_smem<T>(s->tailLd, nv), s->st,
-                     (const T *)s->tailMp, s->tailLd, (const T *)vr<T>(lt), nt, vt<T>(lt), lt.g, lt.nodeGrid, done, lvs(lt), nv);
+            launch_k(s, tail_gemv_kernel<T, 1>, gt, kTailThreads, 0, s->st,
+                     (const T *)s->tailMp, s->tailLd, (const T *)s->tailR, nt, vt<T>(lt), lt.g, lt.nodeGrid, done, lvs(lt), nv);
         else
-            launch_k(s, tail_gemv_kernel<T, 4>, gt, kTailThreads, tail_gemv_smem<T>(s->tailLd, nv), s->st,
-                     (const T *)s->tailMp, s->tailLd, (const T *)vr<T>(lt), nt, vt<T>(lt), lt.g, lt.nodeGrid, done, lvs(lt), nv);
+            launch_k(s, tail_gemv_kernel<T, 4>, gt, kTailThreads, 0, s->st,
+                     (const T *)s->tailMp, s->tailLd, (const T *)s->tailR, nt, vt<T>(lt), lt.g, lt.nodeGrid, done, lvs(lt), nv);
         TOPGPU_COUNT_LAUNCH();
     } else if (persist) {
         CoarseVc<T> A{};
@@ -1190,9 +1169,14 @@ extern "C" int top_solver_create(const top_mesh *mesh, const top_solver_params *
         s->tailQ = s->dalloc<double>((size_t)(n * m));
         s->tailT = s->dalloc<double>((size_t)(n * m));
         s->tailJ = s->dalloc<double>((size_t)n);
-        if (s->p.precision == TOP_PREC_MIXED) s->tailMp = s->dalloc<float>((size_t)(n * s->tailLd));
-        else s->tailMp = s->dalloc<double>((size_t)(n * s->tailLd));
-        if (!s->tailK || !s->tailQ || !s->tailT || !s->tailJ || !s->tailMp) return fail("out of device memory");
+        if (s->p.precision == TOP_PREC_MIXED) {
+            s->tailMp = s->dalloc<float>((size_t)(n * s->tailLd));
+            s->tailR = s->dalloc<float>((size_t)(s->tailLd * s->kMax));
+        } else {
+            s->tailMp = s->dalloc<double>((size_t)(n * s->tailLd));
+            s->tailR = s->dalloc<double>((size_t)(s->tailLd * s->kMax));
+        }
+        if (!s->tailK || !s->tailQ || !s->tailT || !s->tailJ || !s->tailMp || !s->tailR) return fail("out of device memory");
     }
     {
         int dev = 0, nsm = 0;

@@ -92,6 +92,7 @@ struct top_solver {
     std::vector<double *> tailMs;    // M of levels tailL..nL-2, column-major, FP64
     double *tailK = nullptr, *tailQ = nullptr, *tailT = nullptr, *tailJ = nullptr;
     void *tailMp = nullptr;          // M of level tailL by rows at stride tailLd, in the V-cycle's precision
+    void *tailR = nullptr;           // its operand in compact order (stride tailLd per right-hand side, zero beyond n)
     int64_t tailLd = 0;
     // test of that give-up path: the next two-pass product withholds one tile copy
     // (one-shot, armed by top_solver_test_withhold_tile)
