@@ -35,6 +35,7 @@ struct FilterState {
     double *invD = nullptr;  // Jacobi of the filter operator, node grid
     double *rhs = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *v = nullptr, *eg = nullptr;
     PcgState *st = nullptr;
+    double *part2 = nullptr;           // per-CTA partials of rho = z.r (the update's second sum)
     cudaGraphExec_t chunk = nullptr;   // kChunk filter-PCG iterations as one graph (built on first use)
     int64_t chunkNodes = 0;
 };
@@ -208,32 +209,9 @@ __global__ void fpcg_init_kernel(const double *__restrict__ b, double *__restric
     }
     block_sum_to<256>(s1, bb.partials, bb.counter, bb.result);
 }
-__global__ void fpcg_update_kernel(double *__restrict__ x, double *__restrict__ r, double *__restrict__ z,
-                                   const double *__restrict__ p, const double *__restrict__ v,
-                                   const double *__restrict__ invD, int64_t n, PcgState *st, Reduce rr)
-{   // x += l p ; r -= l v ; z = M r ; ||r||^2 (rho from z.r in a second pass)
-    if (st->done) return;
-    const double l = st->rho / st->pv;
-    double s = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += l * p[i];
-        const double ri = r[i] - l * v[i];
-        r[i] = ri;
-        z[i] = invD[i] * ri;
-        s += ri * ri;
-    }
-    block_sum_to<256>(s, rr.partials, rr.counter, rr.result);
-}
-__global__ void fpcg_zr_kernel(const double *__restrict__ z, const double *__restrict__ r, int64_t n, PcgState *st, Reduce red)
+// the filter-PCG check: same stopping rule as Solving_PCG (TOP_GPU.m:637-649)
+__device__ __forceinline__ void fpcg_check(PcgState *st)
 {
-    if (st->done) return;
-    double s = 0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += z[i] * r[i];
-    block_sum_to<256>(s, red.partials, red.counter, red.result);
-}
-__global__ void fpcg_check_kernel(PcgState *st)
-{   // same stopping rule as Solving_PCG (TOP_GPU.m:637-649)
-    if (st->done) return;
     st->its += 1;
     const double res = sqrt(st->rr) / st->normB;
     st->resnorm = res;
@@ -242,12 +220,100 @@ __global__ void fpcg_check_kernel(PcgState *st)
     if (st->its >= st->maxIT) { st->status = TOP_ERR_NOT_CONVERGED; st->done = 1; return; }
     st->rhoOld = st->rho;
 }
+// one filter-PCG step after v = A p: x += l p, r -= l v, z = M r, rr = r.r
+// and rho = z.r in one pass (four grid strides of loads ahead of the stores;
+// each thread adds its terms in index order); the CTA that completes both
+// sums runs the iteration's check (TOP_GPU.m:637-649) and then stores rho,
+// as the separate update, check and z.r launches did (same sums, same order)
+__global__ void __launch_bounds__(256)
+fpcg_update_kernel(double *__restrict__ x, double *__restrict__ r, double *__restrict__ z,
+                   const double *__restrict__ p, const double *__restrict__ v, const double *__restrict__ invD,
+                   int64_t n, PcgState *st, double *__restrict__ part1, double *__restrict__ part2, unsigned *counter)
+{
+    if (st->done) return;
+    const double l = st->rho / st->pv;
+    double s1 = 0, s2 = 0;
+    const int64_t S = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 4 * S) {
+        double xo[4], po[4], ro[4], vo[4], dq[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i + q * S < n) {
+                const int64_t k = i + q * S;
+                xo[q] = x[k]; po[q] = p[k]; ro[q] = r[k]; vo[q] = v[k]; dq[q] = invD[k];
+            }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i + q * S < n) {
+                const int64_t k = i + q * S;
+                x[k] = xo[q] + l * po[q];
+                const double ri = ro[q] - l * vo[q];
+                r[k] = ri;
+                const double zi = dq[q] * ri;
+                z[k] = zi;
+                s1 += ri * ri;
+                s2 += zi * ri;
+            }
+    }
+    // two block sums, each as block_sum_last forms it; the last CTA adds the
+    // partials of both in index order
+    __shared__ double red[2][8];
+    __shared__ bool last;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const unsigned nb = gridDim.x, bid = blockIdx.x;
+    for (int o = 16; o > 0; o >>= 1) { s1 += __shfl_down_sync(0xffffffffu, s1, o); s2 += __shfl_down_sync(0xffffffffu, s2, o); }
+    if (lane == 0) { red[0][w] = s1; red[1][w] = s2; }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0, b = 0;
+        for (int k = 0; k < 8; ++k) a += red[0][k];
+        for (int k = 0; k < 8; ++k) b += red[1][k];
+        part1[bid] = a; part2[bid] = b;
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == nb - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double a = 0, b = 0;
+    for (unsigned k = tid; k < nb; k += 256) { a += ((volatile double *)part1)[k]; b += ((volatile double *)part2)[k]; }
+    for (int o = 16; o > 0; o >>= 1) { a += __shfl_down_sync(0xffffffffu, a, o); b += __shfl_down_sync(0xffffffffu, b, o); }
+    __syncthreads();
+    if (lane == 0) { red[0][w] = a; red[1][w] = b; }
+    __syncthreads();
+    if (tid == 0) {
+        double ta = 0, tb = 0;
+        for (int k = 0; k < 8; ++k) ta += red[0][k];
+        for (int k = 0; k < 8; ++k) tb += red[1][k];
+        *counter = 0;
+        st->rr = ta;
+        // the iteration's check, then rho for the next direction (left as it
+        // was once the solve has stopped)
+        fpcg_check(st);
+        if (!st->done) st->rho = tb;
+    }
+}
+__global__ void fpcg_zr_kernel(const double *__restrict__ z, const double *__restrict__ r, int64_t n, PcgState *st, Reduce red)
+{
+    if (st->done) return;
+    double s = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += z[i] * r[i];
+    block_sum_to<256>(s, red.partials, red.counter, red.result);
+}
 __global__ void fpcg_p_kernel(double *__restrict__ p, const double *__restrict__ z, int64_t n, const PcgState *st)
 {
     if (st->done) return;
     const double beta = st->rho / st->rhoOld;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = z[i] + beta * p[i];
+    const int64_t S = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 4 * S) {
+        double zo[4], po[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i + q * S < n) { zo[q] = z[i + q * S]; po[q] = p[i + q * S]; }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i + q * S < n) p[i + q * S] = zo[q] + beta * po[q];
+    }
 }
 __global__ void fpcg_start_kernel(PcgState *st, double tol, int maxIT)
 {
@@ -569,7 +635,8 @@ extern "C" int top_solver_filter_setup(top_solver *s, double rMin)
         f.z = s->galloc<double>(cs, 1); f.p = s->galloc<double>(cs, 1); f.v = s->galloc<double>(cs, 1);
         f.eg = s->galloc<double>(cs, 1);
         f.st = s->dalloc<PcgState>(1);
-        if (!f.act || !f.invD || !f.rhs || !f.x || !f.r || !f.z || !f.p || !f.v || !f.eg || !f.st) {
+        f.part2 = s->dalloc<double>(4096);
+        if (!f.act || !f.invD || !f.rhs || !f.x || !f.r || !f.z || !f.p || !f.v || !f.eg || !f.st || !f.part2) {
             set_error("top_solver_filter_setup: out of device memory"); return TOP_ERR_NOMEM;
         }
     }
@@ -613,11 +680,7 @@ static int filter_apply(top_solver *s, const double *src, double *tar, int *itsO
     auto iteration = [&](cudaStream_t q) {
         filter_apply_kernel<<<dim3(g.nbx, g.NZ), kNodeThreads, 0, q>>>(f.KEF, f.act, f.p, f.v, g, s->red(&f.st->pv), done);
         TOPGPU_COUNT_LAUNCH();
-        fpcg_update_kernel<<<VB, 256, 0, q>>>(f.x, f.r, f.z, f.p, f.v, f.invD, ng, f.st, s->red(&f.st->rr));
-        TOPGPU_COUNT_LAUNCH();
-        fpcg_check_kernel<<<1, 1, 0, q>>>(f.st);
-        TOPGPU_COUNT_LAUNCH();
-        fpcg_zr_kernel<<<VB, 256, 0, q>>>(f.z, f.r, ng, f.st, s->red(&f.st->rho));
+        fpcg_update_kernel<<<VB, 256, 0, q>>>(f.x, f.r, f.z, f.p, f.v, f.invD, ng, f.st, s->partials, f.part2, s->counter);
         TOPGPU_COUNT_LAUNCH();
         fpcg_p_kernel<<<VB, 256, 0, q>>>(f.p, f.z, ng, f.st);
         TOPGPU_COUNT_LAUNCH();
