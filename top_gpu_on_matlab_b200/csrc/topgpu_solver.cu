@@ -154,25 +154,33 @@ __global__ void diag_coarse_kernel(const double *__restrict__ P64, Geom g, const
         inv32[c * g.cs + idx] = on ? float(1.0 / d) : 0.0f;
     }
 }
-// Dense coarsest matrix, one thread per row (compact node n, component c):
-// each thread owns its row, so the sums are race-free and deterministic.
-__global__ void coarsest_assemble_kernel(const double *__restrict__ KsC, const int32_t *__restrict__ nodeGrid,
-                                         const int32_t *__restrict__ eleCompact, const int32_t *__restrict__ nodeCompact,
-                                         Geom g, int64_t Nn, double *__restrict__ A)
+// Dense coarsest (or condensed-tail level) matrix, one warp per row (compact
+// node n, component c): lanes (j, d), j < 8, d < 3, add the incident element
+// i's 24 entries of the row -- 24 different columns -- for i = 0..7 in turn,
+// the warp synchronised between elements, so every entry receives its
+// additions in the order of a one-thread-per-row loop over i, j, d
+// (race-free, deterministic, the same sums).
+__global__ void __launch_bounds__(256)
+coarsest_assemble_kernel(const double *__restrict__ KsC, const int32_t *__restrict__ nodeGrid,
+                         const int32_t *__restrict__ eleCompact, const int32_t *__restrict__ nodeCompact,
+                         Geom g, int64_t Nn, double *__restrict__ A)
 {
-    const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= 3 * Nn) return;
+    const int64_t row = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= 3 * Nn) return;                   // whole warps
     const int64_t n = row / 3; const int c = int(row % 3);
     const int64_t nC = 3 * Nn;
     const int64_t idx = nodeGrid[n];
+    const int j = lane / 3, d = lane % 3;
     for (int i = 0; i < 8; ++i) {
         const int64_t slot = idx - cdy(i) - g.PY * cdx(i) - g.plane * cdz(i);
         const int32_t e = eleCompact[slot];
-        if (e < 0) continue;
-        for (int j = 0; j < 8; ++j) {
+        if (e < 0) continue;                     // uniform in the warp
+        if (lane < 24) {
             const int32_t m = nodeCompact[slot + cdy(j) + g.PY * cdx(j) + g.plane * cdz(j)];
-            for (int d = 0; d < 3; ++d) A[row + nC * (3 * (int64_t)m + d)] += KsC[(int64_t)e * 576 + (3 * i + c) + 24 * (3 * j + d)];
+            A[row + nC * (3 * (int64_t)m + d)] += KsC[(int64_t)e * 576 + (3 * i + c) + 24 * (3 * j + d)];
         }
+        __syncwarp();                            // element i's additions before element i + 1's
     }
 }
 // ---- coarsest level ----
@@ -1413,7 +1421,7 @@ int build_tail(top_solver *s, cudaStream_t st)
         const int64_t n = 3 * lv.Nn, m = 3 * s->L[l + 1].Nn;
         double *K = s->tailK, *M = s->tailMs[k];
         CK(cudaMemsetAsync(K, 0, sizeof(double) * n * n, st));
-        coarsest_assemble_kernel<<<nb256(n), 256, 0, st>>>(lv.KsC, lv.nodeGrid, s->tailEleCompact[k], s->tailNodeCompact[k], lv.g, lv.Nn, K);
+        coarsest_assemble_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(lv.KsC, lv.nodeGrid, s->tailEleCompact[k], s->tailNodeCompact[k], lv.g, lv.Nn, K);
         tail_jacobi_kernel<<<nb256(n), 256, 0, st>>>(s->tailJ, lv.invD64, lv.nodeGrid, lv.Nn, lv.g.cs, s->p.omega);
         tail_q_kernel<<<nb256(n * m), 256, 0, st>>>(s->tailQ, s->tailPt[k], K, s->tailJ, s->tailNbr[k], n, m);
         dgemm(st, false, true, s->tailT, n, s->tailQ, n, Mnext, m, n, m, m, 1.0, 0.0, false, false);   // T = Q M'
@@ -1508,7 +1516,7 @@ extern "C" int top_solver_assemble(top_solver *s)
     DevLevel &lc = s->L[s->nL - 1];
     const int64_t n = s->nC;
     CK(cudaMemsetAsync(s->Ac, 0, sizeof(double) * n * n, st));
-    coarsest_assemble_kernel<<<nb256(n), 256, 0, st>>>(lc.KsC, lc.nodeGrid, s->eleCompactC, s->nodeCompactC, lc.g, lc.Nn, s->Ac);
+    coarsest_assemble_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(lc.KsC, lc.nodeGrid, s->eleCompactC, s->nodeCompactC, lc.g, lc.Nn, s->Ac);
     TOPGPU_COUNT_LAUNCH();
     CK(cudaMemsetAsync(s->zeroDone, 0, sizeof(int) * 4, st));
     { const int rc = coarsest_inverse(s, st); if (rc) return rc; }
