@@ -193,6 +193,8 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, i
                      T *__restrict__ x, Geom g, const int32_t *__restrict__ nodeGrid,
                      const int *__restrict__ done0, int64_t vs, int nv, int staged)
 {
+    // staged 1: the right-hand sides gathered from the grid into shared memory;
+    // 2 (FP64): read from their compact copy r; 0: read from the grid per term
     pdl_enter();
     __shared__ double red[kCoarsestThreads / 32][4];
     extern __shared__ double rstage[];           // staged: the right-hand sides [4][n]
@@ -208,7 +210,7 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, i
         }
         if (!any) continue;                      // uniform in the CTA
         double out[4];
-        if (staged) {
+        if (staged == 1) {
             // the right-hand sides into shared memory first (all the node-map
             // loads of a thread, then all its value loads), then the same sums
             __syncthreads();                     // the previous group's reads are done
@@ -230,6 +232,10 @@ coarsest_gemv_kernel(const double *__restrict__ Ainv, const T *__restrict__ r, i
             }
             __syncthreads();
             coarsest_row(Ainv + n * row, StagedRhs{rstage, n, v0}, n, v0, act, red, out);
+        } else if (staged == 2) {
+            // FP64: r is the compact copy the restriction wrote ([k][n], the same values)
+            if constexpr (sizeof(T) == 8)
+                coarsest_row(Ainv + n * row, CompactRhs{reinterpret_cast<const double *>(r), n}, n, v0, act, red, out);
         } else {
             coarsest_row(Ainv + n * row, GridRhs<T>{r, vs, g.cs, nodeGrid}, n, v0, act, red, out);
         }
@@ -729,6 +735,8 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
     // in the precision of the solver's V-cycle
     const bool tailT = sizeof(T) == (s->p.precision == TOP_PREC_MIXED ? 4u : 8u);
     const int tl = (!persist && tailT && s->tailReady && tail_on(s)) ? s->tailL : 0;
+    // FP64 coarsest GEMV reading the compact copy of its right-hand sides
+    const bool cmpC = sizeof(T) == 8 && !persist && !tl && nv <= s->kMax;
     if (!z1Ready) {
         DevLevel &l0 = s->L[0];
         const int64_t n0 = lvs(l0), M = kMargin;
@@ -746,9 +754,12 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         else
             coarse_op<T>(s, l, JacobiIn<T, T>{vr<T>(lv), invd<T>(lv), lv.g.cs, omega, vs}, ResidOut<T, T, T>{vr<T>(lv), d, lv.g.cs, vs},
                          none, done, nv);
-        // into the tail's level: r also in compact order, the GEMV's operand
+        // into the tail's level: r also in compact order, the GEMV's operand;
+        // likewise (FP64) into the coarsest level for its GEMV
         if (tl && l + 1 == tl)
             restrict_op<T>(s, l, d, vr<T>(lc), done, nv, static_cast<T *>(s->tailR), s->tailNodeCompact[0], s->tailLd);
+        else if (cmpC && l + 1 == nL - 1)
+            restrict_op<T>(s, l, d, vr<T>(lc), done, nv, reinterpret_cast<T *>(s->cr), s->nodeCompactC, s->nC);
         else
             restrict_op<T>(s, l, d, vr<T>(lc), done, nv);
     }
@@ -787,9 +798,10 @@ void vcycle(top_solver *s, const TR *r0, TZ *z0, double *zr, const int *done, in
         TOPGPU_COUNT_LAUNCH();
     } else {
         // coarsest direct solve, FP64 (the right-hand side read from the grid by the product)
-        const size_t sm = gemv_stage_bytes<T>(n, nv);
-        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, sm, s->st, s->Ainv, (const T *)vr<T>(lc), n, vt<T>(lc), lc.g,
-                 lc.nodeGrid, done, lvs(lc), nv, sm ? 1 : 0);
+        const size_t sm = cmpC ? 0 : gemv_stage_bytes<T>(n, nv);
+        launch_k(s, coarsest_gemv_kernel<T>, (unsigned)n, kCoarsestThreads, sm, s->st, s->Ainv,
+                 cmpC ? reinterpret_cast<const T *>(s->cr) : (const T *)vr<T>(lc), n, vt<T>(lc), lc.g,
+                 lc.nodeGrid, done, lvs(lc), nv, cmpC ? 2 : (sm ? 1 : 0));
         TOPGPU_COUNT_LAUNCH();
     }
     // interpolation leg
