@@ -199,7 +199,9 @@ int assemble_level2_f64(double *Ks, const int32_t *upMap, const double *E, const
     if (nElem == 0) return TOP_OK;
     if (nCh <= kGemmK) {
         cudaFuncSetAttribute(dgemm_k64_kernel<Level2Row>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
-        dim3 grid((unsigned)((nElem + kGemmBM - 1) / kGemmBM), (576 + kGemmBN - 1) / kGemmBN);
+        // one CTA per row block, looping over the column tiles (the gathered A
+        // tile loaded once instead of once per column tile)
+        dim3 grid((unsigned)((nElem + kGemmBM - 1) / kGemmBM), 1);
         // B = Qscratch has 64 rows whatever nCh is: the GEMM's K tiles load rows
         // nCh..63 too and multiply them by the zero A entries that ARow returns
         // there, so those rows must exist and hold finite values (0 * NaN = NaN)

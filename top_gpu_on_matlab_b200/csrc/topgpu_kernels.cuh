@@ -112,47 +112,51 @@ dgemm_k64_kernel(double *__restrict__ C, int64_t M, int N, int64_t ldc,
     double *sA = smem;                                  // [BM][K + pad]
     double *sB = smem + kGemmBM * (kGemmK + kGemmPad);  // [K][BN + pad]
     const int64_t m0 = (int64_t)blockIdx.x * kGemmBM;
-    const int n0 = blockIdx.y * kGemmBN;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // A tile: thread per (row, k) pair, 32 rows per pass
+    // A tile (gathered rows: a few dependent loads each), once per CTA: thread
+    // per (row, k) pair, 32 rows per pass
     for (int idx = tid; idx < kGemmBM * kGemmK; idx += 128) {
         const int r = idx % kGemmBM, k = idx / kGemmBM;
         const int64_t m = m0 + r;
         sA[r * (kGemmK + kGemmPad) + k] = (m < M) ? arow(m, k) : 0.0;
     }
-    for (int idx = tid; idx < kGemmK * kGemmBN; idx += 128) {
-        const int k = idx / kGemmBN, c = idx % kGemmBN;
-        sB[k * (kGemmBN + kGemmPad) + c] = (n0 + c < N) ? B[(size_t)k * ldb + n0 + c] : 0.0;
-    }
-    __syncthreads();
-    const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;
-    const int g = lane >> 2, q = lane & 3;
-    double acc[4][4][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-#pragma unroll 4
-    for (int k0 = 0; k0 < kGemmK; k0 += 4) {
-        double a[4], b[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = sA[(wr + 8 * i + g) * (kGemmK + kGemmPad) + k0 + q];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = sB[(k0 + q) * (kGemmBN + kGemmPad) + wc + 8 * j + g];
+    // the CTA's column tiles in turn, the A tile reused from shared memory
+    for (int n0 = blockIdx.y * kGemmBN; n0 < N; n0 += gridDim.y * kGemmBN) {
+        __syncthreads();                                    // sB free (and sA complete)
+        for (int idx = tid; idx < kGemmK * kGemmBN; idx += 128) {
+            const int k = idx / kGemmBN, c = idx % kGemmBN;
+            sB[k * (kGemmBN + kGemmPad) + c] = (n0 + c < N) ? B[(size_t)k * ldb + n0 + c] : 0.0;
+        }
+        __syncthreads();
+        const int wr = (warp & 1) * 32, wc = (warp >> 1) * 32;
+        const int g = lane >> 2, q = lane & 3;
+        double acc[4][4][2];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-    }
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 4
+        for (int k0 = 0; k0 < kGemmK; k0 += 4) {
+            double a[4], b[4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int64_t m = m0 + wr + 8 * i + g;
-        if (m >= M) continue;
+            for (int i = 0; i < 4; ++i) a[i] = sA[(wr + 8 * i + g) * (kGemmK + kGemmPad) + k0 + q];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = n0 + wc + 8 * j + 2 * q;
-            if (n < N) C[m * ldc + n] = acc[i][j][0];
-            if (n + 1 < N) C[m * ldc + n + 1] = acc[i][j][1];
+            for (int j = 0; j < 4; ++j) b[j] = sB[(k0 + q) * (kGemmBN + kGemmPad) + wc + 8 * j + g];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int64_t m = m0 + wr + 8 * i + g;
+            if (m >= M) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int n = n0 + wc + 8 * j + 2 * q;
+                if (n < N) C[m * ldc + n] = acc[i][j][0];
+                if (n + 1 < N) C[m * ldc + n + 1] = acc[i][j][1];
+            }
         }
     }
 }
