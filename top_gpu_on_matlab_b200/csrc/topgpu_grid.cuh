@@ -827,6 +827,19 @@ coarse_gather_kernel(Out out0, const T *__restrict__ W0, int64_t wvs, Geom g, Re
 // One lane group per coarse node (32 lanes for span 4, 8 for span 2): the
 // (2S-1)^2 (z, x) tap columns are dealt out over the group, each lane runs
 // its columns' 2S-1 y taps, the group adds up with shuffles.
+// (a, b, c) of index k = a + na (b + nb c), k < na nb nc: 32-bit unsigned
+// division when k fits (every grid here), the 64-bit one otherwise (the
+// same results; a 64-bit division by a run-time value is a long sequence)
+__device__ __forceinline__ void split3(int64_t k, int na, int nb, int &a, int &b, int &c)
+{
+    if (k < (int64_t)0xffffffff) {
+        const unsigned u = (unsigned)k, q = u / (unsigned)na;
+        a = (int)(u - q * (unsigned)na); b = (int)(q % (unsigned)nb); c = (int)(q / (unsigned)nb);
+    } else {
+        a = (int)(k % na); b = (int)((k / na) % nb); c = (int)(k / ((int64_t)na * nb));
+    }
+}
+
 template <int S> struct RestrictLanes { static constexpr int value = (S >= 4) ? 32 : 8; };
 
 // lane-group restriction of one coarse node; gt = the thread's index in the
@@ -842,7 +855,8 @@ __device__ __forceinline__ void restrict_lanes(const T *__restrict__ rf, const G
     const int64_t nq = (int64_t)gc.PY * gc.NX * gc.NZ;
     const bool inRange = node < nq;
     const int64_t nq2 = inRange ? node : 0;
-    const int QY = int(nq2 % gc.PY), QX = int((nq2 / gc.PY) % gc.NX), QZ = int(nq2 / ((int64_t)gc.PY * gc.NX));
+    int QY, QX, QZ;
+    split3(nq2, gc.PY, gc.NX, QY, QX, QZ);
     const bool valid = inRange && QY < gc.NY;
     const int64_t ic = gc.origin + QY + (int64_t)gc.PY * QX + gc.plane * QZ;
     T acc[3] = {T(0), T(0), T(0)};
@@ -922,7 +936,8 @@ restrict_y_kernel(const T *__restrict__ rf, Geom gf, T *__restrict__ t, int NYc,
     const int64_t nt = (int64_t)NYc * gf.NX * gf.NZ;
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nt) return;
-    const int QY = (int)(k % NYc), X = (int)((k / NYc) % gf.NX), Z = (int)(k / ((int64_t)NYc * gf.NX));
+    int QY, X, Z;
+    split3(k, NYc, gf.NX, QY, X, Z);
     const int64_t base = gf.origin + (int64_t)gf.PY * X + gf.plane * Z;
     T acc[3] = {T(0), T(0), T(0)};
     if constexpr (V4) {
@@ -1102,7 +1117,8 @@ prolong4_kernel(const T *__restrict__ xc, Geom gc, T *__restrict__ xf, Geom gf,
     const int nqy = (gf.NY + S - 1) / S;
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (int64_t)nqy * gf.NX * gf.NZ) return;
-    const int qy = (int)(k % nqy), X = (int)((k / nqy) % gf.NX), Z = (int)(k / ((int64_t)nqy * gf.NX));
+    int qy, X, Z;
+    split3(k, nqy, gf.NX, qy, X, Z);
     const int qx = X / S, rx = X - qx * S, qz = Z / S, rz = Z - qz * S;
     const T wx[2] = {T(S - rx) / T(S), T(rx) / T(S)};
     const T wz[2] = {T(S - rz) / T(S), T(rz) / T(S)};
