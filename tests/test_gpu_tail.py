@@ -159,3 +159,26 @@ def test_tail_batched_rhs_equal_per_load(mixed):
         Uk, its_k, res_k = s.pcg(k)
         assert its_b[k] == its_k and res_b[k] == res_k, k
         assert torch.equal(Ub[k * nd:(k + 1) * nd], Uk), k
+
+
+@pytest.mark.parametrize("case", ["no_level", "super_element"])
+def test_tail_not_used_where_it_does_not_apply(case):
+    """no level between level 1 and the coarsest with at most 2500 DOFs
+    (40x80x40, control 3000: level 1 has 7623), or super-element mode (the
+    level-0 operator is per-element): the tail reports level 0 and the
+    V-cycle is the launched steps', bit for bit"""
+    from top_gpu_on_matlab_b200.fea import Mesh, Solver
+    if case == "no_level":
+        m = Mesh(np.ones((40, 80, 40), bool), control=3000)
+    else:
+        m = Mesh(np.ones((10, 60, 10), bool), control=20000, super_element=1)
+    m.apply_optcase(1)
+    s = Solver(m, E0=1.0, Emin=1e-9, penal=3.0, tol=1e-6, maxIT=800, omega=0.6, mixed=True)
+    s.set_density(torch.full((s.num_design,), 0.5, dtype=torch.float64, device="cuda"))
+    s.assemble()
+    r = torch.from_numpy(np.random.default_rng(15).standard_normal(s.numDOFs)).cuda()
+    assert s.set_tail_operator(None) == 0
+    z0 = s.vcycle(r)
+    assert s.set_tail_operator(True) == 0
+    z1 = s.vcycle(r)
+    assert torch.equal(z0, z1)
