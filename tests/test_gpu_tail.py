@@ -134,7 +134,7 @@ def test_tail_vcycle_matches_oracle():
 @pytest.mark.parametrize("mixed", [False, True])
 def test_tail_batched_rhs_equal_per_load(mixed):
     """several load cases in one batched PCG pass through the tail GEMV
-    together (right-hand sides staged four at a time): every load case's
+    together (four right-hand sides per pass of the GEMV): every load case's
     iterates equal its own PCG bit for bit"""
     from top_gpu_on_matlab_b200.fea import Mesh
     ny, nx, nz = 16, 32, 16
